@@ -1,0 +1,300 @@
+"""Pins the CPU oracle to the reference's own golden vectors (tests/golden/).
+
+Every assertion here compares the C++ restatement with a value the reference's
+tests or checked-in benchmark reports hold.  Python's hashlib (FIPS 202) is an
+independent SHA3 cross-check.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from tests import generators as G
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_sha3_and_keccak_kats(oracle, golden):
+    assert oracle.sha3_256(b"").hex() == golden["sha3_empty"]["hex"]
+    assert oracle.sha3_256(b"abc").hex() == golden["sha3_abc"]["hex"]
+    assert oracle.keccak_256(b"").hex() == golden["keccak_empty"]["hex"]
+    assert oracle.keccak_256(b"abc").hex() == golden["keccak_abc"]["hex"]
+    for length, want in golden["sha3_rate_boundary"]["cases"]:
+        assert oracle.sha3_256(G.sha3_pattern(length)).hex() == want
+    for length, want in golden["keccak_rate_boundary"]["cases"]:
+        assert oracle.keccak_256(G.sha3_pattern(length)).hex() == want
+    assert oracle.sha3_256(b"") != oracle.keccak_256(b"")
+
+
+@pytest.mark.parametrize("length", [0, 1, 31, 32, 64, 128, 135, 136, 137, 200, 272, 513])
+def test_sha3_matches_hashlib(oracle, length):
+    msg = bytes((i * 131 + 7) & 0xFF for i in range(length))
+    assert oracle.sha3_256(msg) == hashlib.sha3_256(msg).digest()
+
+
+def test_keccak_f1600_zero_state_kat(oracle):
+    # Keccak-f[1600] applied once to the all-zero state (Keccak team's published
+    # intermediate value; first lane F1258F7940E1DDE7).
+    out = oracle.keccak_f1600(np.zeros(200, np.uint8))
+    lanes = np.frombuffer(out.tobytes(), dtype="<u8")
+    assert int(lanes[0]) == 0xF1258F7940E1DDE7
+    assert int(lanes[1]) == 0x84D5CCF933C0478A
+
+
+def test_hash_batch_layout(oracle):
+    for length in [0, 32, 64, 128, 136]:
+        count, stride, ostride = 7, (length + 5 if length else 0), 40
+        msgs = G.make_batch_messages(count, stride, length)
+        out = oracle.hash_batch(msgs, count, stride, length, ostride)
+        for i in range(count):
+            m = msgs[i * stride:i * stride + length]
+            assert out[i * ostride:i * ostride + 32] == hashlib.sha3_256(m).digest()
+            assert out[i * ostride + 32:(i + 1) * ostride] == b"\0" * (ostride - 32)
+
+
+def test_hash_batch_rejects_past_rate(oracle):
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.hash_batch(b"\0" * 137, 1, 137, 137)
+    assert e.value.code == 3  # unsupportedOneBlockLength
+
+
+def test_merkle_roots_from_reference_tests(oracle, golden):
+    v = golden["merkle_root_8x32"]
+    leaves = G.make_leaves(8, 32, 32)
+    assert oracle.merkle_root(leaves, 8, 32, 32).hex() == v["hex"]
+    v = golden["merkle_root_1024x32_salt71"]
+    leaves = G.make_leaves(1024, 32, 32, salt=71)
+    assert oracle.merkle_root(leaves, 1024, 32, 32).hex() == v["hex"]
+
+
+def test_merkle_roots_from_reference_bench_16384(oracle, golden):
+    roots = golden["bench_merkle_roots_16384"]["roots_by_leaf_length"]
+    for length, want in roots.items():
+        length = int(length)
+        leaves = G.make_bench_leaves(16384, length)
+        assert oracle.merkle_root(leaves, 16384, length, length).hex() == want, length
+
+
+def test_merkle_opening_verify_and_literal(oracle):
+    leaves = G.make_leaves(16, 72, 64, salt=41)
+    root, [sib] = oracle.merkle_openings(leaves, 16, 72, 64, [11])
+    assert len(sib) == 4
+    leaf = leaves[11 * 72:11 * 72 + 64]
+    assert oracle.merkle_verify(leaf, 11, sib, root)
+    bad = bytes([leaf[0] ^ 0x80]) + leaf[1:]
+    assert not oracle.merkle_verify(bad, 11, sib, root)
+    lroot, lsib = oracle.merkle_opening_literal(leaves, 16, 72, 64, 11)
+    assert lroot == root and lsib == sib
+    assert root == oracle.merkle_root(leaves, 16, 72, 64)
+
+
+def test_merkle_rejects_malformed(oracle):
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.merkle_root(b"\0" * 96, 3, 32, 32)
+    assert e.value.code == 2  # invalidLeafCount
+    with pytest.raises(oracle.OracleError):
+        oracle.merkle_root(b"\0" * 31, 1, 32, 32)
+    with pytest.raises(oracle.OracleError):
+        oracle.merkle_openings(G.make_leaves(4, 32, 32), 4, 32, 32, [4])
+
+
+def test_transcript_squeeze_vector(oracle, golden):
+    data = bytes((i * 31) & 0xFF for i in range(513))
+    words = golden["transcript_squeeze_40"]["words"]
+    assert oracle.transcript_squeeze([data], 40, G.P) == words
+    # squeeze is non-mutating: repeated squeezes agree
+    assert oracle.transcript_squeeze([data], 8, G.P) == words[:8]
+
+
+def test_sumcheck_chunk_vector(oracle, golden):
+    v = golden["sumcheck_chunk_16x3"]
+    ev = [(i + 1) * 17 for i in range(16)]
+    fin, co, ch = oracle.sumcheck_chunk(ev, 3)
+    assert fin == v["final"] and ch == v["challenges"] and co == v["coefficients"]
+
+
+def test_circle_layout_log3(oracle, golden):
+    # natural-order point indices of the canonical log-3 domain are (1,5,9,...)*2^27
+    pts = oracle.domain_points(3)  # storage (bit-reversed) order
+    v = golden["circle_layout_log3"]
+    # storage index s holds natural index bitrev(s)
+    nat = [int(f"{s:03b}"[::-1], 2) for s in range(8)]
+    # recompute the expected points from the pinned indices
+    gen = (2, 1268011823)
+
+    def mul(p, q):
+        return ((p[0] * q[0] - p[1] * q[1]) % G.P, (p[0] * q[1] + p[1] * q[0]) % G.P)
+
+    def power(k):
+        r, b = (1, 0), gen
+        while k:
+            if k & 1:
+                r = mul(r, b)
+            b = mul(b, b)
+            k >>= 1
+        return r
+
+    for s in range(8):
+        idx = v["natural_indices_over_2^27"][nat[s]] << 27
+        assert tuple(int(x) for x in pts[s]) == power(idx)
+
+
+def test_circle_log5_stable_digests(oracle, golden):
+    v = golden["circle_log5_digests"]
+    pts = oracle.domain_points(5)
+    assert oracle.sha3_256(pts.astype("<u4").tobytes()).hex() == v["points"]
+    tw = oracle.fft_twiddles(5)
+    assert len(tw) == 31
+    assert oracle.sha3_256(tw.astype("<u4").tobytes()).hex() == v["fft_twiddles"]
+    layers = oracle.inverse_layers(5, 4)
+    q = np.concatenate([np.stack([l, 0 * l, 0 * l, 0 * l], axis=1) for l in layers]).astype("<u4")
+    assert oracle.sha3_256(q.tobytes()).hex() == v["inverse_layers_4"]
+
+
+@pytest.mark.parametrize("log_size", [1, 2, 3, 4, 5, 6])
+def test_fft_matches_direct_evaluation(oracle, log_size):
+    # CircleDomainTests.swift:1200-1240
+    half = 1 << (log_size - 1)
+    cases = [
+        (np.array([[7, 11, 13, 17]], np.uint32), np.zeros((0, 4), np.uint32)),
+        (np.zeros((0, 4), np.uint32), np.array([[19, 23, 29, 31]], np.uint32)),
+        (G.deterministic_qm31_coefficients(half, 0x40), G.deterministic_qm31_coefficients(half, 0x80)),
+    ]
+    for x, y in cases:
+        coeffs = oracle.fft_basis_coefficients(log_size, x, y)
+        assert coeffs.shape == (1 << log_size, 4)
+        fft = oracle.fft_evaluate(log_size, coeffs)
+        direct = oracle.evaluate_direct(log_size, x, y)
+        assert np.array_equal(fft, direct)
+
+
+def test_first_fold_proof_digest_log4(oracle, golden):
+    v = golden["circle_first_fold_proof_log4"]
+    ev = G.stable_circle_evaluations(16)
+    pub = bytes(0x10 + i for i in range(32))
+    r = oracle.prove(4, ev, 2, 3, pub, 1)
+    assert oracle.sha3_256(r.proof).hex() == v["hex"]
+    assert oracle.verify(r.proof, pub)
+    oracle.proof_roundtrip(r.proof)
+
+
+def test_three_round_proof_digest_log5(oracle, golden):
+    v = golden["circle_3round_proof_log5"]
+    ev = G.stable_circle_evaluations(32)
+    pub = bytes(0x50 + i for i in range(32))
+    r = oracle.prove(5, ev, 2, 5, pub, 3)
+    assert len(r.commitments) == 3 and r.final_layer.shape == (4, 4)
+    assert oracle.sha3_256(r.proof).hex() == v["hex"]
+    assert oracle.verify(r.proof, pub)
+    # final layer = explicit fold chain with the transcript's challenges
+    assert np.array_equal(oracle.circle_fold_chain(5, ev, r.challenges), r.final_layer)
+    assert not oracle.verify(r.proof, bytes([0x44] * 32))
+
+
+def _corpus(golden):
+    c = golden["corpus"]
+    valid = open(os.path.join(GOLDEN, c["valid_file"]), "rb").read()
+
+    def q(hexes):
+        return np.array([[int.from_bytes(bytes.fromhex(h)[4 * k:4 * k + 4], "little") for k in range(4)] for h in hexes], np.uint32)
+
+    return c, valid, q(c["x_hex"]), q(c["y_hex"])
+
+
+def test_corpus_valid_proof(oracle, golden):
+    c, valid, x, y = _corpus(golden)
+    prof = c["profile"]
+    assert len(valid) == c["valid_bytes"]
+    assert oracle.sha3_256(valid).hex() == c["valid_digest"]
+    oracle.proof_roundtrip(valid)
+    assert oracle.claim_digest(c["log"], x, y, c["claimed"]).hex() == c["public_digest"]
+    assert oracle.verify_contract(valid, c["log"], x, y, c["claimed"], prof["logBlowupFactor"], prof["queryCount"], prof["grindingBits"]) == 1
+
+
+def test_corpus_proof_regenerated_bit_exact(oracle, golden):
+    """Re-prove the corpus statement with the oracle builder: same 31,788 bytes."""
+    c, valid, x, y = _corpus(golden)
+    prof = c["profile"]
+    ev = oracle.evaluate_direct(c["log"], x, y)
+    pub = bytes.fromhex(c["public_digest"])
+    r = oracle.prove(c["log"], ev, prof["logBlowupFactor"], prof["queryCount"], pub, c["rounds"], prof["grindingBits"], claimed=c["claimed"])
+    assert r.proof == valid
+
+
+def test_corpus_tamper_vectors(oracle, golden):
+    c, valid, x, y = _corpus(golden)
+    prof = c["profile"]
+    assert len(c["tampers"]) == 3
+    for t in c["tampers"]:
+        if "patch" in t:
+            b = bytearray(valid)
+            for off, val in t["patch"]:
+                b[off] = val
+            b = bytes(b)
+        else:
+            b = open(os.path.join(GOLDEN, t["file"]), "rb").read()
+        assert len(b) == t["bytes"] and oracle.sha3_256(b).hex() == t["digest"], t["id"]
+        oracle.proof_roundtrip(b)
+        got = oracle.verify_contract(b, c["log"], x, y, c["claimed"], prof["logBlowupFactor"], prof["queryCount"], prof["grindingBits"])
+        assert got == (1 if t["expected_accepted"] else 0), t["id"]
+        if t["id"] == "developer-parameter-proof-rejected-by-contract":
+            # accepted by the artifact verifier with its own parameters
+            assert oracle.verify(b, bytes.fromhex(c["public_digest"]))
+
+
+def test_bench_first_fold_log14(oracle, golden):
+    v = golden["bench_circle_first_fold_log14"]
+    ev = G.deterministic_qm31(1 << 14, v["salts"])
+    out = oracle.circle_fold_chain(14, ev, np.array([v["challenge"]], np.uint32))
+    assert oracle.sha3_256(out.astype("<u4").tobytes()).hex() == v["hex"]
+
+
+def test_bench_explicit_chain_log14(oracle, golden):
+    v = golden["bench_circle_fold_chain_explicit_log14"]
+    ev = G.deterministic_qm31(1 << 14, v["salts"])
+    out = oracle.circle_fold_chain(14, ev, G.circle_fri_challenges(3))
+    assert oracle.sha3_256(out.astype("<u4").tobytes()).hex() == v["hex"]
+
+
+def test_bench_merkle_transcript_chain_log14(oracle, golden):
+    v = golden["bench_circle_fold_chain_merkle_log14"]
+    ev = G.deterministic_qm31(1 << 14, v["salts"])
+    pub = bytes(0x90 + i for i in range(32))
+    r = oracle.prove(14, ev, 2, 4, pub, 3)
+    assert oracle.sha3_256(r.final_layer.astype("<u4").tobytes()).hex() == v["hex"]
+    assert len(r.proof) == v["proof_bytes"]
+
+
+@pytest.mark.parametrize("log_size", [10, 14])
+def test_bench_codeword_prover(oracle, golden, log_size):
+    v = golden[f"bench_codeword_prover_log{log_size}"]
+    x, y = G.bench_codeword_polynomial(1 << log_size)
+    direct = oracle.evaluate_direct(log_size, x, y)
+    assert oracle.sha3_256(direct.astype("<u4").tobytes()).hex() == v["codeword_hex"]
+    fft = oracle.fft_evaluate(log_size, oracle.fft_basis_coefficients(log_size, x, y))
+    assert np.array_equal(fft, direct)
+    pub = bytes(0xA0 + i for i in range(32))
+    r = oracle.prove(log_size, direct, 2, 4, pub, 3)
+    assert len(r.proof) == v["proof_bytes"]
+    assert oracle.sha3_256(r.proof).hex() == v["proof_hex"]
+    assert oracle.verify(r.proof, pub)
+
+
+def test_qm31_field_identities(oracle):
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        x = tuple(int(v) for v in rng.integers(0, G.P, 4))
+        xi = oracle.qm31_inv(x)
+        assert oracle.qm31_mul(x, xi) == (1, 0, 0, 0)
+
+
+def test_multilinear_sumcheck_relations(oracle):
+    ev = [(i * 7919 + 13) % G.P for i in range(64)]
+    p = oracle.sumcheck_multilinear(ev)
+    assert p["claimed_sum"] == sum(ev) % G.P
+    prev = p["claimed_sum"]
+    for z, o, c in zip(p["r0"], p["r1"], p["challenges"]):
+        assert (int(z) + int(o)) % G.P == prev
+        prev = ((1 - int(c)) * int(z) + int(c) * int(o)) % G.P
+    assert prev == p["final"]
