@@ -1,0 +1,36 @@
+"""apple_b200: B200 (sm_100a) commit-and-fold superstep behind a C ABI.
+
+Python mirror of AppleZKProver's plan API over libazk_cuda.so (include/azk_cuda.h).
+The CUDA library is the product; this module only marshals arguments.  Importing
+it loads the in-tree shared library and fails loudly when it is missing: there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+from ._capi import (  # noqa: F401
+    AZK_STATUS_NAMES,
+    AZKError,
+    Schedule,
+    Stats,
+    lib,
+    library_path,
+)
+from .plans import (  # noqa: F401
+    BatchProver,
+    CircleCodewordPlan,
+    CirclePCSFRIProver,
+    Context,
+    KeccakF1600PermutationPlan,
+    SHA3FixedOneBlockHashPlan,
+    SHA3RawLeavesMerkleCommitPlan,
+    circle_domain_points,
+    circle_fft_twiddles,
+    circle_fold_chain,
+    circle_inverse_layers,
+    circle_merkle_fold_chain,
+    commit_prehashed_leaves,
+    pcs_proof_size,
+    qm31_fold,
+    qm31_merkle_fold_chain,
+    qm31_transcript_challenges,
+)

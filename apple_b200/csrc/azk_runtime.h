@@ -1,0 +1,201 @@
+// Host-side runtime shared by the C-ABI translation units: context, error
+// handling, device buffers, domain-table cache and the work-list builders.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/azk_cuda.h"
+#include "azk_internal.h"
+
+struct azk_ctx {
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  uint64_t total_mem = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  std::string last_error;
+  struct Domain {
+    uint32_t* tw = nullptr;
+    uint32_t* inv = nullptr;
+  };
+  std::map<uint32_t, Domain> domains;
+};
+
+namespace azk {
+
+struct Error {
+  azk_status code;
+  std::string msg;
+};
+
+[[noreturn]] inline void fail(azk_status code, const std::string& msg) { throw Error{code, msg}; }
+inline void require(bool ok, azk_status code, const std::string& msg) {
+  if (!ok) fail(code, msg);
+}
+inline void layout(bool ok, const char* what = "The provided input bytes do not match the declared count/stride/length layout.") {
+  if (!ok) fail(AZK_ERR_INVALID_INPUT_LAYOUT, what);
+}
+
+#define AZK_CU(expr)                                                                                   \
+  do {                                                                                                 \
+    cudaError_t azk_e_ = (expr);                                                                       \
+    if (azk_e_ != cudaSuccess)                                                                         \
+      ::azk::fail(AZK_ERR_COMMAND_EXECUTION_FAILED, std::string(#expr) + ": " + cudaGetErrorString(azk_e_)); \
+  } while (0)
+
+void set_error(const azk_ctx* ctx, const std::string& msg);
+
+template <class F>
+azk_status guarded(const azk_ctx* ctx, F&& f) {
+  try {
+    f();
+    return AZK_OK;
+  } catch (const Error& e) {
+    set_error(ctx, e.msg);
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error(ctx, "host allocation failed");
+    return AZK_ERR_FAILED_TO_CREATE_BUFFER;
+  } catch (const std::exception& e) {
+    set_error(ctx, e.what());
+    return AZK_ERR_COMMAND_EXECUTION_FAILED;
+  }
+}
+
+inline bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+inline uint32_t ilog2(uint64_t v) {
+  uint32_t r = 0;
+  while (v > 1) { v >>= 1; r++; }
+  return r;
+}
+inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+// Owning device allocation.
+struct DevBuf {
+  void* p = nullptr;
+  uint64_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(uint64_t n, const char* label = "buffer") { alloc(n, label); }
+  void alloc(uint64_t n, const char* label = "buffer") {
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      fail(AZK_ERR_FAILED_TO_CREATE_BUFFER, std::string("Failed to create device buffer '") + label + "' of length " + std::to_string(n));
+    }
+    bytes = n;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// Bump allocator over one device allocation (the reference's ResidencyArena,
+// Planner/ResidencyArena.swift:36-92: 256-byte aligned slices).
+struct Arena {
+  DevBuf buf;
+  uint64_t used = 0;
+  std::vector<std::pair<uint64_t, uint64_t>> plan;  // (offset, bytes) reservations before alloc
+  uint64_t reserve(uint64_t bytes) {
+    uint64_t off = align_up(used, 256);
+    used = off + (bytes ? bytes : 16);
+    return off;
+  }
+  void commit(const char* label) { buf.alloc(used, label); }
+  template <class T>
+  T* at(uint64_t off) const { return reinterpret_cast<T*>(reinterpret_cast<uint8_t*>(buf.p) + off); }
+};
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double seconds() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+  uint64_t ns() const { return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+// CUDA events around a region of one stream.
+struct GpuTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit GpuTimer(cudaStream_t st) : s(st) {
+    AZK_CU(cudaEventCreate(&a));
+    AZK_CU(cudaEventCreate(&b));
+    AZK_CU(cudaEventRecord(a, s));
+  }
+  void stop() { AZK_CU(cudaEventRecord(b, s)); }
+  double seconds() {
+    float ms = 0;
+    AZK_CU(cudaEventSynchronize(b));
+    AZK_CU(cudaEventElapsedTime(&ms, a, b));
+    return ms / 1000.0;
+  }
+  ~GpuTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+inline void fill_stats(azk_stats* st, const Timer& t, uint64_t submit_ns, double gpu_s) {
+  if (!st) return;
+  st->cpu_wall_s = t.seconds();
+  st->gpu_s = gpu_s;
+  st->cpu_submit_ns = submit_ns;
+}
+
+// Domain tables of size 2^logn, materialised once per context.
+const azk_ctx::Domain& domain_tables(azk_ctx* ctx, uint32_t logn);
+
+// Resolved hashing schedule.
+struct Sched {
+  uint32_t tile_log = 10;
+  uint32_t group_log = 10;
+  uint32_t threads = 256;
+  bool graph = true;
+};
+Sched resolve_schedule(const azk_schedule* s);
+// Tile depth used for a tree of 2^logn leaves under a schedule.
+inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
+  uint32_t t = s.tile_log < logn ? s.tile_log : logn;
+  return t;
+}
+
+// FFT work for a set of transforms: one FftJob per (transform, pass); passes of
+// all transforms are aligned so every transform's last (low-stage) pass runs at
+// the final step.
+struct FftPlan {
+  std::vector<FftJob> jobs;
+  std::vector<uint2> work;                       // all steps, step-major, transform-contiguous
+  std::vector<uint64_t> step_off, step_cnt;      // per step
+  std::vector<std::vector<std::pair<uint64_t, uint64_t>>> inst_range;  // [step][transform] -> (offset, count)
+  DevBuf d_jobs, d_work;
+  void build(const std::vector<FftJob>& transforms);
+  void upload(cudaStream_t s);
+  void launch_step(size_t step, cudaStream_t s) const;
+  void launch_step_for(size_t step, size_t t, cudaStream_t s) const;
+  void launch_all(cudaStream_t s) const {
+    for (size_t k = 0; k < step_cnt.size(); k++) launch_step(k, s);
+  }
+};
+
+// Monomial -> interleaved circle FFT-basis coefficients, host-side like the
+// reference's CircleCodewordPlan (CircleCodeword.swift:100-127, 187-263).
+std::vector<uint32_t> fft_basis_from_monomials(uint32_t logn, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny);
+
+}  // namespace azk

@@ -1,0 +1,252 @@
+// SHA3 Merkle commitment kernels: fused leaf hashing + shared-memory treelets +
+// last-arriver upper levels, for raw leaves, prehashed digests, QM31 layers and
+// fold-then-hash layers (reference: MerkleCommitter.swift:526-1063 and the Metal
+// kernels HashMerkleKernels.metal:1064-1292; oracle MerkleOracle.swift:4-141).
+//
+// Tree layout: level 0 (leaf digests) optional; levels >= 1 in `inner`, level l
+// at inner_offset(logn, l), root last.  A digest is 4 little-endian u64 lanes.
+//
+// Upper levels need no grid-wide wait: each CTA that completes a treelet root
+// bumps its group's arrival counter; the CTA that arrives last reads the group's
+// roots (written by the others before their fence + atomic) and reduces them.
+// Counters reset themselves, so the same job list can be relaunched (and
+// captured in a CUDA graph).
+#include "azk_field.cuh"
+#include "azk_internal.h"
+#include "azk_message.cuh"
+
+namespace azk {
+
+struct Dig {
+  uint64_t w[4];
+};
+
+__device__ __forceinline__ void st_dig(uint64_t* p, const uint64_t (&d)[4]) {
+  reinterpret_cast<ulonglong2*>(p)[0] = make_ulonglong2(d[0], d[1]);
+  reinterpret_cast<ulonglong2*>(p)[1] = make_ulonglong2(d[2], d[3]);
+}
+__device__ __forceinline__ void ld_dig(const uint64_t* p, uint64_t (&d)[4]) {
+  ulonglong2 a = reinterpret_cast<const ulonglong2*>(p)[0], b = reinterpret_cast<const ulonglong2*>(p)[1];
+  d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
+}
+// L2 read of a digest written by another CTA in this launch.
+__device__ __forceinline__ void ld_dig_cg(const uint64_t* p, uint64_t (&d)[4]) {
+  ulonglong2 a = __ldcg(reinterpret_cast<const ulonglong2*>(p));
+  ulonglong2 b = __ldcg(reinterpret_cast<const ulonglong2*>(p) + 1);
+  d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
+}
+
+template <uint32_t KIND>
+__device__ __forceinline__ void leaf_digest(const TreeJob& job, uint64_t leaf, const uint32_t (&ch)[4], uint64_t (&d)[4]) {
+  if constexpr (KIND == kLeafQM31) {
+    uint4 v = __ldg(job.layer + leaf);
+    sha3_16((uint64_t)v.x | ((uint64_t)v.y << 32), (uint64_t)v.z | ((uint64_t)v.w << 32), d);
+  } else if constexpr (KIND == kLeafFold) {
+    uint4 p = __ldg(job.layer + 2 * leaf), q = __ldg(job.layer + 2 * leaf + 1);
+    uint32_t t = __ldg(job.inv + leaf);
+    qm31 r = fri_fold_pair(qm31{p.x, p.y, p.z, p.w}, qm31{q.x, q.y, q.z, q.w}, t, qm31{ch[0], ch[1], ch[2], ch[3]});
+    job.out_layer[leaf] = make_uint4(r.a, r.b, r.c, r.d);
+    sha3_16((uint64_t)r.a | ((uint64_t)r.b << 32), (uint64_t)r.c | ((uint64_t)r.d << 32), d);
+  } else if constexpr (KIND == kLeafDigest) {
+    ld_dig(reinterpret_cast<const uint64_t*>(job.raw) + 4 * leaf, d);
+  } else {
+    hash_message(job.raw + leaf * job.stride, job.len, job.suffix, job.aligned8 != 0, d);
+  }
+}
+
+// Reduce `count` digests in buffer a (scratch b holds count/2) level by level,
+// storing each level into the job's inner nodes.  Returns the buffer holding the
+// single remaining digest.  `level`/`idx0`: level and first node index of the
+// input digests.
+__device__ uint64_t* reduce_levels(uint64_t* a, uint64_t* b, uint32_t count, const TreeJob& job, uint32_t level, uint64_t idx0) {
+  uint64_t* src = a;
+  uint64_t* dst = b;
+  while (count > 1) {
+    count >>= 1;
+    idx0 >>= 1;
+    level++;
+    uint64_t* lv = job.inner + 4 * (inner_offset(job.logn, level) + idx0);
+    for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
+      uint64_t l[4], r[4], d[4];
+      ld_dig(src + 8 * i, l);
+      ld_dig(src + 8 * i + 4, r);
+      sha3_pair(l, r, d);
+      st_dig(dst + 4 * i, d);
+      st_dig(lv + 4 * i, d);
+    }
+    __syncthreads();
+    uint64_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+__device__ void root_action(const TreeJob& job, const uint64_t* rootp) {
+  uint64_t root[4];
+  ld_dig(rootp, root);
+  if (job.root_out) st_dig(job.root_out, root);
+  if (job.root_action == kRootNone) return;
+  Transcript t = *job.transcript;
+  uint32_t ch[4];
+  if (job.root_action == kRootCircleRound)
+    circle_round(t, job.round, root, ch);
+  else
+    qm31_round(t, job.round, job.frame_in_count, root, ch);
+  *job.transcript = t;
+  for (int k = 0; k < 4; k++) job.challenge_out[k] = ch[k];
+}
+
+template <uint32_t KIND, int THREADS>
+__global__ void __launch_bounds__(THREADS) tree_tiles_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  __shared__ uint32_t s_last;
+  __shared__ uint32_t s_ch[4];
+  const uint2 w = work[blockIdx.x];
+  const TreeJob& job = jobs[w.x];
+  const uint32_t tl = job.tile_log < job.logn ? job.tile_log : job.logn;
+  const uint32_t T = 1u << tl;
+  uint64_t* bufA = sm;           // T digests
+  uint64_t* bufB = sm + 4 * T;   // T/2 digests
+  const uint64_t tile = w.y;
+
+  uint32_t ch[4] = {0, 0, 0, 0};
+  if constexpr (KIND == kLeafFold) {
+    if (threadIdx.x < 4) s_ch[threadIdx.x] = __ldcg(job.fold_ch + threadIdx.x);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; k++) ch[k] = s_ch[k];
+  }
+
+  // 1) leaf digests of this tile
+  for (uint32_t i = threadIdx.x; i < T; i += THREADS) {
+    uint64_t leaf = tile * T + i;
+    uint64_t d[4];
+    leaf_digest<KIND>(job, leaf, ch, d);
+    st_dig(bufA + 4 * i, d);
+    if (job.leaf_digests) st_dig(job.leaf_digests + 4 * leaf, d);
+  }
+  __syncthreads();
+  // 2) treelet
+  uint64_t* res = reduce_levels(bufA, bufB, T, job, 0, tile * T);
+  // 3) climb: last arriver of each group continues
+  uint32_t level = tl;
+  uint64_t idx = tile;
+  uint64_t cnt_off = 0;
+  while (level < job.logn) {
+    uint32_t glog = job.group_log;
+    if (glog > job.logn - level) glog = job.logn - level;
+    if (glog > tl) glog = tl;  // the group must fit the shared buffers (host keeps tl >= 1)
+    const uint32_t G = 1u << glog;
+    const uint64_t gidx = idx >> glog;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      uint32_t old = atomicAdd(job.counters + cnt_off + gidx, 1u);
+      s_last = (old == G - 1) ? 1u : 0u;
+      if (s_last) job.counters[cnt_off + gidx] = 0;  // reset for the next launch
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const uint64_t* lv = job.inner + 4 * (inner_offset(job.logn, level) + gidx * G);
+    for (uint32_t i = threadIdx.x; i < G; i += THREADS) {
+      uint64_t d[4];
+      ld_dig_cg(lv + 4 * i, d);
+      st_dig(bufA + 4 * i, d);
+    }
+    __syncthreads();
+    res = reduce_levels(bufA, bufB, G, job, level, gidx * G);
+    cnt_off += (1ull << (job.logn - level)) >> glog;
+    level += glog;
+    idx = gidx;
+  }
+  if (threadIdx.x == 0) root_action(job, res);
+}
+
+static constexpr int kMaxTreeSmem = 48 << 11;  // 2^11 digests + 2^10 digests
+
+template <uint32_t KIND>
+static cudaError_t prepare_kind() {
+  cudaError_t e = cudaSuccess;
+  for (auto k : {tree_tiles_kernel<KIND, 128>, tree_tiles_kernel<KIND, 256>, tree_tiles_kernel<KIND, 512>}) {
+    cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTreeSmem);
+    if (r != cudaSuccess) e = r;
+  }
+  return e;
+}
+
+// Opt the tree kernels into > 48 KiB of dynamic shared memory once, outside any
+// stream capture.
+cudaError_t prepare_tree_kernels() {
+  cudaError_t e = prepare_kind<kLeafRaw>();
+  if (e == cudaSuccess) e = prepare_kind<kLeafQM31>();
+  if (e == cudaSuccess) e = prepare_kind<kLeafFold>();
+  if (e == cudaSuccess) e = prepare_kind<kLeafDigest>();
+  return e;
+}
+
+template <uint32_t KIND>
+static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t threads, cudaStream_t s) {
+  size_t smem = (size_t)48 << max_tile_log;  // T digests + T/2 digests
+  if (threads == 128)
+    tree_tiles_kernel<KIND, 128><<<nwork, 128, smem, s>>>(d_jobs, d_work);
+  else if (threads == 512)
+    tree_tiles_kernel<KIND, 512><<<nwork, 512, smem, s>>>(d_jobs, d_work);
+  else
+    tree_tiles_kernel<KIND, 256><<<nwork, 256, smem, s>>>(d_jobs, d_work);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t kind, uint32_t threads,
+                             cudaStream_t s) {
+  if (nwork == 0) return cudaSuccess;
+  if (max_tile_log > 11) return cudaErrorInvalidValue;
+  switch (kind) {
+    case kLeafRaw: return launch_kind<kLeafRaw>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafQM31: return launch_kind<kLeafQM31>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafFold: return launch_kind<kLeafFold>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafDigest: return launch_kind<kLeafDigest>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Sibling paths for leaves of a committed tree: out[k][level] = digest of the
+// sibling at `level` (bottom-up), depth = job.logn digests per index.  Level 0
+// comes from stored leaf digests, or is recomputed from the leaf source.
+__global__ void gather_openings_kernel(const TreeJob* __restrict__ jobp, const uint64_t* __restrict__ idx, uint32_t nidx, uint64_t* __restrict__ out) {
+  const TreeJob& job = *jobp;
+  uint32_t depth = job.logn;
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)nidx * depth) return;
+  uint32_t k = (uint32_t)(t / depth), level = (uint32_t)(t % depth);
+  uint64_t leaf = idx[k];
+  uint64_t node = (leaf >> level) ^ 1ull;
+  uint64_t d[4];
+  if (level == 0) {
+    if (job.leaf_digests) {
+      ld_dig(job.leaf_digests + 4 * node, d);
+    } else {
+      uint32_t ch[4] = {0, 0, 0, 0};
+      if (job.kind == kLeafQM31)
+        leaf_digest<kLeafQM31>(job, node, ch, d);
+      else if (job.kind == kLeafDigest)
+        leaf_digest<kLeafDigest>(job, node, ch, d);
+      else
+        leaf_digest<kLeafRaw>(job, node, ch, d);
+    }
+  } else {
+    ld_dig(job.inner + 4 * (inner_offset(job.logn, level) + node), d);
+  }
+  st_dig(out + 4 * ((uint64_t)k * depth + level), d);
+}
+
+cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, uint32_t nidx, uint64_t* d_out, cudaStream_t s) {
+  // depth is read on the device; launch enough threads for the deepest tree (31 levels)
+  uint64_t total = (uint64_t)nidx * 32;
+  if (total == 0) return cudaSuccess;
+  gather_openings_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_job, d_idx, nidx, d_out);
+  return cudaGetLastError();
+}
+
+}  // namespace azk

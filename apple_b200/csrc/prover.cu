@@ -1,0 +1,610 @@
+// Circle PCS/FRI proving engine: FFT -> per-round (fold + leaf hash + treelet +
+// upper tree + transcript) -> final fold -> final-layer binding -> queries ->
+// proof bytes, for one instance (azk_pcs_prover, mirroring
+// CirclePCSFRIResidentProverV1 / CircleCodewordPCSFRIProverV1) or many uneven
+// instances at once (azk_batch).
+//
+// Batched form: each stage is one launch over the work items of every instance
+// still active in that round, so small instances share the GPU with large ones
+// and the whole superstep is a fixed launch sequence captured in a CUDA graph.
+// Plain form: the same kernels, launched instance after instance.
+#include <algorithm>
+
+#include "azk_field.cuh"
+#include "azk_runtime.h"
+
+using namespace azk;
+
+namespace {
+
+struct InstanceCfg {
+  uint32_t logn, rounds, queries, log_blowup, grinding;
+  std::vector<uint64_t> claimed;
+};
+
+struct Engine {
+  azk_ctx* ctx = nullptr;
+  cudaStream_t s = nullptr;
+  Sched sched;
+  std::vector<InstanceCfg> cfg;
+  uint32_t rmax = 0, qmax = 0;
+  bool any_grinding = false;
+
+  Arena arena;
+  std::vector<uint64_t> off_input, off_layers, off_trees, off_tr, off_ch, off_cm, off_qp, off_claim, off_proof, off_cnt;
+  std::vector<uint64_t> proof_len, proof_off;
+  uint64_t proof_total = 0;
+  uint64_t off_inst = 0, off_flag = 0;
+
+  std::vector<PcsInstance> h_inst;
+  // FFT
+  FftPlan fft;
+  // rounds: tree step k (kind QM31 at k == 0, fold+hash after), final folds at step k
+  std::vector<TreeJob> tree_jobs;
+  std::vector<uint2> tree_work;
+  std::vector<uint64_t> tstep_off, tstep_cnt;
+  std::vector<std::vector<std::pair<uint64_t, uint64_t>>> tstep_inst;  // [step][inst]
+  std::vector<uint32_t> tstep_tile;                                     // max tile log per step
+  std::vector<FoldJob> fold_jobs;
+  std::vector<uint2> fold_work;
+  std::vector<uint64_t> fstep_off, fstep_cnt;
+  std::vector<std::vector<std::pair<uint64_t, uint64_t>>> fstep_inst;
+  std::vector<uint32_t> ids;
+  DevBuf d_tree_jobs, d_tree_work, d_fold_jobs, d_fold_work, d_ids;
+
+  cudaGraphExec_t graph = nullptr;
+  bool graph_from_coeffs = false;
+
+  ~Engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  PcsInstance* d_inst() const { return arena.at<PcsInstance>(off_inst); }
+  uint32_t* d_flag() const { return arena.at<uint32_t>(off_flag); }
+
+  void init(azk_ctx* c, const std::vector<InstanceCfg>& cf, const Sched& sc) {
+    ctx = c;
+    sched = sc;
+    cfg = cf;
+    AZK_CU(cudaSetDevice(ctx->device));
+    AZK_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    size_t n = cfg.size();
+    for (auto& i : cfg) {
+      rmax = std::max(rmax, i.rounds);
+      qmax = std::max(qmax, i.queries);
+      any_grinding |= i.grinding > 0;
+    }
+    // ---- memory plan ----
+    auto resz = [&](std::vector<uint64_t>& v) { v.assign(n, 0); };
+    for (auto* v : {&off_input, &off_layers, &off_trees, &off_tr, &off_ch, &off_cm, &off_qp, &off_claim, &off_proof, &off_cnt}) resz(*v);
+    proof_len.assign(n, 0);
+    proof_off.assign(n, 0);
+    for (size_t i = 0; i < n; i++) {
+      const auto& c2 = cfg[i];
+      uint64_t N = 1ull << c2.logn;
+      off_input[i] = arena.reserve(16 * N);
+      off_layers[i] = arena.reserve(16 * 2 * N);
+      off_trees[i] = arena.reserve(32 * 2 * N);
+      off_tr[i] = arena.reserve(sizeof(Transcript));
+      off_ch[i] = arena.reserve(16ull * c2.rounds);
+      off_cm[i] = arena.reserve(32ull * c2.rounds);
+      off_qp[i] = arena.reserve(4ull * c2.queries);
+      off_claim[i] = arena.reserve(8ull * c2.claimed.size());
+      off_cnt[i] = arena.reserve(4 * tree_counter_count(c2.logn, 1));
+      proof_len[i] = proof_total_bytes(c2.logn, c2.rounds, c2.queries, (uint32_t)c2.claimed.size(), c2.grinding > 0);
+    }
+    uint64_t pbase = arena.reserve(0);
+    arena.used = pbase;
+    for (size_t i = 0; i < n; i++) {
+      proof_off[i] = proof_total;
+      proof_total += align_up(proof_len[i], 16);
+    }
+    uint64_t off_proofs = arena.reserve(proof_total);
+    for (size_t i = 0; i < n; i++) off_proof[i] = off_proofs + proof_off[i];
+    off_inst = arena.reserve(sizeof(PcsInstance) * n);
+    off_flag = arena.reserve(16);
+    arena.commit("PCS.Arena");
+    // counters and inputs start at zero
+    AZK_CU(cudaMemsetAsync(arena.buf.p, 0, arena.used, s));
+
+    // ---- instance table ----
+    h_inst.resize(n);
+    for (size_t i = 0; i < n; i++) {
+      const auto& c2 = cfg[i];
+      const auto& dom = domain_tables(ctx, c2.logn);
+      PcsInstance& I = h_inst[i];
+      I = PcsInstance{};
+      I.logn = c2.logn;
+      I.rounds = c2.rounds;
+      I.queries = c2.queries;
+      I.log_blowup = c2.log_blowup;
+      I.grinding_bits = c2.grinding;
+      I.n_claimed = (uint32_t)c2.claimed.size();
+      I.layers = arena.at<uint4>(off_layers[i]);
+      I.trees = arena.at<uint64_t>(off_trees[i]);
+      I.tw = dom.tw;
+      I.inv = dom.inv;
+      I.transcript = arena.at<Transcript>(off_tr[i]);
+      I.challenges = arena.at<uint32_t>(off_ch[i]);
+      I.commitments = arena.at<uint64_t>(off_cm[i]);
+      I.query_pairs = arena.at<uint32_t>(off_qp[i]);
+      I.claimed = arena.at<uint64_t>(off_claim[i]);
+      I.proof = arena.at<uint8_t>(off_proof[i]);
+      I.proof_len = proof_len[i];
+      if (!c2.claimed.empty())
+        AZK_CU(cudaMemcpyAsync(arena.at<uint64_t>(off_claim[i]), c2.claimed.data(), 8 * c2.claimed.size(), cudaMemcpyHostToDevice, s));
+    }
+    AZK_CU(cudaMemcpyAsync(d_inst(), h_inst.data(), sizeof(PcsInstance) * n, cudaMemcpyHostToDevice, s));
+    ids.resize(n);
+    for (size_t i = 0; i < n; i++) ids[i] = (uint32_t)i;
+    d_ids.alloc(4 * n, "PCS.Ids");
+    AZK_CU(cudaMemcpyAsync(d_ids.p, ids.data(), 4 * n, cudaMemcpyHostToDevice, s));
+
+    // ---- FFT ----
+    std::vector<FftJob> tf;
+    for (size_t i = 0; i < n; i++)
+      tf.push_back(FftJob{cfg[i].logn, 0, arena.at<uint4>(off_input[i]), arena.at<uint4>(off_layers[i]), h_inst[i].tw});
+    fft.build(tf);
+    fft.upload(s);
+
+    // ---- rounds ----
+    tstep_off.assign(rmax, 0);
+    tstep_cnt.assign(rmax, 0);
+    tstep_tile.assign(rmax, 1);
+    tstep_inst.assign(rmax, std::vector<std::pair<uint64_t, uint64_t>>(n, {0, 0}));
+    fstep_off.assign(rmax + 1, 0);
+    fstep_cnt.assign(rmax + 1, 0);
+    fstep_inst.assign(rmax + 1, std::vector<std::pair<uint64_t, uint64_t>>(n, {0, 0}));
+    // large instances first inside a step, so their upper-tree tails overlap the rest
+    std::vector<uint32_t> order(n);
+    for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cfg[a].logn > cfg[b].logn; });
+    for (uint32_t k = 0; k < rmax; k++) {
+      tstep_off[k] = tree_work.size();
+      for (uint32_t i : order) {
+        const auto& c2 = cfg[i];
+        if (k >= c2.rounds) continue;
+        const PcsInstance& I = h_inst[i];
+        uint32_t lg = c2.logn - k;
+        uint32_t tl = tree_tile_log(sched, lg);
+        if (tl == 0 && lg > 0) tl = 1;
+        TreeJob j{};
+        j.logn = lg;
+        j.kind = k == 0 ? kLeafQM31 : kLeafFold;
+        j.tile_log = tl;
+        j.group_log = std::max<uint32_t>(1, std::min(sched.group_log, tl));
+        if (k == 0) {
+          j.layer = I.layers;
+        } else {
+          j.layer = I.layers + layer_offset(c2.logn, k - 1);
+          j.inv = I.inv + (k - 1 == 0 ? 0 : (1ull << c2.logn) - ((1ull << c2.logn) >> (k - 1)));
+          j.fold_ch = I.challenges + 4 * (k - 1);
+          j.out_layer = I.layers + layer_offset(c2.logn, k);
+        }
+        j.inner = I.trees + 4 * tree_offset(c2.logn, k);
+        j.counters = arena.at<uint32_t>(off_cnt[i]);
+        j.root_action = kRootCircleRound;
+        j.round = k;
+        j.transcript = I.transcript;
+        j.challenge_out = I.challenges + 4 * k;
+        j.root_out = I.commitments + 4 * k;
+        uint32_t jid = (uint32_t)tree_jobs.size();
+        tree_jobs.push_back(j);
+        uint64_t tiles = 1ull << (lg - tl);
+        tstep_inst[k][i] = {tree_work.size(), tiles};
+        for (uint64_t t = 0; t < tiles; t++) tree_work.push_back(make_uint2(jid, (uint32_t)t));
+        tstep_tile[k] = std::max(tstep_tile[k], tl);
+      }
+      tstep_cnt[k] = tree_work.size() - tstep_off[k];
+    }
+    for (uint32_t k = 1; k <= rmax; k++) {
+      fstep_off[k] = fold_work.size();
+      for (uint32_t i : order) {
+        const auto& c2 = cfg[i];
+        if (c2.rounds != k) continue;
+        const PcsInstance& I = h_inst[i];
+        uint64_t N = 1ull << c2.logn;
+        FoldJob f{N >> k, I.layers + layer_offset(c2.logn, k - 1), I.inv + (k - 1 == 0 ? 0 : N - (N >> (k - 1))), I.challenges + 4 * (k - 1),
+                  I.layers + layer_offset(c2.logn, k)};
+        uint32_t fid = (uint32_t)fold_jobs.size();
+        fold_jobs.push_back(f);
+        uint64_t chunks = (f.n_out + kFoldChunk - 1) / kFoldChunk;
+        fstep_inst[k][i] = {fold_work.size(), chunks};
+        for (uint64_t c3 = 0; c3 < chunks; c3++) fold_work.push_back(make_uint2(fid, (uint32_t)c3));
+      }
+      fstep_cnt[k] = fold_work.size() - fstep_off[k];
+    }
+    auto up = [&](DevBuf& d, const void* src, size_t bytes, const char* label) {
+      d.alloc(std::max<size_t>(bytes, 16), label);
+      if (bytes) AZK_CU(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, s));
+    };
+    up(d_tree_jobs, tree_jobs.data(), tree_jobs.size() * sizeof(TreeJob), "PCS.TreeJobs");
+    up(d_tree_work, tree_work.data(), tree_work.size() * sizeof(uint2), "PCS.TreeWork");
+    up(d_fold_jobs, fold_jobs.data(), fold_jobs.size() * sizeof(FoldJob), "PCS.FoldJobs");
+    up(d_fold_work, fold_work.data(), fold_work.size() * sizeof(uint2), "PCS.FoldWork");
+    AZK_CU(cudaStreamSynchronize(s));
+  }
+
+  void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt) {
+    if (!cnt) return;
+    AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], k == 0 ? kLeafQM31 : kLeafFold,
+                            sched.threads, s));
+  }
+  void launch_fold_range(uint64_t off, uint64_t cnt) {
+    if (!cnt) return;
+    AZK_CU(launch_fold_jobs(d_fold_jobs.as<FoldJob>(), d_fold_work.as<uint2>() + off, (uint32_t)cnt, s));
+  }
+
+  // Everything up to (not including) grinding.  from_coeffs: run the FFT first.
+  void enqueue_rounds_batched(bool from_coeffs) {
+    if (from_coeffs) fft.launch_all(s);
+    AZK_CU(launch_pcs_prefix(d_inst(), (uint32_t)cfg.size(), s));
+    for (uint32_t k = 0; k <= rmax; k++) {
+      if (k < rmax) launch_tree_range(k, tstep_off[k], tstep_cnt[k]);
+      if (k >= 1) launch_fold_range(fstep_off[k], fstep_cnt[k]);
+    }
+    AZK_CU(launch_pcs_finalize(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
+  }
+  void enqueue_tail_batched() {
+    AZK_CU(launch_pcs_queries(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
+    AZK_CU(launch_pcs_emit(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), qmax, s));
+  }
+  void enqueue_instance(uint32_t i, bool from_coeffs) {
+    if (from_coeffs)
+      for (size_t st = 0; st < fft.step_cnt.size(); st++)
+        if (fft.inst_range[st][i].second) fft.launch_step_for(st, i, s);
+    AZK_CU(launch_pcs_prefix(d_inst() + i, 1, s));
+    const uint32_t* id = d_ids.as<uint32_t>() + i;
+    for (uint32_t k = 0; k <= cfg[i].rounds; k++) {
+      if (k < cfg[i].rounds) launch_tree_range(k, tstep_inst[k][i].first, tstep_inst[k][i].second);
+      if (k == cfg[i].rounds) launch_fold_range(fstep_inst[k][i].first, fstep_inst[k][i].second);
+    }
+    AZK_CU(launch_pcs_finalize(d_inst(), id, 1, s));
+    grind_instance(i);
+    AZK_CU(launch_pcs_queries(d_inst(), id, 1, s));
+    AZK_CU(launch_pcs_emit(d_inst(), id, 1, cfg[i].queries, s));
+  }
+
+  // Smallest nonce meeting the grinding target (CircleProofFormat.swift:753-794),
+  // searched in increasing chunks on the device.
+  void grind_instance(uint32_t i) {
+    if (!cfg[i].grinding) return;
+    DevBuf found(8, "PCS.GrindingNonce");
+    uint64_t chunk = 1ull << std::min<uint32_t>(cfg[i].grinding + 4, 26);
+    for (uint64_t start = 0;; start += chunk) {
+      AZK_CU(cudaMemsetAsync(found.p, 0xFF, 8, s));
+      AZK_CU(launch_pcs_grind(d_inst(), i, start, chunk, found.as<unsigned long long>(), s));
+      uint64_t nonce = ~0ull;
+      AZK_CU(cudaMemcpyAsync(&nonce, found.p, 8, cudaMemcpyDeviceToHost, s));
+      AZK_CU(cudaStreamSynchronize(s));
+      if (nonce != ~0ull) {
+        h_inst[i].nonce = nonce;
+        h_inst[i].has_nonce = 1;
+        AZK_CU(cudaMemcpyAsync(&d_inst()[i].nonce, &h_inst[i].nonce, 8, cudaMemcpyHostToDevice, s));
+        AZK_CU(cudaMemcpyAsync(&d_inst()[i].has_nonce, &h_inst[i].has_nonce, 4, cudaMemcpyHostToDevice, s));
+        return;
+      }
+      require(start < (1ull << 40), AZK_ERR_COMMAND_EXECUTION_FAILED, "grinding nonce search exhausted");
+    }
+  }
+
+  void set_publics(const uint8_t* pubs) {
+    for (size_t i = 0; i < cfg.size(); i++) std::memcpy(h_inst[i].pub, pubs + 32 * i, 32);
+    AZK_CU(cudaMemcpy2DAsync(reinterpret_cast<uint8_t*>(d_inst()) + offsetof(PcsInstance, pub), sizeof(PcsInstance), pubs, 32, 32, cfg.size(),
+                             cudaMemcpyHostToDevice, s));
+  }
+
+  // Run the whole superstep; returns device seconds.
+  double run(bool from_coeffs, bool plain, uint64_t* submit_ns, const Timer& t) {
+    AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
+    GpuTimer g(s);
+    if (plain) {
+      for (uint32_t i = 0; i < cfg.size(); i++) enqueue_instance(i, from_coeffs);
+    } else if (!any_grinding && sched.graph) {
+      if (!graph || graph_from_coeffs != from_coeffs) {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        cudaGraph_t gr;
+        AZK_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_rounds_batched(from_coeffs);
+        enqueue_tail_batched();
+        AZK_CU(cudaStreamEndCapture(s, &gr));
+        AZK_CU(cudaGraphInstantiate(&graph, gr, 0));
+        cudaGraphDestroy(gr);
+        graph_from_coeffs = from_coeffs;
+      }
+      AZK_CU(cudaGraphLaunch(graph, s));
+    } else {
+      enqueue_rounds_batched(from_coeffs);
+      for (uint32_t i = 0; i < cfg.size(); i++) grind_instance(i);
+      enqueue_tail_batched();
+    }
+    if (submit_ns) *submit_ns = t.ns();
+    g.stop();
+    return g.seconds();
+  }
+
+  // Reject non-canonical inputs (QM31CanonicalityCheck.swift): checked on the
+  // device before the proof is trusted.
+  void check_input_canonical(const void* dptr, uint64_t words) {
+    AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
+    AZK_CU(launch_check_canonical(static_cast<const uint32_t*>(dptr), words, d_flag(), s));
+    uint32_t f = 0;
+    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaStreamSynchronize(s));
+    layout(f == 0, "input contains a non-canonical field element");
+  }
+
+  void trace(uint32_t i, uint8_t* cm, uint32_t* ch, uint32_t* fl, uint32_t* qp) {
+    const auto& c2 = cfg[i];
+    if (cm) AZK_CU(cudaMemcpyAsync(cm, arena.at<uint8_t>(off_cm[i]), 32ull * c2.rounds, cudaMemcpyDeviceToHost, s));
+    if (ch) AZK_CU(cudaMemcpyAsync(ch, arena.at<uint8_t>(off_ch[i]), 16ull * c2.rounds, cudaMemcpyDeviceToHost, s));
+    if (fl)
+      AZK_CU(cudaMemcpyAsync(fl, h_inst[i].layers + layer_offset(c2.logn, c2.rounds), 16ull << (c2.logn - c2.rounds), cudaMemcpyDeviceToHost, s));
+    if (qp) AZK_CU(cudaMemcpyAsync(qp, arena.at<uint8_t>(off_qp[i]), 4ull * c2.queries, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaStreamSynchronize(s));
+  }
+};
+
+void validate_params(uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t grinding, uint32_t rounds) {
+  // CircleFRISecurityParametersV1.init (CircleProofFormat.swift:136-151) and
+  // CircleFRIProofBuilderV1.prove (CircleProofFormat.swift:1181-1189)
+  layout(logn >= 1 && logn <= 26);
+  layout(log_blowup > 0 && queries > 0 && grinding <= 20);
+  layout((uint64_t)log_blowup * queries + grinding <= 0xFFFFFFFFull);
+  layout(rounds >= 1 && rounds <= logn);
+}
+
+}  // namespace
+
+struct azk_pcs_prover {
+  azk_ctx* ctx;
+  std::mutex mu;
+  Engine eng;
+  uint32_t logn, rounds, queries, log_blowup, grinding;
+};
+
+struct azk_batch {
+  azk_ctx* ctx;
+  std::mutex mu;
+  Engine eng;
+};
+
+extern "C" {
+
+uint64_t azk_pcs_proof_size(uint32_t logn, uint32_t rounds, uint32_t queries, uint32_t claimed, uint32_t grinding) {
+  if (logn < 1 || logn > 30 || rounds < 1 || rounds > logn) return 0;
+  return proof_total_bytes(logn, rounds, queries, claimed, grinding > 0);
+}
+
+azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t grinding, uint32_t rounds,
+                                 const azk_schedule* schedule, azk_pcs_prover** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out);
+    validate_params(logn, log_blowup, queries, grinding, rounds);
+    auto p = std::make_unique<azk_pcs_prover>();
+    p->ctx = ctx;
+    p->logn = logn;
+    p->rounds = rounds;
+    p->queries = queries;
+    p->log_blowup = log_blowup;
+    p->grinding = grinding;
+    Sched sc = resolve_schedule(schedule);
+    sc.graph = false;
+    p->eng.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
+    *out = p.release();
+  });
+}
+
+// Claimed openings change the proof layout: rebuild the engine for a new set
+// before any input is staged into it.
+static void pcs_ensure_claimed(azk_pcs_prover* p, const std::vector<uint64_t>& claimed) {
+  Engine& e = p->eng;
+  if (claimed == e.cfg[0].claimed) return;
+  Sched sc = e.sched;
+  e.~Engine();
+  new (&e) Engine();
+  e.init(p->ctx, {InstanceCfg{p->logn, p->rounds, p->queries, p->log_blowup, p->grinding, claimed}}, sc);
+}
+
+static void pcs_prove_common(azk_pcs_prover* p, bool coeffs, const uint8_t pub[32], uint8_t* proof_out, bool proof_on_device, uint64_t* proof_len,
+                             azk_stats* st, const Timer& t) {
+  Engine& e = p->eng;
+  e.set_publics(pub);
+  uint64_t sub = 0;
+  double gs = e.run(coeffs, true, &sub, t);
+  uint64_t len = e.proof_len[0];
+  layout(*proof_len >= len, "proof buffer too small");
+  *proof_len = len;
+  if (proof_on_device)
+    AZK_CU(cudaMemcpyAsync(proof_out, e.h_inst[0].proof, len, cudaMemcpyDeviceToDevice, e.s));
+  else
+    AZK_CU(cudaMemcpyAsync(proof_out, e.h_inst[0].proof, len, cudaMemcpyDeviceToHost, e.s));
+  AZK_CU(cudaStreamSynchronize(e.s));
+  fill_stats(st, t, sub, gs);
+}
+
+azk_status azk_pcs_prover_prove_evaluations(azk_pcs_prover* p, const uint32_t* ev, const uint8_t pub[32], const uint64_t* claimed, uint64_t nclaimed,
+                                            uint8_t* proof_out, uint64_t* proof_len, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && ev && pub && proof_out && proof_len && (claimed || !nclaimed));
+    std::lock_guard<std::mutex> lk(p->mu);
+    uint64_t N = 1ull << p->logn;
+    std::vector<uint64_t> cl(claimed, claimed + nclaimed);
+    std::sort(cl.begin(), cl.end());
+    for (size_t i = 0; i < cl.size(); i++) layout(cl[i] < N && (i == 0 || cl[i - 1] < cl[i]));
+    Timer t;
+    pcs_ensure_claimed(p, cl);
+    Engine& e = p->eng;
+    // evaluations go straight into layer 0
+    AZK_CU(cudaMemcpyAsync(e.h_inst[0].layers, ev, 16 * N, cudaMemcpyHostToDevice, e.s));
+    e.check_input_canonical(e.h_inst[0].layers, 4 * N);
+    pcs_prove_common(p, false, pub, proof_out, false, proof_len, st, t);
+  });
+}
+
+azk_status azk_pcs_prover_prove_coefficients(azk_pcs_prover* p, const uint32_t* coeffs, uint64_t count, const uint8_t pub[32], uint8_t* proof_out,
+                                             uint64_t* proof_len, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && coeffs && pub && proof_out && proof_len);
+    std::lock_guard<std::mutex> lk(p->mu);
+    uint64_t N = 1ull << p->logn;
+    layout(count >= 1 && count <= N);
+    Timer t;
+    pcs_ensure_claimed(p, {});
+    Engine& e = p->eng;
+    uint4* in = e.arena.at<uint4>(e.off_input[0]);
+    AZK_CU(cudaMemcpyAsync(in, coeffs, 16 * count, cudaMemcpyHostToDevice, e.s));
+    if (count < N) AZK_CU(cudaMemsetAsync(in + count, 0, 16 * (N - count), e.s));
+    e.check_input_canonical(in, 4 * count);
+    pcs_prove_common(p, true, pub, proof_out, false, proof_len, st, t);
+  });
+}
+
+azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* din, uint64_t in_off, int is_coeffs, const uint8_t pub[32], void* dproof,
+                                         uint64_t* proof_len, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && din && pub && dproof && proof_len && in_off % 16 == 0);
+    std::lock_guard<std::mutex> lk(p->mu);
+    uint64_t N = 1ull << p->logn;
+    Timer t;
+    pcs_ensure_claimed(p, {});
+    Engine& e = p->eng;
+    const uint8_t* src = static_cast<const uint8_t*>(din) + in_off;
+    e.check_input_canonical(src, 4 * N);
+    void* dst = is_coeffs ? (void*)e.arena.at<uint4>(e.off_input[0]) : (void*)e.h_inst[0].layers;
+    AZK_CU(cudaMemcpyAsync(dst, src, 16 * N, cudaMemcpyDeviceToDevice, e.s));
+    pcs_prove_common(p, is_coeffs != 0, pub, static_cast<uint8_t*>(dproof), true, proof_len, st, t);
+  });
+}
+
+azk_status azk_pcs_prover_trace(azk_pcs_prover* p, uint8_t* cm, uint32_t* ch, uint32_t* fl, uint32_t* qp) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    std::lock_guard<std::mutex> lk(p->mu);
+    p->eng.trace(0, cm, ch, fl, qp);
+  });
+}
+
+void azk_pcs_prover_destroy(azk_pcs_prover* p) { delete p; }
+
+azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint32_t* ev, uint32_t log_blowup, uint32_t queries, uint32_t grinding,
+                                        const uint8_t pub[32], uint32_t rounds, uint32_t* final_out, uint8_t* cm_out, uint32_t* ch_out, azk_stats* st) {
+  return guarded(ctx, [&] {
+    layout(ctx && ev && pub && final_out);
+    validate_params(logn, log_blowup, queries, grinding, rounds);
+    uint64_t N = 1ull << logn;
+    Timer t;
+    Engine e;
+    Sched sc;
+    sc.graph = false;
+    e.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
+    AZK_CU(cudaMemcpyAsync(e.h_inst[0].layers, ev, 16 * N, cudaMemcpyHostToDevice, e.s));
+    e.check_input_canonical(e.h_inst[0].layers, 4 * N);
+    e.set_publics(pub);
+    GpuTimer g(e.s);
+    AZK_CU(launch_pcs_prefix(e.d_inst(), 1, e.s));
+    for (uint32_t k = 0; k <= rounds; k++) {
+      if (k < rounds) e.launch_tree_range(k, e.tstep_inst[k][0].first, e.tstep_inst[k][0].second);
+      if (k == rounds) e.launch_fold_range(e.fstep_inst[k][0].first, e.fstep_inst[k][0].second);
+    }
+    g.stop();
+    double gs = g.seconds();
+    e.trace(0, cm_out, ch_out, final_out, nullptr);
+    fill_stats(st, t, 0, gs);
+  });
+}
+
+// ---- batch ----
+azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* logs, const uint32_t* rounds, uint32_t log_blowup, uint32_t queries,
+                            const azk_schedule* schedule, azk_batch** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && logs && rounds && count >= 1);
+    std::vector<InstanceCfg> cf;
+    for (uint32_t i = 0; i < count; i++) {
+      validate_params(logs[i], log_blowup, queries, 0, rounds[i]);
+      cf.push_back(InstanceCfg{logs[i], rounds[i], queries, log_blowup, 0, {}});
+    }
+    auto b = std::make_unique<azk_batch>();
+    b->ctx = ctx;
+    b->eng.init(ctx, cf, resolve_schedule(schedule));
+    *out = b.release();
+  });
+}
+
+azk_status azk_batch_input(azk_batch* b, uint32_t i, void** dev) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && dev && i < b->eng.cfg.size());
+    *dev = b->eng.arena.at<void>(b->eng.off_input[i]);
+  });
+}
+
+azk_status azk_batch_upload(azk_batch* b, const uint32_t* host, const uint64_t* offsets, const uint64_t* counts) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && host && offsets && counts);
+    std::lock_guard<std::mutex> lk(b->mu);
+    Engine& e = b->eng;
+    for (size_t i = 0; i < e.cfg.size(); i++) {
+      uint64_t N = 1ull << e.cfg[i].logn;
+      layout(counts[i] >= 1 && counts[i] <= N);
+      uint4* in = e.arena.at<uint4>(e.off_input[i]);
+      AZK_CU(cudaMemcpyAsync(in, host + 4 * offsets[i], 16 * counts[i], cudaMemcpyHostToDevice, e.s));
+      if (counts[i] < N) AZK_CU(cudaMemsetAsync(in + counts[i], 0, 16 * (N - counts[i]), e.s));
+    }
+    AZK_CU(cudaStreamSynchronize(e.s));
+  });
+}
+
+azk_status azk_batch_prove(azk_batch* b, const uint8_t* pubs, int plain, azk_stats* st) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && pubs);
+    std::lock_guard<std::mutex> lk(b->mu);
+    Timer t;
+    Engine& e = b->eng;
+    e.set_publics(pubs);
+    uint64_t sub = 0;
+    double gs = e.run(true, plain != 0, &sub, t);
+    AZK_CU(cudaStreamSynchronize(e.s));
+    fill_stats(st, t, sub, gs);
+  });
+}
+
+azk_status azk_batch_proof_sizes(azk_batch* b, uint64_t* sizes, uint64_t* total) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b != nullptr);
+    uint64_t tt = 0;
+    for (size_t i = 0; i < b->eng.cfg.size(); i++) {
+      if (sizes) sizes[i] = b->eng.proof_len[i];
+      tt += b->eng.proof_len[i];
+    }
+    if (total) *total = tt;
+  });
+}
+
+azk_status azk_batch_download_proofs(azk_batch* b, uint8_t* out, uint64_t cap) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && out);
+    std::lock_guard<std::mutex> lk(b->mu);
+    Engine& e = b->eng;
+    uint64_t pos = 0;
+    for (size_t i = 0; i < e.cfg.size(); i++) {
+      layout(pos + e.proof_len[i] <= cap, "proof buffer too small");
+      AZK_CU(cudaMemcpyAsync(out + pos, e.h_inst[i].proof, e.proof_len[i], cudaMemcpyDeviceToHost, e.s));
+      pos += e.proof_len[i];
+    }
+    AZK_CU(cudaStreamSynchronize(e.s));
+  });
+}
+
+azk_status azk_batch_trace(azk_batch* b, uint32_t i, uint8_t* cm, uint32_t* ch, uint32_t* fl, uint32_t* qp) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && i < b->eng.cfg.size());
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->eng.trace(i, cm, ch, fl, qp);
+  });
+}
+
+void azk_batch_destroy(azk_batch* b) { delete b; }
+
+}  // extern "C"

@@ -1,0 +1,463 @@
+"""Plan objects mirroring AppleZKProver's Swift plan API over the C ABI.
+
+Names follow the reference (MetalContext -> Context, KeccakF1600PermutationBatchPlan
+-> KeccakF1600PermutationPlan, SHA3FixedOneBlockHashPlan, SHA3RawLeavesMerkleCommitPlan,
+CircleCodewordPlan, CirclePCSFRIResidentProverV1 -> CirclePCSFRIProver); each call
+goes straight to libazk_cuda.so.  Errors raise AZKError carrying the
+AppleZKProverError case name.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._capi import AZKError, Schedule, Stats, check, lib
+
+_vp = ctypes.c_void_p
+
+
+def _ptr(a) -> int:
+    return a.ctypes.data if a is not None else None
+
+
+def _u8(data) -> np.ndarray:
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    return np.frombuffer(bytes(data), dtype=np.uint8)
+
+
+def _q(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1, 4))
+
+
+class Context:
+    """One CUDA device (MetalContext.swift:62-112).  Raises AZKError(unavailableOnThisPlatform)
+    when no sm_100 device is present."""
+
+    def __init__(self, device: int = 0):
+        self._h = _vp()
+        check(lib().azk_ctx_create(device, ctypes.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().azk_ctx_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_info(self):
+        sm, mem, ma, mi = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_int(), ctypes.c_int()
+        check(lib().azk_ctx_device_info(self._h, ctypes.byref(sm), ctypes.byref(mem), ctypes.byref(ma), ctypes.byref(mi)), self._h)
+        return {"sm_count": sm.value, "total_bytes": mem.value, "cc": (ma.value, mi.value)}
+
+    def alloc(self, nbytes: int) -> "DeviceBuffer":
+        return DeviceBuffer(self, nbytes)
+
+    def synchronize(self):
+        check(lib().azk_synchronize(self._h), self._h)
+
+
+class DeviceBuffer:
+    """Device allocation owned by a context (MetalBufferFactory.makePrivateBuffer)."""
+
+    def __init__(self, ctx: Context, nbytes: int):
+        self.ctx = ctx
+        self.nbytes = int(nbytes)
+        self.ptr = _vp()
+        check(lib().azk_buf_alloc(ctx.handle, self.nbytes, ctypes.byref(self.ptr)), ctx.handle)
+
+    def upload(self, data, offset: int = 0):
+        b = _u8(data)
+        check(lib().azk_buf_upload(self.ctx.handle, self.ptr, offset, _ptr(b), b.nbytes), self.ctx.handle)
+
+    def download(self, nbytes: int | None = None, offset: int = 0) -> bytes:
+        n = self.nbytes - offset if nbytes is None else nbytes
+        out = np.empty(n, np.uint8)
+        check(lib().azk_buf_download(self.ctx.handle, _ptr(out), self.ptr, offset, n), self.ctx.handle)
+        return out.tobytes()
+
+    def zero(self):
+        check(lib().azk_buf_zero(self.ctx.handle, self.ptr, self.nbytes), self.ctx.handle)
+
+    def free(self):
+        if self.ptr:
+            lib().azk_buf_free(self.ctx.handle, self.ptr)
+            self.ptr = _vp()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class _Plan:
+    _destroy = None
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self._h = _vp()
+        self.last_stats = Stats()
+
+    def close(self):
+        if self._h and self._destroy:
+            getattr(lib(), self._destroy)(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        check(rc, self.ctx.handle)
+
+
+class KeccakF1600PermutationPlan(_Plan):
+    """KeccakF1600PermutationBatchPlan (KeccakF1600PermutationBatcher.swift:73-294)."""
+
+    _destroy = "azk_keccakf_plan_destroy"
+
+    def __init__(self, ctx: Context, count: int, input_stride: int = 200, output_stride: int = 200, threads: int = 0):
+        super().__init__(ctx)
+        self.count, self.input_stride, self.output_stride = count, input_stride, output_stride
+        self._check(lib().azk_keccakf_plan_create(ctx.handle, count, input_stride, output_stride, threads, ctypes.byref(self._h)))
+
+    def permute(self, states) -> bytes:
+        b = _u8(states)
+        if b.nbytes < self.count * self.input_stride:
+            raise AZKError(1, "state bytes shorter than count * inputStride")
+        out = np.empty(self.count * self.output_stride, np.uint8)
+        self._check(lib().azk_keccakf_plan_permute(self._h, _ptr(b), _ptr(out), ctypes.byref(self.last_stats)))
+        return out.tobytes()
+
+    def permute_resident(self, dev_in, dev_out, in_offset=0, out_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_keccakf_plan_permute_resident(self._h, dev_in, in_offset, dev_out, out_offset, ctypes.byref(st)))
+        return st
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_keccakf_plan_clear(self._h))
+
+
+class SHA3FixedOneBlockHashPlan(_Plan):
+    """SHA3FixedOneBlockHashPlan (SHA3BatchHasher.swift:81-264); keccak=True gives the
+    Keccak-256 twin (Keccak256BatchHasher.swift)."""
+
+    _destroy = "azk_hash_plan_destroy"
+
+    def __init__(self, ctx: Context, count: int, message_stride: int, message_length: int, output_stride: int = 32, keccak: bool = False,
+                 threads: int = 0):
+        super().__init__(ctx)
+        self.count, self.message_stride, self.message_length, self.output_stride = count, message_stride, message_length, output_stride
+        suffix = 0x01 if keccak else 0x06
+        self._check(lib().azk_hash_plan_create(ctx.handle, count, message_stride, message_length, output_stride, suffix, threads,
+                                               ctypes.byref(self._h)))
+
+    def hash(self, messages) -> bytes:
+        b = _u8(messages) if self.count * self.message_stride else np.zeros(1, np.uint8)
+        if self.count * self.message_stride and b.nbytes < self.count * self.message_stride:
+            raise AZKError(1, "message bytes shorter than count * messageStride")
+        out = np.empty(self.count * self.output_stride, np.uint8)
+        self._check(lib().azk_hash_plan_hash(self._h, _ptr(b), _ptr(out), ctypes.byref(self.last_stats)))
+        return out.tobytes()
+
+    def hash_resident(self, dev_in, dev_out, in_offset=0, out_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_hash_plan_hash_resident(self._h, dev_in, in_offset, dev_out, out_offset, ctypes.byref(st)))
+        return st
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_hash_plan_clear(self._h))
+
+
+class SHA3RawLeavesMerkleCommitPlan(_Plan):
+    """SHA3RawLeavesMerkleCommitPlan (MerkleCommitter.swift:526-1182).  treelet_log 0 = automatic."""
+
+    _destroy = "azk_merkle_plan_destroy"
+
+    def __init__(self, ctx: Context, leaf_count: int, leaf_stride: int, leaf_length: int, treelet_log: int = 0):
+        super().__init__(ctx)
+        self.leaf_count, self.leaf_stride, self.leaf_length = leaf_count, leaf_stride, leaf_length
+        self._check(lib().azk_merkle_plan_create(ctx.handle, leaf_count, leaf_stride, leaf_length, treelet_log, ctypes.byref(self._h)))
+        d, t = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib().azk_merkle_plan_info(self._h, ctypes.byref(d), ctypes.byref(t)))
+        self.tree_depth, self.treelet_leaf_count = d.value, t.value
+
+    def _leaves(self, leaves):
+        need = self.leaf_count * self.leaf_stride
+        if need == 0:
+            return np.zeros(1, np.uint8)
+        b = _u8(leaves)
+        if b.nbytes < need:
+            raise AZKError(1, "leaf bytes shorter than leafCount * leafStride")
+        return b
+
+    def commit(self, leaves) -> bytes:
+        b = self._leaves(leaves)
+        root = np.empty(32, np.uint8)
+        self._check(lib().azk_merkle_plan_commit(self._h, _ptr(b), _ptr(root), ctypes.byref(self.last_stats)))
+        return root.tobytes()
+
+    def commit_resident(self, dev_leaves, offset: int = 0) -> bytes:
+        root = np.empty(32, np.uint8)
+        self._check(lib().azk_merkle_plan_commit_resident(self._h, dev_leaves, offset, _ptr(root), ctypes.byref(self.last_stats)))
+        return root.tobytes()
+
+    def open_raw_leaf(self, leaves, leaf_index: int):
+        """Returns (leaf bytes, sibling digests bottom-up, root)."""
+        b = self._leaves(leaves)
+        leaf = np.zeros(max(1, self.leaf_length), np.uint8)
+        sib = np.zeros(max(1, self.tree_depth * 32), np.uint8)
+        root = np.empty(32, np.uint8)
+        self._check(lib().azk_merkle_plan_open(self._h, _ptr(b), leaf_index, _ptr(leaf), _ptr(sib), _ptr(root), ctypes.byref(self.last_stats)))
+        return leaf[: self.leaf_length].tobytes(), [sib[32 * l:32 * l + 32].tobytes() for l in range(self.tree_depth)], root.tobytes()
+
+    def open_resident(self, indices):
+        """Sibling paths of several leaves of the last committed tree (no recomputation)."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint64)
+        sib = np.zeros(max(1, len(idx) * self.tree_depth * 32), np.uint8)
+        self._check(lib().azk_merkle_plan_open_resident(self._h, _ptr(idx), len(idx), _ptr(sib), ctypes.byref(self.last_stats)))
+        d = self.tree_depth
+        return [[sib[(k * d + l) * 32:(k * d + l + 1) * 32].tobytes() for l in range(d)] for k in range(len(idx))]
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_merkle_plan_clear(self._h))
+
+
+def commit_prehashed_leaves(ctx: Context, digests) -> bytes:
+    """SHA3MerkleCommitter.commitPrehashedLeaves (MerkleCommitter.swift:225-304)."""
+    b = _u8(digests)
+    root = np.empty(32, np.uint8)
+    check(lib().azk_merkle_commit_prehashed(ctx.handle, _ptr(b) if b.nbytes else None, b.nbytes, _ptr(root), None), ctx.handle)
+    return root.tobytes()
+
+
+def circle_domain_points(ctx: Context, log_size: int) -> np.ndarray:
+    out = np.empty((1 << log_size, 2), np.uint32)
+    check(lib().azk_circle_domain_points(ctx.handle, log_size, _ptr(out)), ctx.handle)
+    return out
+
+
+def circle_fft_twiddles(ctx: Context, log_size: int) -> np.ndarray:
+    out = np.empty(max(1, (1 << log_size) - 1), np.uint32)
+    check(lib().azk_circle_fft_twiddles(ctx.handle, log_size, _ptr(out)), ctx.handle)
+    return out[: (1 << log_size) - 1]
+
+
+def circle_inverse_layers(ctx: Context, log_size: int, rounds: int) -> list:
+    n = 1 << log_size
+    out = np.empty(max(1, n - (n >> rounds)), np.uint32)
+    check(lib().azk_circle_inverse_layers(ctx.handle, log_size, rounds, _ptr(out)), ctx.handle)
+    layers, off = [], 0
+    for r in range(rounds):
+        m = n >> (r + 1)
+        layers.append(out[off:off + m].copy())
+        off += m
+    return layers
+
+
+class CircleCodewordPlan(_Plan):
+    """CircleCodewordPlan (CircleCodeword.swift:411-887)."""
+
+    _destroy = "azk_codeword_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int):
+        super().__init__(ctx)
+        self.log_size = log_size
+        self._check(lib().azk_codeword_plan_create(ctx.handle, log_size, ctypes.byref(self._h)))
+
+    def execute_coefficients(self, coefficients) -> np.ndarray:
+        c = _q(coefficients)
+        out = np.empty((1 << self.log_size, 4), np.uint32)
+        self._check(lib().azk_codeword_plan_execute(self._h, _ptr(c), len(c), _ptr(out), ctypes.byref(self.last_stats)))
+        return out
+
+    def execute(self, x_coefficients, y_coefficients=()) -> np.ndarray:
+        x = _q(x_coefficients) if len(x_coefficients) else np.zeros((1, 4), np.uint32)
+        y = _q(y_coefficients) if len(y_coefficients) else np.zeros((1, 4), np.uint32)
+        out = np.empty((1 << self.log_size, 4), np.uint32)
+        self._check(lib().azk_codeword_plan_execute_polynomial(self._h, _ptr(x), len(x_coefficients), _ptr(y), len(y_coefficients), _ptr(out),
+                                                               ctypes.byref(self.last_stats)))
+        return out
+
+    def execute_resident(self, dev_in, dev_out, in_offset=0, out_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_codeword_plan_execute_resident(self._h, dev_in, in_offset, dev_out, out_offset, ctypes.byref(st)))
+        return st
+
+
+def qm31_fold(ctx: Context, evaluations, inverse_points, challenge) -> np.ndarray:
+    """QM31FRIFoldPlan.execute (QM31FRIFold.swift:960-1117)."""
+    ev, inv, ch = _q(evaluations), _q(inverse_points), _q(challenge)
+    out = np.empty((len(ev) // 2, 4), np.uint32)
+    check(lib().azk_qm31_fold(ctx.handle, _ptr(ev), len(ev), _ptr(inv), _ptr(ch), _ptr(out), None), ctx.handle)
+    return out
+
+
+def circle_fold_chain(ctx: Context, log_size: int, evaluations, challenges) -> np.ndarray:
+    """CircleFRIFoldChainPlan.execute (CircleFRIFoldPlan.swift:132-280)."""
+    ev, ch = _q(evaluations), _q(challenges)
+    out = np.empty(((1 << log_size) >> len(ch), 4), np.uint32)
+    check(lib().azk_circle_fold_chain(ctx.handle, log_size, _ptr(ev), _ptr(ch), len(ch), _ptr(out), None), ctx.handle)
+    return out
+
+
+def qm31_merkle_fold_chain(ctx: Context, evaluations, inverse_layers):
+    """QM31FRIFoldChainPlan Merkle-transcript mode: (final layer, commitments, challenges)."""
+    ev = _q(evaluations)
+    inv = np.concatenate([_q(l) for l in inverse_layers])
+    r = len(inverse_layers)
+    fin = np.empty((len(ev) >> r, 4), np.uint32)
+    cm = np.empty(32 * r, np.uint8)
+    ch = np.empty((r, 4), np.uint32)
+    check(lib().azk_qm31_merkle_fold_chain(ctx.handle, _ptr(ev), len(ev), _ptr(inv), r, _ptr(fin), _ptr(cm), _ptr(ch), None), ctx.handle)
+    return fin, [cm[32 * k:32 * k + 32].tobytes() for k in range(r)], ch
+
+
+def qm31_transcript_challenges(ctx: Context, input_count: int, commitments) -> np.ndarray:
+    cm = _u8(b"".join(commitments))
+    out = np.empty((len(commitments), 4), np.uint32)
+    check(lib().azk_qm31_transcript_challenges(ctx.handle, input_count, _ptr(cm), len(commitments), _ptr(out)), ctx.handle)
+    return out
+
+
+def circle_merkle_fold_chain(ctx: Context, log_size: int, evaluations, log_blowup: int, queries: int, public_digest: bytes, rounds: int,
+                             grinding_bits: int = 0):
+    """CircleFRIMerkleTranscriptFoldChainPlan (CircleFRIFoldPlan.swift:301-518)."""
+    ev = _q(evaluations)
+    pub = _u8(public_digest)
+    fin = np.empty(((1 << log_size) >> rounds, 4), np.uint32)
+    cm = np.empty(32 * rounds, np.uint8)
+    ch = np.empty((rounds, 4), np.uint32)
+    check(lib().azk_circle_merkle_fold_chain(ctx.handle, log_size, _ptr(ev), log_blowup, queries, grinding_bits, _ptr(pub), rounds, _ptr(fin),
+                                             _ptr(cm), _ptr(ch), None), ctx.handle)
+    return fin, [cm[32 * k:32 * k + 32].tobytes() for k in range(rounds)], ch
+
+
+def pcs_proof_size(log_size, rounds, queries, claimed=0, grinding_bits=0) -> int:
+    return int(lib().azk_pcs_proof_size(log_size, rounds, queries, claimed, grinding_bits))
+
+
+def _sched(schedule):
+    if schedule is None:
+        return None
+    if isinstance(schedule, Schedule):
+        return ctypes.byref(schedule)
+    s = Schedule(schedule.get("treelet_log", 0), schedule.get("group_log", 0), schedule.get("threads", 0), schedule.get("use_graph", 1))
+    return ctypes.byref(s)
+
+
+class CirclePCSFRIProver(_Plan):
+    """CirclePCSFRIResidentProverV1 + CircleCodewordPCSFRIProverV1: evaluations or FFT-basis
+    coefficients -> CirclePCSFRIProofCodecV1 bytes, all on the device."""
+
+    _destroy = "azk_pcs_prover_destroy"
+
+    def __init__(self, ctx: Context, log_size: int, log_blowup: int, queries: int, rounds: int, grinding_bits: int = 0, schedule=None):
+        super().__init__(ctx)
+        self.log_size, self.log_blowup, self.queries, self.rounds, self.grinding_bits = log_size, log_blowup, queries, rounds, grinding_bits
+        self._check(lib().azk_pcs_prover_create(ctx.handle, log_size, log_blowup, queries, grinding_bits, rounds, _sched(schedule),
+                                                ctypes.byref(self._h)))
+
+    def _buf(self, claimed=0):
+        n = pcs_proof_size(self.log_size, self.rounds, self.queries, claimed, self.grinding_bits)
+        return np.empty(n, np.uint8), ctypes.c_uint64(n)
+
+    def prove_evaluations(self, evaluations, public_digest: bytes, claimed_indices=()) -> bytes:
+        ev, pub = _q(evaluations), _u8(public_digest)
+        cl = np.ascontiguousarray(list(claimed_indices) or [0], dtype=np.uint64)
+        out, n = self._buf(len(claimed_indices))
+        self._check(lib().azk_pcs_prover_prove_evaluations(self._h, _ptr(ev), _ptr(pub), _ptr(cl), len(claimed_indices), _ptr(out), ctypes.byref(n),
+                                                           ctypes.byref(self.last_stats)))
+        return out[: n.value].tobytes()
+
+    def prove_coefficients(self, coefficients, public_digest: bytes) -> bytes:
+        c, pub = _q(coefficients), _u8(public_digest)
+        out, n = self._buf()
+        self._check(lib().azk_pcs_prover_prove_coefficients(self._h, _ptr(c), len(c), _ptr(pub), _ptr(out), ctypes.byref(n),
+                                                            ctypes.byref(self.last_stats)))
+        return out[: n.value].tobytes()
+
+    def prove_resident(self, dev_input, public_digest: bytes, dev_proof, input_is_coefficients=True, in_offset=0) -> int:
+        pub = _u8(public_digest)
+        n = ctypes.c_uint64(pcs_proof_size(self.log_size, self.rounds, self.queries, 0, self.grinding_bits))
+        self._check(lib().azk_pcs_prover_prove_resident(self._h, dev_input, in_offset, 1 if input_is_coefficients else 0, _ptr(pub), dev_proof,
+                                                        ctypes.byref(n), ctypes.byref(self.last_stats)))
+        return n.value
+
+    def trace(self):
+        """(commitments, challenges, final layer, query pairs) of the last proof."""
+        cm = np.empty(32 * self.rounds, np.uint8)
+        ch = np.empty((self.rounds, 4), np.uint32)
+        fl = np.empty(((1 << self.log_size) >> self.rounds, 4), np.uint32)
+        qp = np.empty(self.queries, np.uint32)
+        self._check(lib().azk_pcs_prover_trace(self._h, _ptr(cm), _ptr(ch), _ptr(fl), _ptr(qp)))
+        return [cm[32 * k:32 * k + 32].tobytes() for k in range(self.rounds)], ch, fl, [int(v) for v in qp]
+
+
+class BatchProver(_Plan):
+    """Batched commit-and-fold superstep over uneven instances (azk_batch_*)."""
+
+    _destroy = "azk_batch_destroy"
+
+    def __init__(self, ctx: Context, log_sizes, rounds, log_blowup: int, queries: int, schedule=None):
+        super().__init__(ctx)
+        self.log_sizes = [int(v) for v in log_sizes]
+        self.rounds = [int(v) for v in rounds]
+        self.queries = queries
+        ls = np.ascontiguousarray(self.log_sizes, dtype=np.uint32)
+        rs = np.ascontiguousarray(self.rounds, dtype=np.uint32)
+        self._check(lib().azk_batch_create(ctx.handle, len(ls), _ptr(ls), _ptr(rs), log_blowup, queries, _sched(schedule), ctypes.byref(self._h)))
+        sizes = np.empty(len(ls), np.uint64)
+        total = ctypes.c_uint64()
+        self._check(lib().azk_batch_proof_sizes(self._h, _ptr(sizes), ctypes.byref(total)))
+        self.proof_sizes = [int(v) for v in sizes]
+        self.proof_total = total.value
+
+    def upload(self, coefficients_flat, offsets, counts):
+        """coefficients_flat: (M, 4) u32; instance i uses rows offsets[i] : offsets[i] + counts[i]."""
+        c = _q(coefficients_flat)
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        cnt = np.ascontiguousarray(counts, dtype=np.uint64)
+        self._check(lib().azk_batch_upload(self._h, _ptr(c), _ptr(off), _ptr(cnt)))
+
+    def input_pointer(self, index: int) -> int:
+        p = _vp()
+        self._check(lib().azk_batch_input(self._h, index, ctypes.byref(p)))
+        return p.value
+
+    def prove(self, public_digests: bytes, plain: bool = False) -> Stats:
+        pub = _u8(public_digests)
+        st = Stats()
+        self._check(lib().azk_batch_prove(self._h, _ptr(pub), 1 if plain else 0, ctypes.byref(st)))
+        self.last_stats = st
+        return st
+
+    def proofs(self):
+        out = np.empty(max(1, self.proof_total), np.uint8)
+        self._check(lib().azk_batch_download_proofs(self._h, _ptr(out), self.proof_total))
+        res, pos = [], 0
+        for n in self.proof_sizes:
+            res.append(out[pos:pos + n].tobytes())
+            pos += n
+        return res
+
+    def trace(self, index: int):
+        r, logn = self.rounds[index], self.log_sizes[index]
+        cm = np.empty(32 * r, np.uint8)
+        ch = np.empty((r, 4), np.uint32)
+        fl = np.empty(((1 << logn) >> r, 4), np.uint32)
+        qp = np.empty(self.queries, np.uint32)
+        self._check(lib().azk_batch_trace(self._h, index, _ptr(cm), _ptr(ch), _ptr(fl), _ptr(qp)))
+        return [cm[32 * k:32 * k + 32].tobytes() for k in range(r)], ch, fl, [int(v) for v in qp]

@@ -1,0 +1,225 @@
+/*
+ * azk_cuda.h -- C ABI of the B200 (sm_100a) commit-and-fold library.
+ *
+ * Drop-in boundary for AppleZKProver's Metal plans: every entry point below
+ * replaces one reference API (cited as path:line inside the reference package)
+ * with the same argument meaning and error behaviour.  Plain pointers and sizes
+ * only; "host" pointers are CPU memory, "device" pointers come from
+ * azk_buf_alloc (or any CUDA allocation on the context's device).
+ *
+ * Threading: every plan handle serialises its own calls with a mutex (the
+ * reference's per-plan NSLock, e.g. MerkleCommitter.swift:548); distinct plans may
+ * be used from different threads.  Calls are synchronous unless named _async.
+ *
+ * Field elements: M31 values are u32 in [0, 2^31-1); a QM31 value is four u32
+ * limbs (a, b, c, d) = (a + b i) + (c + d i) u, 16 bytes little-endian.
+ */
+#ifndef AZK_CUDA_H
+#define AZK_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes mirror AppleZKProverError (Sources/AppleZKProver/MetalTypes.swift:3-22). */
+typedef enum azk_status {
+  AZK_OK = 0,
+  AZK_ERR_INVALID_INPUT_LAYOUT = 1,          /* .invalidInputLayout */
+  AZK_ERR_INVALID_LEAF_COUNT = 2,            /* .invalidLeafCount(n) */
+  AZK_ERR_UNSUPPORTED_ONE_BLOCK_LENGTH = 3,  /* .unsupportedOneBlockLength(n) */
+  AZK_ERR_INVALID_PREHASHED_LEAF_LENGTH = 4, /* .invalidPrehashedLeafLength(n) */
+  AZK_ERR_CORRECTNESS_VALIDATION_FAILED = 5, /* .correctnessValidationFailed(msg) */
+  AZK_ERR_COMMAND_EXECUTION_FAILED = 6,      /* .commandExecutionFailed(msg) */
+  AZK_ERR_UNAVAILABLE = 7,                   /* .unavailableOnThisPlatform / .noMetalDevice */
+  AZK_ERR_INVALID_KERNEL_CONFIGURATION = 8,  /* .invalidKernelConfiguration(msg) */
+  AZK_ERR_FAILED_TO_CREATE_BUFFER = 9,       /* .failedToCreateBuffer(label, length) */
+  AZK_ERR_DEVICE_TIMEOUT = 10,               /* a bounded device wait gave up */
+  AZK_ERR_HBM_BUDGET = 11                    /* admission refused: HBM budget exhausted */
+} azk_status;
+
+/* GPUExecutionStats (MetalTypes.swift:71-79): wall time of the call, device
+ * time between the first and last kernel (CUDA events), host submit time. */
+typedef struct azk_stats {
+  double cpu_wall_s;
+  double gpu_s;
+  uint64_t cpu_submit_ns;
+} azk_stats;
+
+typedef struct azk_ctx azk_ctx;
+typedef struct azk_keccakf_plan azk_keccakf_plan;
+typedef struct azk_hash_plan azk_hash_plan;
+typedef struct azk_merkle_plan azk_merkle_plan;
+typedef struct azk_codeword_plan azk_codeword_plan;
+typedef struct azk_pcs_prover azk_pcs_prover;
+typedef struct azk_batch azk_batch;
+
+/* ---- context and device buffers (MetalContext.swift:62-327, MetalBufferFactory.swift:8-159) ---- */
+
+/* Create a context on CUDA device `device`.  Fails with AZK_ERR_UNAVAILABLE when
+ * no sm_100 device is present (there is no CPU fallback). */
+azk_status azk_ctx_create(int device, azk_ctx** out);
+void azk_ctx_destroy(azk_ctx* ctx);
+/* Message of the last failed call on this context (thread-local when ctx is NULL). */
+const char* azk_last_error_message(const azk_ctx* ctx);
+azk_status azk_ctx_device_info(azk_ctx* ctx, int* sm_count, uint64_t* total_bytes, int* cc_major, int* cc_minor);
+azk_status azk_buf_alloc(azk_ctx* ctx, uint64_t bytes, void** out);
+azk_status azk_buf_free(azk_ctx* ctx, void* ptr);
+azk_status azk_buf_upload(azk_ctx* ctx, void* dst, uint64_t dst_offset, const void* src, uint64_t bytes);
+azk_status azk_buf_download(azk_ctx* ctx, void* dst, const void* src, uint64_t src_offset, uint64_t bytes);
+azk_status azk_buf_zero(azk_ctx* ctx, void* dst, uint64_t bytes);
+azk_status azk_synchronize(azk_ctx* ctx);
+
+/* ---- Keccak-f[1600] permutation batch (KeccakF1600PermutationBatcher.swift:31-70, 73-294) ----
+ * Strides are multiples of 8 and >= 200; output bytes past 200 in each stride
+ * are zeroed.  threads_per_block 0 selects the default. */
+azk_status azk_keccakf_plan_create(azk_ctx* ctx, uint64_t count, uint64_t input_stride, uint64_t output_stride,
+                                   uint32_t threads_per_block, azk_keccakf_plan** out);
+azk_status azk_keccakf_plan_permute(azk_keccakf_plan* plan, const void* host_states, void* host_out, azk_stats* stats);
+azk_status azk_keccakf_plan_permute_resident(azk_keccakf_plan* plan, const void* dev_in, uint64_t in_offset, void* dev_out,
+                                             uint64_t out_offset, azk_stats* stats);
+azk_status azk_keccakf_plan_clear(azk_keccakf_plan* plan);
+void azk_keccakf_plan_destroy(azk_keccakf_plan* plan);
+
+/* ---- fixed-rate SHA3-256 / Keccak-256 batch (SHA3BatchHasher.swift:39-264,
+ * Keccak256BatchHasher.swift:5-257) ----
+ * domain_suffix 0x06 = SHA3-256, 0x01 = Keccak-256.  length <= 136, stride >=
+ * length, output_stride >= 32 (padding bytes zeroed). */
+azk_status azk_hash_plan_create(azk_ctx* ctx, uint64_t count, uint64_t message_stride, uint64_t message_length, uint64_t output_stride,
+                                uint32_t domain_suffix, uint32_t threads_per_block, azk_hash_plan** out);
+azk_status azk_hash_plan_hash(azk_hash_plan* plan, const void* host_messages, void* host_digests, azk_stats* stats);
+azk_status azk_hash_plan_hash_resident(azk_hash_plan* plan, const void* dev_messages, uint64_t in_offset, void* dev_digests,
+                                       uint64_t out_offset, azk_stats* stats);
+azk_status azk_hash_plan_clear(azk_hash_plan* plan);
+void azk_hash_plan_destroy(azk_hash_plan* plan);
+
+/* ---- SHA3 Merkle commitment over raw leaves (MerkleCommitter.swift:152-223, 526-1063) ----
+ * leaf_count a power of two, leaf_length <= 136, leaf_stride >= leaf_length.
+ * treelet_log: 0 = automatic, else leaves per CTA treelet = 2^treelet_log (1..11).
+ * The tree stays resident after a commit, so openings gather sibling paths
+ * without recomputing it. */
+azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t leaf_count, uint64_t leaf_stride, uint64_t leaf_length, uint32_t treelet_log,
+                                  azk_merkle_plan** out);
+azk_status azk_merkle_plan_commit(azk_merkle_plan* plan, const void* host_leaves, uint8_t root_out[32], azk_stats* stats);
+azk_status azk_merkle_plan_commit_resident(azk_merkle_plan* plan, const void* dev_leaves, uint64_t offset, uint8_t root_out[32],
+                                           azk_stats* stats);
+/* Commit `host_leaves` and open `leaf_index`: leaf bytes, depth sibling digests
+ * (bottom-up) and the root (SHA3RawLeavesMerkleCommitPlan.openRawLeaf, :667-720). */
+azk_status azk_merkle_plan_open(azk_merkle_plan* plan, const void* host_leaves, uint64_t leaf_index, uint8_t* leaf_out,
+                                uint8_t* siblings_out, uint8_t root_out[32], azk_stats* stats);
+/* Openings of `count` leaves of the last committed tree: count * depth digests. */
+azk_status azk_merkle_plan_open_resident(azk_merkle_plan* plan, const uint64_t* leaf_indices, uint64_t count, uint8_t* siblings_out,
+                                         azk_stats* stats);
+azk_status azk_merkle_plan_info(azk_merkle_plan* plan, uint32_t* tree_depth, uint32_t* treelet_leaf_count);
+azk_status azk_merkle_plan_clear(azk_merkle_plan* plan);
+void azk_merkle_plan_destroy(azk_merkle_plan* plan);
+/* Root over 32-byte prehashed leaves (SHA3MerkleCommitter.commitPrehashedLeaves, :225-304;
+ * SHA3PrehashedLeavesMerkleCommitPlan, :314-524). */
+azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* host_digests, uint64_t digest_bytes, uint8_t root_out[32], azk_stats* stats);
+
+/* ---- circle domain materialisation (CircleDomainMaterializationPlan.swift:52-219) ----
+ * Canonical bit-reversed domain of size 2^log_size (1..26).  Points in storage
+ * order as (x, y); FFT twiddles (N - 1 words, stage s at N - (N >> s)); inverse
+ * domain layers for `rounds` folds concatenated (N/2 + N/4 + ... words, M31). */
+azk_status azk_circle_domain_points(azk_ctx* ctx, uint32_t log_size, uint32_t* xy_out);
+azk_status azk_circle_fft_twiddles(azk_ctx* ctx, uint32_t log_size, uint32_t* out);
+azk_status azk_circle_inverse_layers(azk_ctx* ctx, uint32_t log_size, uint32_t rounds, uint32_t* out);
+
+/* ---- Circle FFT codeword (CircleCodeword.swift:411-887) ----
+ * Input: N interleaved FFT-basis coefficients [x0, y0, x1, y1, ...] (QM31),
+ * output: the codeword in bit-reversed domain order.  coefficient_count <= N
+ * leading coefficients are given; the rest are zero. */
+azk_status azk_codeword_plan_create(azk_ctx* ctx, uint32_t log_size, azk_codeword_plan** out);
+azk_status azk_codeword_plan_execute(azk_codeword_plan* plan, const uint32_t* host_coefficients, uint64_t coefficient_count,
+                                     uint32_t* host_codeword, azk_stats* stats);
+/* Monomial polynomial P(x) + y Q(x) (CircleCodewordPlan.execute(polynomial:), :460-475). */
+azk_status azk_codeword_plan_execute_polynomial(azk_codeword_plan* plan, const uint32_t* x_coefficients, uint64_t x_count,
+                                                const uint32_t* y_coefficients, uint64_t y_count, uint32_t* host_codeword, azk_stats* stats);
+azk_status azk_codeword_plan_execute_resident(azk_codeword_plan* plan, const void* dev_coefficients, uint64_t in_offset, void* dev_codeword,
+                                              uint64_t out_offset, azk_stats* stats);
+void azk_codeword_plan_destroy(azk_codeword_plan* plan);
+
+/* ---- FRI folds (QM31FRIFold.swift:960-1877, CircleFRIFoldPlan.swift:5-518) ---- */
+/* One QM31 fold with arbitrary nonzero QM31 inverse-domain points (n/2 of them). */
+azk_status azk_qm31_fold(azk_ctx* ctx, const uint32_t* evaluations, uint64_t n, const uint32_t* inverse_points, const uint32_t challenge[4],
+                         uint32_t* out, azk_stats* stats);
+/* Circle fold chain with explicit challenges (CircleFRIFoldChainPlan, :132-280):
+ * round 0 folds circle -> line, later rounds line -> line. */
+azk_status azk_circle_fold_chain(azk_ctx* ctx, uint32_t log_size, const uint32_t* evaluations, const uint32_t* challenges, uint32_t rounds,
+                                 uint32_t* out, azk_stats* stats);
+/* QM31 fold chain, Merkle-transcript mode (QM31FRIFoldChainPlan.executeMerkleTranscriptDerived,
+ * QM31FRIFold.swift:2203-2531): inverse layers are QM31 (n/2 + n/4 + ...).  Emits the
+ * per-round roots (32 bytes each), challenges (4 limbs each) and the final layer. */
+azk_status azk_qm31_merkle_fold_chain(azk_ctx* ctx, const uint32_t* evaluations, uint64_t n, const uint32_t* inverse_layers, uint32_t rounds,
+                                      uint32_t* final_out, uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* QM31 fold chain challenges derived from caller-supplied commitments
+ * (QM31FRIFoldTranscriptOracle.deriveChallenges, QM31FRIFold.swift:91-125). */
+azk_status azk_qm31_transcript_challenges(azk_ctx* ctx, uint64_t input_count, const uint8_t* commitments, uint32_t rounds,
+                                          uint32_t* challenges_out);
+/* Circle Merkle-transcript fold chain with Circle V1 framing
+ * (CircleFRIMerkleTranscriptFoldChainPlan, CircleFRIFoldPlan.swift:301-518). */
+azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t log_size, const uint32_t* evaluations, uint32_t log_blowup, uint32_t queries,
+                                        uint32_t grinding_bits, const uint8_t public_digest[32], uint32_t rounds, uint32_t* final_out,
+                                        uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* Canonicality gate (QM31CanonicalityCheck.swift:11-117): *non_canonical = 1 if any word >= p. */
+azk_status azk_check_canonical(azk_ctx* ctx, const void* dev_words, uint64_t word_count, uint32_t* non_canonical);
+
+/* ---- Circle PCS/FRI prover (CirclePCSFRIResidentProverV1, CircleFRIFoldPlan.swift:693-1025;
+ * CircleCodewordPCSFRIProverV1, CircleCodeword.swift:920-1419) ----
+ * Produces CirclePCSFRIProofCodecV1 bytes (CircleProofFormat.swift:478-593). */
+typedef struct azk_schedule {
+  uint32_t treelet_log;   /* leaves per CTA treelet = 2^treelet_log (1..11); 0 = default */
+  uint32_t group_log;     /* upper-level group size (1..treelet_log); 0 = default */
+  uint32_t threads;       /* threads per CTA for hashing kernels: 128, 256 or 512; 0 = default */
+  uint32_t use_graph;     /* batched form: capture the superstep in a CUDA graph */
+} azk_schedule;
+
+azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,
+                                 uint32_t rounds, const azk_schedule* schedule, azk_pcs_prover** out);
+/* Bytes of the encoded proof for these parameters. */
+uint64_t azk_pcs_proof_size(uint32_t log_size, uint32_t rounds, uint32_t queries, uint32_t claimed_count, uint32_t grinding_bits);
+/* From codeword evaluations (bit-reversed order). */
+azk_status azk_pcs_prover_prove_evaluations(azk_pcs_prover* p, const uint32_t* host_evaluations, const uint8_t public_digest[32],
+                                            const uint64_t* claimed_indices, uint64_t claimed_count, uint8_t* proof_out,
+                                            uint64_t* proof_len, azk_stats* stats);
+/* From interleaved FFT-basis coefficients (coefficient_count leading values, rest zero):
+ * FFT -> commit -> fold chain -> queries -> proof bytes, all on the device. */
+azk_status azk_pcs_prover_prove_coefficients(azk_pcs_prover* p, const uint32_t* host_coefficients, uint64_t coefficient_count,
+                                             const uint8_t public_digest[32], uint8_t* proof_out, uint64_t* proof_len, azk_stats* stats);
+/* Resident variant: input already on the device (coefficients when
+ * input_is_coefficients, else evaluations); proof bytes written to dev_proof. */
+azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* dev_input, uint64_t in_offset, int input_is_coefficients,
+                                         const uint8_t public_digest[32], void* dev_proof, uint64_t* proof_len, azk_stats* stats);
+/* Public readbacks of the last proof: commitments (32 bytes each), challenges,
+ * final layer and query pair indices (any pointer may be NULL). */
+azk_status azk_pcs_prover_trace(azk_pcs_prover* p, uint8_t* commitments, uint32_t* challenges, uint32_t* final_layer, uint32_t* query_pairs);
+void azk_pcs_prover_destroy(azk_pcs_prover* p);
+
+/* ---- batched commit-and-fold superstep (no counterpart in the reference: it
+ * proves one instance per plan) ----
+ * Many PCS instances of uneven log sizes proved together: one launch per stage
+ * over all instances (FFT passes, per-round fold + commit + transcript, queries,
+ * proof emission), optionally captured in a CUDA graph. */
+azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* log_sizes, const uint32_t* rounds, uint32_t log_blowup,
+                            uint32_t queries, const azk_schedule* schedule, azk_batch** out);
+/* Device pointer of instance i's coefficient input (N_i QM31); the caller may
+ * fill it in place (resident input). */
+azk_status azk_batch_input(azk_batch* b, uint32_t index, void** dev_input);
+/* Copy coefficients from the host: instance i's coefficient_counts[i] leading
+ * values start at host_coefficients + 4 * offsets[i] (u32 words / 4). */
+azk_status azk_batch_upload(azk_batch* b, const uint32_t* host_coefficients, const uint64_t* offsets, const uint64_t* coefficient_counts);
+/* Prove all instances from their resident coefficients.  plain != 0 runs the
+ * per-instance form (each instance's kernels launched in sequence, no graph). */
+azk_status azk_batch_prove(azk_batch* b, const uint8_t* public_digests, int plain, azk_stats* stats);
+azk_status azk_batch_proof_sizes(azk_batch* b, uint64_t* sizes, uint64_t* total);
+/* Proof bytes of all instances, concatenated in instance order. */
+azk_status azk_batch_download_proofs(azk_batch* b, uint8_t* out, uint64_t capacity);
+azk_status azk_batch_trace(azk_batch* b, uint32_t index, uint8_t* commitments, uint32_t* challenges, uint32_t* final_layer, uint32_t* query_pairs);
+void azk_batch_destroy(azk_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AZK_CUDA_H */

@@ -27,3 +27,6 @@ def golden():
 
     with open(os.path.join(ROOT, "tests", "golden", "reference_vectors.json")) as f:
         return json.load(f)["vectors"]
+
+
+from tests.gpu_common import ctx  # noqa: E402,F401  (session GPU context fixture)
