@@ -30,6 +30,7 @@ from .plans import (  # noqa: F401
     circle_merkle_fold_chain,
     commit_prehashed_leaves,
     pcs_proof_size,
+    probe_int_issue,
     qm31_fold,
     qm31_merkle_fold_chain,
     qm31_transcript_challenges,

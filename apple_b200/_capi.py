@@ -116,7 +116,11 @@ PROTOTYPES = {
     "azk_batch_proof_sizes": (I32, [P, P, U64P]),
     "azk_batch_download_proofs": (I32, [P, P, U64]),
     "azk_batch_trace": (I32, [P, U32, P, P, P, P]),
+    "azk_batch_set_profiling": (I32, [P, I32]),
+    "azk_batch_profile": (I32, [P, P]),
+    "azk_batch_work": (I32, [P, U64P, U64P, U64P, U32P]),
     "azk_batch_destroy": (None, [P]),
+    "azk_probe_int_issue": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
 }
 
 

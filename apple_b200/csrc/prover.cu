@@ -55,9 +55,51 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   bool graph_from_coeffs = false;
 
+  // Per-stage CUDA events (profiling): stage kind 0 = FFT, 1 = tree (fold +
+  // hash + transcript), 2 = final fold, 3 = transcript/queries/emission.
+  bool prof = false;
+  std::vector<int> ev_kind;
+  std::vector<cudaEvent_t> ev_a, ev_b;
+  size_t ev_used = 0;
+  // algorithmic work per superstep
+  uint64_t tree_perms = 0, fft_bytes = 0, fold_bytes = 0;
+  uint32_t launches = 0;
+
   ~Engine() {
     if (graph) cudaGraphExecDestroy(graph);
+    for (auto e : ev_a) cudaEventDestroy(e);
+    for (auto e : ev_b) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
+  }
+
+  // Event pair for the next profiled region (created up front, outside capture).
+  void ensure_events(size_t n) {
+    while (ev_a.size() < n) {
+      cudaEvent_t a, b;
+      AZK_CU(cudaEventCreate(&a));
+      AZK_CU(cudaEventCreate(&b));
+      ev_a.push_back(a);
+      ev_b.push_back(b);
+      ev_kind.push_back(0);
+    }
+  }
+  void prof_begin(int kind) {
+    if (!prof) return;
+    ev_kind[ev_used] = kind;
+    AZK_CU(cudaEventRecord(ev_a[ev_used], s));
+  }
+  void prof_end() {
+    if (!prof) return;
+    AZK_CU(cudaEventRecord(ev_b[ev_used], s));
+    ev_used++;
+  }
+  void profile(double* sec) {
+    for (int k = 0; k < 4; k++) sec[k] = 0;
+    for (size_t i = 0; i < ev_used; i++) {
+      float ms = 0;
+      AZK_CU(cudaEventElapsedTime(&ms, ev_a[i], ev_b[i]));
+      sec[ev_kind[i]] += ms / 1000.0;
+    }
   }
 
   PcsInstance* d_inst() const { return arena.at<PcsInstance>(off_inst); }
@@ -224,6 +266,21 @@ struct Engine {
     up(d_fold_jobs, fold_jobs.data(), fold_jobs.size() * sizeof(FoldJob), "PCS.FoldJobs");
     up(d_fold_work, fold_work.data(), fold_work.size() * sizeof(uint2), "PCS.FoldWork");
     AZK_CU(cudaStreamSynchronize(s));
+    // algorithmic work: leaf + parent permutations and 3 transcript absorbs per
+    // committed layer; FFT single-pass bytes (16N in, 16N out, 4(N-1) twiddles);
+    // final fold bytes (16 in + 8 out + 2 twiddle per input element)
+    for (auto& c2 : cfg) {
+      uint64_t N = 1ull << c2.logn;
+      for (uint32_t k = 0; k < c2.rounds; k++) tree_perms += 2 * (N >> k) - 1 + 3;
+      fft_bytes += 32 * N + 4 * (N - 1);
+      fold_bytes += 26 * (N >> (c2.rounds - 1));
+    }
+    launches = 0;
+    for (auto c3 : fft.step_cnt) launches += c3 ? 1 : 0;
+    for (auto c3 : tstep_cnt) launches += c3 ? 1 : 0;
+    for (auto c3 : fstep_cnt) launches += c3 ? 1 : 0;
+    launches += 4;  // prefix, finalize, queries, emit
+    ensure_events(fft.step_cnt.size() + 2 * rmax + 8);
   }
 
   void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt) {
@@ -238,17 +295,38 @@ struct Engine {
 
   // Everything up to (not including) grinding.  from_coeffs: run the FFT first.
   void enqueue_rounds_batched(bool from_coeffs) {
-    if (from_coeffs) fft.launch_all(s);
-    AZK_CU(launch_pcs_prefix(d_inst(), (uint32_t)cfg.size(), s));
-    for (uint32_t k = 0; k <= rmax; k++) {
-      if (k < rmax) launch_tree_range(k, tstep_off[k], tstep_cnt[k]);
-      if (k >= 1) launch_fold_range(fstep_off[k], fstep_cnt[k]);
+    ev_used = 0;
+    if (from_coeffs) {
+      for (size_t st = 0; st < fft.step_cnt.size(); st++) {
+        prof_begin(0);
+        fft.launch_step(st, s);
+        prof_end();
+      }
     }
+    prof_begin(3);
+    AZK_CU(launch_pcs_prefix(d_inst(), (uint32_t)cfg.size(), s));
+    prof_end();
+    for (uint32_t k = 0; k <= rmax; k++) {
+      if (k < rmax) {
+        prof_begin(1);
+        launch_tree_range(k, tstep_off[k], tstep_cnt[k]);
+        prof_end();
+      }
+      if (k >= 1 && fstep_cnt[k]) {
+        prof_begin(2);
+        launch_fold_range(fstep_off[k], fstep_cnt[k]);
+        prof_end();
+      }
+    }
+    prof_begin(3);
     AZK_CU(launch_pcs_finalize(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
+    prof_end();
   }
   void enqueue_tail_batched() {
+    prof_begin(3);
     AZK_CU(launch_pcs_queries(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
     AZK_CU(launch_pcs_emit(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), qmax, s));
+    prof_end();
   }
   void enqueue_instance(uint32_t i, bool from_coeffs) {
     if (from_coeffs)
@@ -300,8 +378,11 @@ struct Engine {
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
     GpuTimer g(s);
     if (plain) {
+      ev_used = 0;
       for (uint32_t i = 0; i < cfg.size(); i++) enqueue_instance(i, from_coeffs);
-    } else if (!any_grinding && sched.graph) {
+    } else if (!any_grinding && sched.graph && !prof) {
+      // (profiled runs take the eager path below: the same launch sequence, with
+      // event pairs around each stage)
       if (!graph || graph_from_coeffs != from_coeffs) {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -602,6 +683,33 @@ azk_status azk_batch_trace(azk_batch* b, uint32_t i, uint8_t* cm, uint32_t* ch, 
     layout(b && i < b->eng.cfg.size());
     std::lock_guard<std::mutex> lk(b->mu);
     b->eng.trace(i, cm, ch, fl, qp);
+  });
+}
+
+azk_status azk_batch_set_profiling(azk_batch* b, int enabled) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b != nullptr);
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->eng.prof = enabled != 0;
+  });
+}
+
+azk_status azk_batch_profile(azk_batch* b, double* seconds4) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b && seconds4);
+    std::lock_guard<std::mutex> lk(b->mu);
+    AZK_CU(cudaStreamSynchronize(b->eng.s));
+    b->eng.profile(seconds4);
+  });
+}
+
+azk_status azk_batch_work(azk_batch* b, uint64_t* tree_permutations, uint64_t* fft_bytes, uint64_t* fold_bytes, uint32_t* launches) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    layout(b != nullptr);
+    if (tree_permutations) *tree_permutations = b->eng.tree_perms;
+    if (fft_bytes) *fft_bytes = b->eng.fft_bytes;
+    if (fold_bytes) *fold_bytes = b->eng.fold_bytes;
+    if (launches) *launches = b->eng.launches;
   });
 }
 

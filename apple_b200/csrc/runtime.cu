@@ -920,6 +920,27 @@ azk_status azk_qm31_transcript_challenges(azk_ctx* ctx, uint64_t input_count, co
   });
 }
 
+azk_status azk_probe_int_issue(azk_ctx* ctx, double* ops_per_second) {
+  return guarded(ctx, [&] {
+    layout(ctx && ops_per_second);
+    AZK_CU(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    DevBuf sink(16, "Probe.Sink");
+    double ops = 0;
+    AZK_CU(launch_int_issue_probe(ctx->sm_count, s, sink.as<uint32_t>(), &ops, nullptr));  // warm-up
+    AZK_CU(cudaStreamSynchronize(s));
+    double best = 0;
+    for (int rep = 0; rep < 5; rep++) {
+      GpuTimer g(s);
+      AZK_CU(launch_int_issue_probe(ctx->sm_count, s, sink.as<uint32_t>(), &ops, nullptr));
+      g.stop();
+      double sec = g.seconds();
+      if (sec > 0) best = std::max(best, ops / sec);
+    }
+    *ops_per_second = best;
+  });
+}
+
 azk_status azk_check_canonical(azk_ctx* ctx, const void* dwords, uint64_t nwords, uint32_t* flag_out) {
   return guarded(ctx, [&] {
     layout(ctx && dwords && flag_out);

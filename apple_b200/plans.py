@@ -345,6 +345,13 @@ def circle_merkle_fold_chain(ctx: Context, log_size: int, evaluations, log_blowu
     return fin, [cm[32 * k:32 * k + 32].tobytes() for k in range(rounds)], ch
 
 
+def probe_int_issue(ctx: Context) -> float:
+    """Sustained LOP3+SHF 32-bit op rate of the device (ops/s)."""
+    v = ctypes.c_double()
+    check(lib().azk_probe_int_issue(ctx.handle, ctypes.byref(v)), ctx.handle)
+    return v.value
+
+
 def pcs_proof_size(log_size, rounds, queries, claimed=0, grinding_bits=0) -> int:
     return int(lib().azk_pcs_proof_size(log_size, rounds, queries, claimed, grinding_bits))
 
@@ -452,6 +459,19 @@ class BatchProver(_Plan):
             res.append(out[pos:pos + n].tobytes())
             pos += n
         return res
+
+    def set_profiling(self, enabled: bool = True):
+        self._check(lib().azk_batch_set_profiling(self._h, 1 if enabled else 0))
+
+    def profile(self) -> dict:
+        sec = np.zeros(4, np.float64)
+        self._check(lib().azk_batch_profile(self._h, _ptr(sec)))
+        return {"fft_s": float(sec[0]), "tree_s": float(sec[1]), "fold_s": float(sec[2]), "transcript_s": float(sec[3])}
+
+    def work(self) -> dict:
+        t, f, d, l = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(lib().azk_batch_work(self._h, ctypes.byref(t), ctypes.byref(f), ctypes.byref(d), ctypes.byref(l)))
+        return {"tree_permutations": t.value, "fft_bytes": f.value, "fold_bytes": d.value, "launches": l.value}
 
     def trace(self, index: int):
         r, logn = self.rounds[index], self.log_sizes[index]

@@ -1,0 +1,400 @@
+"""Benchmark: batched commit-and-fold superstep on B200 (one JSON line).
+
+Workload (default): 512 independent Circle PCS/FRI commit-and-fold instances with
+log codeword sizes drawn uniformly in [10, 22] (SplitMix64 seed 0xA11CE004),
+blowup 4 (the low quarter of each interleaved FFT-basis coefficient buffer holds
+seeded uniform M31 values lifted to QM31, the rest is zero), 16-byte QM31 Merkle
+leaves, SHA3 Merkle commitment per layer, QM31 Circle FRI folds down to log 6
+with Merkle-transcript challenges, 64 queries, proof bytes emitted on device.
+
+Metric: committed-and-folded codeword elements per second (sum of 2^logN over
+the instances / device time of one superstep).  `e2e` is the same metric through
+the C ABI from pinned host buffers: coefficients H2D, prove, proof bytes D2H.
+`plain` is the per-instance form (each instance's kernels launched in sequence).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs one replica per GPU (torchrun; instances do not exchange data, so
+there is no collective on the data path) and reports the max device time over
+ranks.  `--impl reference` times the CPU restatement of the reference's CPU
+oracle on the host cores instead (the reference itself is Swift + Metal and cannot
+run on this box).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 0xA11CE004
+P = 2147483647
+
+
+def splitmix64(seed, n):
+    GOLD = np.uint64(0x9E3779B97F4A7C15)
+    k = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + k * GOLD
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform_m31(seed, n):
+    out, draw = [], 0
+    have = 0
+    while have < n:
+        w = splitmix64((seed + 0x51ED27 * draw) & 0xFFFFFFFFFFFFFFFF, n - have + (n - have) // 16 + 16)
+        v = (w & np.uint64(0x7FFFFFFF)).astype(np.uint32)
+        v = v[v != np.uint32(P)]
+        out.append(v)
+        have += len(v)
+        draw += 1
+    return np.concatenate(out)[:n]
+
+
+def workload(count=512, lo=10, hi=22, final_log=6, seed=SEED):
+    """Log sizes, rounds and the compact coefficient prefix of every instance."""
+    draws = splitmix64(seed, count)
+    logs = [int(lo + (int(d) % (hi - lo + 1))) for d in draws]
+    rounds = [max(1, lg - final_log) for lg in logs]
+    counts = [(1 << lg) >> 2 for lg in logs]  # blowup 4: the low quarter carries the coefficients
+    offsets = list(np.cumsum([0] + counts[:-1]))
+    return logs, rounds, counts, offsets
+
+
+def coefficient_rows(counts, seed=SEED):
+    total = int(sum(counts))
+    rows = np.zeros((total, 4), np.uint32)
+    rows[:, 0] = uniform_m31(seed ^ 0xC0EFF, total)
+    return rows
+
+
+def public_digests(n, seed=SEED):
+    w = splitmix64(seed ^ 0x9B, 4 * n)
+    return w.astype("<u8").tobytes()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        loaded = [v for v in sm if smax and v > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs"), "measured"
+    except (OSError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the tree kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, value: float, local: int) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(logs, rounds, counts, offsets, rows, pubs, budget_elems):
+    """Prove a prefix of the workload's instances with the CPU oracle (all host threads)."""
+    from oracle import pyoracle as O
+
+    t0 = time.perf_counter()
+    elems = 0
+    done = 0
+    for i, lg in enumerate(logs):
+        if elems >= budget_elems and done:
+            break
+        n = 1 << lg
+        c = np.zeros((n, 4), np.uint32)
+        c[: counts[i]] = rows[offsets[i]:offsets[i] + counts[i]]
+        ev = O.fft_evaluate(lg, c)
+        O.prove(lg, ev, 2, 64, pubs[32 * i:32 * i + 32], rounds[i])
+        elems += n
+        done += 1
+    dt = time.perf_counter() - t0
+    return elems, dt, done
+
+
+def run_reference(args, logs, rounds, counts, offsets, rows, pubs, world, rank, dist):
+    if rank != 0:
+        return
+    from oracle import pyoracle as O
+
+    O.lib()
+    threads = O.num_threads()
+    budget = args.cpu_budget_elems
+    for _ in range(args.warmup):
+        cpu_sample(logs[:2], rounds[:2], counts[:2], offsets[:2], rows, pubs, 1)
+    vals = []
+    total_t, total_e, inst = 0.0, 0, 0
+    for _ in range(args.steps):
+        e, dt, k = cpu_sample(logs, rounds, counts, offsets, rows, pubs, budget)
+        vals.append(e / dt)
+        total_t += dt
+        total_e += e
+        inst = k
+    value = total_e / total_t
+    sample = f"first {inst} instances of the workload (sum 2^logN = {total_e // args.steps}), FFT + prove with the C++ oracle per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total_t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64",
+        "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "The reference (Swift + Metal) cannot run on Linux/B200; this arm times the repository's C++ restatement of its CPU oracles.",
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "commit+FRI-fold M31 elems/s batched vs plain on 1 B200, bit-exact; p50/p99"
+UNIT = "elems/s"
+
+
+def config_block(args, logs):
+    return {
+        "workload": f"{len(logs)} Circle PCS/FRI commit-and-fold instances, log sizes U[{args.lo},{args.hi}] (seed 0xA11CE004), blowup 4, "
+                    f"16-B QM31 leaves, fold to log {args.final_log}, 64 queries, proof bytes on device",
+        "instances": len(logs),
+        "total_codeword_elems": int(sum(1 << lg for lg in logs)),
+        "schedule": {"treelet_log": args.treelet_log, "group_log": args.group_log, "threads": args.threads, "graph": True},
+        "l2": "inputs larger than L2 (codewords and trees of one superstep are several GB)",
+        "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))} (no data-path collective)",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--lo", type=int, default=10)
+    ap.add_argument("--hi", type=int, default=22)
+    ap.add_argument("--final-log", type=int, default=6)
+    ap.add_argument("--treelet-log", type=int, default=9)
+    ap.add_argument("--group-log", type=int, default=9)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--cpu-budget-elems", type=int, default=1 << 21)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world, rank, local, dist = dist_setup(args)
+    logs, rounds, counts, offsets = workload(args.instances, args.lo, args.hi, args.final_log)
+    rows = coefficient_rows(counts)
+    pubs = public_digests(len(logs))
+    if args.impl == "reference":
+        run_reference(args, logs, rounds, counts, offsets, rows, pubs, world, rank, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import apple_b200 as azk
+
+    ctx = azk.Context(local)
+    sched = dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1)
+    batch = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=sched)
+    work = batch.work()
+    elems = int(sum(1 << lg for lg in logs))
+
+    # pinned host staging for the end-to-end path
+    import torch
+
+    pinned = torch.empty((rows.shape[0], 4), dtype=torch.int32, pin_memory=True)
+    pinned.numpy().view(np.uint32)[:] = rows
+    host_rows = pinned.numpy().view(np.uint32)
+    proof_host = torch.empty(max(1, batch.proof_total), dtype=torch.uint8, pin_memory=True)
+
+    batch.upload(host_rows, offsets, counts)
+    for _ in range(args.warmup):
+        batch.prove(pubs)
+
+    # ---- device-timed batched superstep ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(dist)
+    gpu_times = []
+    for _ in range(args.steps):
+        st = batch.prove(pubs)
+        gpu_times.append(st.gpu_s)
+    barrier(dist)
+    clk = clocks.stop()
+    t_dev = max_over_ranks(dist, sum(gpu_times), local)
+    value = world * elems * args.steps / t_dev
+    print(f"[bench] batched steps: {[round(1000 * g, 2) for g in gpu_times]} ms", file=sys.stderr, flush=True)
+
+    # ---- per-stage profile (events inside the captured graph) ----
+    batch.set_profiling(True)
+    batch.prove(pubs)
+    prof = batch.profile()
+    batch.set_profiling(False)
+
+    # ---- end to end through the C ABI from pinned host memory ----
+    h2d = int(sum(counts)) * 16
+    d2h = batch.proof_total
+    e2e_times = []
+    import ctypes
+
+    for _ in range(max(1, args.steps // 2)):
+        t0 = time.perf_counter()
+        batch.upload(host_rows, offsets, counts)
+        batch.prove(pubs)
+        azk._capi.check(azk.lib().azk_batch_download_proofs(batch._h, ctypes.c_void_p(proof_host.data_ptr()), batch.proof_total), ctx.handle)
+        e2e_times.append(time.perf_counter() - t0)
+    t_e2e = max_over_ranks(dist, statistics.median(e2e_times), local)
+    e2e_value = world * elems / t_e2e
+
+    # ---- plain per-instance form, same instances ----
+    plain_times = []
+    for _ in range(args.plain_steps):
+        st = batch.prove(pubs, plain=True)
+        plain_times.append(st.gpu_s)
+    t_plain = max_over_ranks(dist, statistics.median(plain_times), local)
+    print(f"[bench] plain: {[round(1000 * g, 2) for g in plain_times]} ms, e2e {[round(1000 * g, 2) for g in e2e_times]} ms, profile {prof}",
+          file=sys.stderr, flush=True)
+    plain_value = world * elems / t_plain
+
+    # ---- rooflines ----
+    int_ops = azk.probe_int_issue(ctx)
+    perm_peak = int_ops / 4320.0
+    tree_rate = work["tree_permutations"] / prof["tree_s"] if prof["tree_s"] > 0 else 0.0
+    tree_launches = max(1, max(rounds))
+    hbm_gbs, hbm_kind = measured_peaks()
+    fft_gbs = work["fft_bytes"] / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
+    traffic = profile_traffic()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            from oracle import pyoracle as O
+
+            e, dt, k = cpu_sample(logs, rounds, counts, offsets, rows, pubs, args.cpu_budget_elems)
+            cpu = {"value": e / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                   "sample": f"first {k} instances of the workload (sum 2^logN = {e}), FFT + prove with the C++ oracle ({dt:.1f} s)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/u64 (M31/QM31 field, Keccak lanes)", "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
+            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": 1000 * t_plain, "batched_over_plain": value / plain_value},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e},
+            "roofline": {
+                "bound": "int32-issue", "kernel": "tree_tiles_kernel (fold + leaf hash + treelet + upper tree + transcript)",
+                "achieved": tree_rate / 1e9, "peak": perm_peak / 1e9, "unit": "Gperm/s", "frac": tree_rate / perm_peak if perm_peak else None,
+                "traffic": traffic.get("tree_bytes_per_launch"),
+                "peak_source": f"probe: {int_ops / 1e12:.2f} T LOP3+SHF ops/s / 4320 ops per Keccak-f",
+                "algorithmic": f"{work['tree_permutations']} permutations per superstep over {tree_launches} launches",
+            },
+            "roofline_hbm": {
+                "bound": "hbm", "kernel": "fft_pass_kernel", "achieved": fft_gbs, "peak": hbm_gbs, "unit": "GB/s",
+                "frac": fft_gbs / hbm_gbs if hbm_gbs else None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_kind})",
+                "algorithmic": "16N read + 16N write + 4(N-1) twiddle bytes per codeword",
+                "traffic": traffic.get("fft_bytes_per_launch"),
+            },
+            "stage_seconds": prof,
+            "gpu_launches": work["launches"] * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "proof_bytes_per_step": batch.proof_total,
+        }
+        print(json.dumps(line), flush=True)
+    del batch
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -163,6 +163,10 @@ azk_status azk_qm31_transcript_challenges(azk_ctx* ctx, uint64_t input_count, co
 azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t log_size, const uint32_t* evaluations, uint32_t log_blowup, uint32_t queries,
                                         uint32_t grinding_bits, const uint8_t public_digest[32], uint32_t rounds, uint32_t* final_out,
                                         uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* Sustained LOP3 + SHF (funnel shift) issue rate of the device, 32-bit ops per
+ * second, from a probe kernel of independent chains: the integer roofline of
+ * the Keccak-bound kernels (no counterpart in the reference). */
+azk_status azk_probe_int_issue(azk_ctx* ctx, double* ops_per_second);
 /* Canonicality gate (QM31CanonicalityCheck.swift:11-117): *non_canonical = 1 if any word >= p. */
 azk_status azk_check_canonical(azk_ctx* ctx, const void* dev_words, uint64_t word_count, uint32_t* non_canonical);
 
@@ -217,6 +221,15 @@ azk_status azk_batch_proof_sizes(azk_batch* b, uint64_t* sizes, uint64_t* total)
 /* Proof bytes of all instances, concatenated in instance order. */
 azk_status azk_batch_download_proofs(azk_batch* b, uint8_t* out, uint64_t capacity);
 azk_status azk_batch_trace(azk_batch* b, uint32_t index, uint8_t* commitments, uint32_t* challenges, uint32_t* final_layer, uint32_t* query_pairs);
+/* Per-stage CUDA-event timing of the next proves (event pairs on the batch's own
+ * stream around each stage; profiled proves launch the graph's kernel sequence
+ * eagerly): seconds4 = {FFT passes, per-round
+ * fold+hash+transcript kernels, final folds, transcript/query/emission}. */
+azk_status azk_batch_set_profiling(azk_batch* b, int enabled);
+azk_status azk_batch_profile(azk_batch* b, double* seconds4);
+/* Algorithmic work of one superstep: Keccak-f permutations of the tree kernels,
+ * single-pass FFT bytes, final-fold bytes, and kernel launches per superstep. */
+azk_status azk_batch_work(azk_batch* b, uint64_t* tree_permutations, uint64_t* fft_bytes, uint64_t* fold_bytes, uint32_t* launches);
 void azk_batch_destroy(azk_batch* b);
 
 #ifdef __cplusplus
