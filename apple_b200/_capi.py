@@ -88,6 +88,7 @@ PROTOTYPES = {
     "azk_merkle_plan_clear": (I32, [P]),
     "azk_merkle_plan_destroy": (None, [P]),
     "azk_merkle_commit_prehashed": (I32, [P, P, U64, P, STATS]),
+    "azk_merkle_root_noalloc": (I32, [P, U64, U64, U64, P, P]),
     "azk_circle_domain_points": (I32, [P, U32, P]),
     "azk_circle_fft_twiddles": (I32, [P, U32, P]),
     "azk_circle_inverse_layers": (I32, [P, U32, U32, P]),

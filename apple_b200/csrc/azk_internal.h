@@ -173,6 +173,7 @@ struct LaunchCfg {
 
 cudaError_t launch_int_issue_probe(int sm_count, cudaStream_t s, uint32_t* d_sink, double* ops_per_launch, uint32_t* blocks_out);
 cudaError_t prepare_tree_kernels();
+cudaError_t launch_tree_direct_raw(const TreeJob& job, cudaStream_t s);
 cudaError_t prepare_fft_kernels();
 cudaError_t launch_keccak_permute(const uint8_t* in, uint64_t in_stride, uint8_t* out, uint64_t out_stride, uint64_t count,
                                   uint32_t threads, cudaStream_t s);

@@ -97,18 +97,16 @@ __device__ void root_action(const TreeJob& job, const uint64_t* rootp) {
   for (int k = 0; k < 4; k++) job.challenge_out[k] = ch[k];
 }
 
+// One tile of one job: leaf digests, treelet, then the last-arriver climb.
 template <uint32_t KIND, int THREADS>
-__global__ void __launch_bounds__(THREADS) tree_tiles_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work) {
+__device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_t tile) {
   extern __shared__ __align__(16) uint64_t sm[];
   __shared__ uint32_t s_last;
   __shared__ uint32_t s_ch[4];
-  const uint2 w = work[blockIdx.x];
-  const TreeJob& job = jobs[w.x];
   const uint32_t tl = job.tile_log < job.logn ? job.tile_log : job.logn;
   const uint32_t T = 1u << tl;
   uint64_t* bufA = sm;           // T digests
   uint64_t* bufB = sm + 4 * T;   // T/2 digests
-  const uint64_t tile = w.y;
 
   uint32_t ch[4] = {0, 0, 0, 0};
   if constexpr (KIND == kLeafFold) {
@@ -164,6 +162,18 @@ __global__ void __launch_bounds__(THREADS) tree_tiles_kernel(const TreeJob* __re
   if (threadIdx.x == 0) root_action(job, res);
 }
 
+template <uint32_t KIND, int THREADS>
+__global__ void __launch_bounds__(THREADS) tree_tiles_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  const uint2 w = work[blockIdx.x];
+  tree_tile_body<KIND, THREADS>(jobs[w.x], w.y);
+}
+
+// Single job passed by value, tile = blockIdx.x: needs no job or work-list buffer.
+template <uint32_t KIND, int THREADS>
+__global__ void __launch_bounds__(THREADS) tree_direct_kernel(const TreeJob job) {
+  tree_tile_body<KIND, THREADS>(job, blockIdx.x);
+}
+
 static constexpr int kMaxTreeSmem = 48 << 11;  // 2^11 digests + 2^10 digests
 
 template <uint32_t KIND>
@@ -209,6 +219,16 @@ cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_
     case kLeafDigest: return launch_kind<kLeafDigest>(d_jobs, d_work, nwork, max_tile_log, threads, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// One raw-leaf tree, job by value, 256 threads, treelets of at most 2^9 leaves
+// (24 KiB of dynamic shared memory: under the default limit, no opt-in needed).
+cudaError_t launch_tree_direct_raw(const TreeJob& job, cudaStream_t s) {
+  if (job.tile_log > 9 || (job.logn > 0 && job.tile_log == 0)) return cudaErrorInvalidValue;
+  uint32_t tl = job.tile_log < job.logn ? job.tile_log : job.logn;
+  unsigned tiles = 1u << (job.logn - tl);
+  tree_direct_kernel<kLeafRaw, 256><<<tiles, 256, (size_t)48 << tl, s>>>(job);
+  return cudaGetLastError();
 }
 
 // Sibling paths for leaves of a committed tree: out[k][level] = digest of the

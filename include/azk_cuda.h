@@ -119,6 +119,23 @@ void azk_merkle_plan_destroy(azk_merkle_plan* plan);
  * SHA3PrehashedLeavesMerkleCommitPlan, :314-524). */
 azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* host_digests, uint64_t digest_bytes, uint8_t root_out[32], azk_stats* stats);
 
+/* Merkle root of raw leaves with no device allocation: no counterpart in the
+ * reference.  For callers that may not call cudaMalloc (a host that gives the
+ * library a fixed memory budget, code that must not risk the implicit device
+ * synchronisation of cudaMalloc/cudaFree, or a loop that cannot afford an
+ * allocation failure).  All scratch lives in one fixed array inside the library's
+ * device image (2 MiB + 768 bytes per device, held until the process exits); the caller
+ * passes the leaves and a 32-byte root buffer on the device.  At most 65536
+ * leaves (leaf_length <= 136, leaf_stride >= leaf_length); larger counts are
+ * rejected with AZK_ERR_INVALID_INPUT_LAYOUT.  Work is queued on `stream`
+ * (NULL = default stream) and the call returns without waiting.  The first call on
+ * a device resolves the array's device address, so make it before any stream
+ * capture.  The array is shared by every call on a device: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller.  Errors are
+ * reported through azk_last_error_message(NULL). */
+azk_status azk_merkle_root_noalloc(const void* dev_leaves, uint64_t leaf_count, uint64_t leaf_stride, uint64_t leaf_length, void* dev_root,
+                                   void* stream);
+
 /* ---- circle domain materialisation (CircleDomainMaterializationPlan.swift:52-219) ----
  * Canonical bit-reversed domain of size 2^log_size (1..26).  Points in storage
  * order as (x, y); FFT twiddles (N - 1 words, stage s at N - (N >> s)); inverse
