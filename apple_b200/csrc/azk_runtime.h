@@ -164,8 +164,8 @@ const azk_ctx::Domain& domain_tables(azk_ctx* ctx, uint32_t logn);
 
 // Resolved hashing schedule.
 struct Sched {
-  uint32_t tile_log = 10;
-  uint32_t group_log = 10;
+  uint32_t tile_log = 12;
+  uint32_t group_log = 12;
   uint32_t threads = 256;
   bool graph = true;
 };

@@ -58,7 +58,7 @@ __device__ __forceinline__ void leaf_digest(const TreeJob& job, uint64_t leaf, c
 // storing each level into the job's inner nodes.  Returns the buffer holding the
 // single remaining digest.  `level`/`idx0`: level and first node index of the
 // input digests.
-__device__ uint64_t* reduce_levels(uint64_t* a, uint64_t* b, uint32_t count, const TreeJob& job, uint32_t level, uint64_t idx0) {
+__device__ __noinline__ uint64_t* reduce_levels(uint64_t* a, uint64_t* b, uint32_t count, const TreeJob& job, uint32_t level, uint64_t idx0) {
   uint64_t* src = a;
   uint64_t* dst = b;
   while (count > 1) {
@@ -82,7 +82,7 @@ __device__ uint64_t* reduce_levels(uint64_t* a, uint64_t* b, uint32_t count, con
   return src;
 }
 
-__device__ void root_action(const TreeJob& job, const uint64_t* rootp) {
+__device__ __noinline__ void root_action(const TreeJob& job, const uint64_t* rootp) {
   uint64_t root[4];
   ld_dig(rootp, root);
   if (job.root_out) st_dig(job.root_out, root);
@@ -97,7 +97,120 @@ __device__ void root_action(const TreeJob& job, const uint64_t* rootp) {
   for (int k = 0; k < 4; k++) job.challenge_out[k] = ch[k];
 }
 
+// Sets up the sponge input of one leaf (message lanes, suffix and end padding)
+// and returns how many permutations it takes (2 for a 136-byte raw leaf).
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t leaf_setup(const TreeJob& job, uint64_t leaf, const uint32_t (&ch)[4], uint64_t (&a)[25]) {
+  if constexpr (KIND == kLeafQM31 || KIND == kLeafFold) {
+    uint4 v;
+    if constexpr (KIND == kLeafQM31) {
+      v = __ldg(job.layer + leaf);
+    } else {
+      uint4 p = __ldg(job.layer + 2 * leaf), q = __ldg(job.layer + 2 * leaf + 1);
+      qm31 r = fri_fold_pair(qm31{p.x, p.y, p.z, p.w}, qm31{q.x, q.y, q.z, q.w}, __ldg(job.inv + leaf), qm31{ch[0], ch[1], ch[2], ch[3]});
+      v = make_uint4(r.a, r.b, r.c, r.d);
+      job.out_layer[leaf] = v;
+    }
+    a[0] = (uint64_t)v.x | ((uint64_t)v.y << 32);
+    a[1] = (uint64_t)v.z | ((uint64_t)v.w << 32);
+    a[2] = 0x06;
+    a[16] = kPadEnd;
+    return 1;
+  } else {
+    xor_message(a, job.raw + leaf * job.stride, job.len, job.aligned8 != 0);
+    if (job.len == 136) return 2;
+    const uint32_t lane = job.len >> 3;
+    const uint64_t v = (uint64_t)job.suffix << (8 * (job.len & 7));
+#pragma unroll
+    for (uint32_t i = 0; i < 17; i++)
+      if (i == lane) a[i] ^= v;
+    a[16] ^= kPadEnd;
+    return 1;
+  }
+}
+
+// Subtrees of height h = min(2, log2(items)), one per thread.  Items are the
+// tile's leaves, or (from_nodes) digests already in the tree at level `base`.  The
+// subtree's inner nodes are stored (levels base+1 .. base+h, first node idx0 >> l)
+// and its root written to `out` in shared memory.  A 4-item subtree runs as a
+// 7-step loop around ONE permutation site (leaf, leaf, pair, leaf, leaf, pair,
+// pair), which keeps the kernel's code small enough for the instruction cache.
+template <uint32_t KIND, int THREADS>
+__device__ __noinline__ uint32_t subtree_phase(const TreeJob& job, uint32_t items, uint32_t base, uint64_t idx0, const uint64_t* nodes, bool from_nodes,
+                                               uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint64_t* out) {
+  const uint32_t ch[4] = {c0, c1, c2, c3};
+  const uint32_t h = items >= 4 ? 2u : (items >= 2 ? 1u : 0u);
+  const uint32_t groups = items >> h;
+  const bool item_is_digest = from_nodes || KIND == kLeafDigest;
+  const uint64_t* digests = from_nodes ? nodes : reinterpret_cast<const uint64_t*>(job.raw) + 4 * idx0;
+  uint64_t* l1 = job.inner + 4 * (inner_offset(job.logn, base + 1) + (idx0 >> 1));
+  uint64_t* l2 = job.inner + 4 * (inner_offset(job.logn, base + 2) + (idx0 >> 2));
+  // step k: item index within the subtree (leaf steps) and the step's kind
+  //   k:     0  1  2  3  4  5  6        (h == 2)
+  //   item:  0  1  -  2  3  -  -
+  const uint32_t steps = h == 2 ? 7 : (h == 1 ? 3 : 1);
+  for (uint32_t j = threadIdx.x; j < groups; j += THREADS) {
+    uint64_t X[4] = {0, 0, 0, 0}, Y[4] = {0, 0, 0, 0}, P[4] = {0, 0, 0, 0};
+#pragma unroll 1
+    for (uint32_t k = 0; k < steps; k++) {
+      const bool pair = (h == 2) ? (k == 2 || k == 5 || k == 6) : (h == 1 && k == 2);
+      const uint32_t item = k < 2 ? k : k - 1;  // leaf steps only (h == 2: k = 0, 1, 3, 4)
+      const uint64_t leaf = idx0 + (uint64_t)j * (1u << h) + item;
+      uint64_t d[4];
+      if (!pair && item_is_digest) {
+        ld_dig_cg(digests + 4 * ((uint64_t)j * (1u << h) + item), d);
+      } else {
+        uint64_t a[25];
+#pragma unroll
+        for (int i = 0; i < 25; i++) a[i] = 0;
+        uint32_t perms = 1;
+        if (pair) {
+          const bool top = (h == 2 && k == 6);
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            a[i] = top ? P[i] : X[i];
+            a[4 + i] = Y[i];
+          }
+          a[8] = 0x06;
+          a[16] = kPadEnd;
+        } else {
+          perms = leaf_setup<KIND>(job, leaf, ch, a);
+        }
+#pragma unroll 1
+        for (uint32_t b = 0; b < perms; b++) {
+          if (b == 1) {
+            a[0] ^= job.suffix;
+            a[16] ^= kPadEnd;
+          }
+          keccak_f1600(a);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) d[i] = a[i];
+        if (!pair && job.leaf_digests) st_dig(job.leaf_digests + 4 * leaf, d);
+      }
+      // route the step's digest
+      const bool toX = (h == 2) ? (k == 0 || k == 3) : (h == 1 && k == 0);
+      const bool toY = (h == 2) ? (k == 1 || k == 4 || k == 5) : (h == 1 && k == 1);
+      const bool toP = (h == 2 && k == 2);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        X[i] = toX ? d[i] : X[i];
+        Y[i] = toY ? d[i] : Y[i];
+        P[i] = toP ? d[i] : P[i];
+      }
+      if (h == 2 && k == 2) st_dig(l1 + 8 * j, d);
+      if (h == 2 && k == 5) st_dig(l1 + 8 * j + 4, d);
+      if (h == 2 && k == 6) st_dig(l2 + 4 * j, d);
+      if (h == 1 && k == 2) st_dig(l1 + 4 * j, d);
+      if (k + 1 == steps) st_dig(out + 4 * j, d);
+    }
+  }
+  __syncthreads();
+  return h;
+}
+
 // One tile of one job: leaf digests, treelet, then the last-arriver climb.
+// Shared memory: 2^(tl-2) digests + half as many for the ping-pong (12 bytes per leaf).
 template <uint32_t KIND, int THREADS>
 __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_t tile) {
   extern __shared__ __align__(16) uint64_t sm[];
@@ -105,8 +218,9 @@ __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_
   __shared__ uint32_t s_ch[4];
   const uint32_t tl = job.tile_log < job.logn ? job.tile_log : job.logn;
   const uint32_t T = 1u << tl;
-  uint64_t* bufA = sm;           // T digests
-  uint64_t* bufB = sm + 4 * T;   // T/2 digests
+  const uint32_t Q = T >= 4 ? T / 4 : 1;
+  uint64_t* bufA = sm;           // Q digests
+  uint64_t* bufB = sm + 4 * Q;   // Q/2 digests
 
   uint32_t ch[4] = {0, 0, 0, 0};
   if constexpr (KIND == kLeafFold) {
@@ -116,17 +230,11 @@ __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_
     for (int k = 0; k < 4; k++) ch[k] = s_ch[k];
   }
 
-  // 1) leaf digests of this tile
-  for (uint32_t i = threadIdx.x; i < T; i += THREADS) {
-    uint64_t leaf = tile * T + i;
-    uint64_t d[4];
-    leaf_digest<KIND>(job, leaf, ch, d);
-    st_dig(bufA + 4 * i, d);
-    if (job.leaf_digests) st_dig(job.leaf_digests + 4 * leaf, d);
-  }
-  __syncthreads();
+  // 1) leaf digests and the two lowest levels of this tile, per thread
+  const uint64_t first = tile * T;
+  uint32_t h = subtree_phase<KIND, THREADS>(job, T, 0, first, nullptr, false, ch[0], ch[1], ch[2], ch[3], bufA);
   // 2) treelet
-  uint64_t* res = reduce_levels(bufA, bufB, T, job, 0, tile * T);
+  uint64_t* res = reduce_levels(bufA, bufB, T >> h, job, h, first >> h);
   // 3) climb: last arriver of each group continues
   uint32_t level = tl;
   uint64_t idx = tile;
@@ -148,13 +256,8 @@ __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_
     if (!s_last) return;
     __threadfence();
     const uint64_t* lv = job.inner + 4 * (inner_offset(job.logn, level) + gidx * G);
-    for (uint32_t i = threadIdx.x; i < G; i += THREADS) {
-      uint64_t d[4];
-      ld_dig_cg(lv + 4 * i, d);
-      st_dig(bufA + 4 * i, d);
-    }
-    __syncthreads();
-    res = reduce_levels(bufA, bufB, G, job, level, gidx * G);
+    uint32_t hg = subtree_phase<KIND, THREADS>(job, G, level, gidx * G, lv, true, 0, 0, 0, 0, bufA);
+    res = reduce_levels(bufA, bufB, G >> hg, job, level + hg, (gidx * G) >> hg);
     cnt_off += (1ull << (job.logn - level)) >> glog;
     level += glog;
     idx = gidx;
@@ -163,18 +266,19 @@ __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_
 }
 
 template <uint32_t KIND, int THREADS>
-__global__ void __launch_bounds__(THREADS) tree_tiles_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work) {
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) tree_tiles_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work) {
   const uint2 w = work[blockIdx.x];
   tree_tile_body<KIND, THREADS>(jobs[w.x], w.y);
 }
 
 // Single job passed by value, tile = blockIdx.x: needs no job or work-list buffer.
 template <uint32_t KIND, int THREADS>
-__global__ void __launch_bounds__(THREADS) tree_direct_kernel(const TreeJob job) {
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) tree_direct_kernel(const TreeJob job) {
   tree_tile_body<KIND, THREADS>(job, blockIdx.x);
 }
 
-static constexpr int kMaxTreeSmem = 48 << 11;  // 2^11 digests + 2^10 digests
+static constexpr int kMaxTreeLog = 13;
+static constexpr int kMaxTreeSmem = 12 << kMaxTreeLog;  // 2^11 digests + 2^10 digests
 
 template <uint32_t KIND>
 static cudaError_t prepare_kind() {
@@ -198,7 +302,7 @@ cudaError_t prepare_tree_kernels() {
 
 template <uint32_t KIND>
 static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t threads, cudaStream_t s) {
-  size_t smem = (size_t)48 << max_tile_log;  // T digests + T/2 digests
+  size_t smem = max_tile_log >= 2 ? ((size_t)12 << max_tile_log) : 48;  // T/4 digests + T/8 digests
   if (threads == 128)
     tree_tiles_kernel<KIND, 128><<<nwork, 128, smem, s>>>(d_jobs, d_work);
   else if (threads == 512)
@@ -211,7 +315,7 @@ static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint3
 cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t kind, uint32_t threads,
                              cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
-  if (max_tile_log > 11) return cudaErrorInvalidValue;
+  if (max_tile_log > kMaxTreeLog) return cudaErrorInvalidValue;
   switch (kind) {
     case kLeafRaw: return launch_kind<kLeafRaw>(d_jobs, d_work, nwork, max_tile_log, threads, s);
     case kLeafQM31: return launch_kind<kLeafQM31>(d_jobs, d_work, nwork, max_tile_log, threads, s);
@@ -227,7 +331,7 @@ cudaError_t launch_tree_direct_raw(const TreeJob& job, cudaStream_t s) {
   if (job.tile_log > 9 || (job.logn > 0 && job.tile_log == 0)) return cudaErrorInvalidValue;
   uint32_t tl = job.tile_log < job.logn ? job.tile_log : job.logn;
   unsigned tiles = 1u << (job.logn - tl);
-  tree_direct_kernel<kLeafRaw, 256><<<tiles, 256, (size_t)48 << tl, s>>>(job);
+  tree_direct_kernel<kLeafRaw, 256><<<tiles, 256, tl >= 2 ? ((size_t)12 << tl) : 48, s>>>(job);
   return cudaGetLastError();
 }
 

@@ -41,7 +41,7 @@ Sched azk::resolve_schedule(const azk_schedule* s) {
     if (s->threads) r.threads = s->threads;
     r.graph = s->use_graph != 0;
   }
-  require(r.tile_log >= 1 && r.tile_log <= 11, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 1...11");
+  require(r.tile_log >= 1 && r.tile_log <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 1...13");
   if (r.group_log > r.tile_log) r.group_log = r.tile_log;
   require(r.group_log >= 1, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "group_log must be >= 1");
   require(r.threads == 128 || r.threads == 256 || r.threads == 512, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "threads must be 128, 256 or 512");
@@ -472,7 +472,7 @@ azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t count, uint64_t stride,
     require(length <= 136, AZK_ERR_UNSUPPORTED_ONE_BLOCK_LENGTH,
             "Fixed-rate SHA3/Keccak path supports at most 136 bytes, got " + std::to_string(length) + ".");
     layout(stride >= length && count <= 0xFFFFFFFFull && stride <= 0xFFFFFFFFull);
-    require(treelet_log <= 11, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 0...11");
+    require(treelet_log <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 0...13");
     AZK_CU(cudaSetDevice(ctx->device));
     auto p = std::make_unique<azk_merkle_plan>();
     p->ctx = ctx;
@@ -480,7 +480,7 @@ azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t count, uint64_t stride,
     p->stride = stride;
     p->length = length;
     p->logn = ilog2(count);
-    uint32_t tl = treelet_log ? treelet_log : 10;
+    uint32_t tl = treelet_log ? treelet_log : 12;
     if (tl > p->logn) tl = p->logn;
     if (tl == 0 && p->logn > 0) tl = 1;
     p->tile_log = tl;

@@ -97,7 +97,7 @@ void azk_hash_plan_destroy(azk_hash_plan* plan);
 
 /* ---- SHA3 Merkle commitment over raw leaves (MerkleCommitter.swift:152-223, 526-1063) ----
  * leaf_count a power of two, leaf_length <= 136, leaf_stride >= leaf_length.
- * treelet_log: 0 = automatic, else leaves per CTA treelet = 2^treelet_log (1..11).
+ * treelet_log: 0 = automatic, else leaves per CTA treelet = 2^treelet_log (1..13).
  * The tree stays resident after a commit, so openings gather sibling paths
  * without recomputing it. */
 azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t leaf_count, uint64_t leaf_stride, uint64_t leaf_length, uint32_t treelet_log,
@@ -191,7 +191,7 @@ azk_status azk_check_canonical(azk_ctx* ctx, const void* dev_words, uint64_t wor
  * CircleCodewordPCSFRIProverV1, CircleCodeword.swift:920-1419) ----
  * Produces CirclePCSFRIProofCodecV1 bytes (CircleProofFormat.swift:478-593). */
 typedef struct azk_schedule {
-  uint32_t treelet_log;   /* leaves per CTA treelet = 2^treelet_log (1..11); 0 = default */
+  uint32_t treelet_log;   /* leaves per CTA treelet = 2^treelet_log (1..13); 0 = default */
   uint32_t group_log;     /* upper-level group size (1..treelet_log); 0 = default */
   uint32_t threads;       /* threads per CTA for hashing kernels: 128, 256 or 512; 0 = default */
   uint32_t use_graph;     /* batched form: capture the superstep in a CUDA graph */

@@ -27,10 +27,10 @@ def test_golden_roots(ctx, golden):
         assert azk.SHA3RawLeavesMerkleCommitPlan(ctx, 16384, length, length).commit(leaves).hex() == want, length
 
 
-@pytest.mark.parametrize("treelet_log", [1, 3, 4, 6, 8, 10, 11])
+@pytest.mark.parametrize("treelet_log", [1, 2, 3, 4, 6, 8, 10, 11, 12, 13])
 @pytest.mark.parametrize("length,stride", [(0, 5), (64, 72), (128, 136), (135, 144), (136, 144), (32, 40)])
 def test_treelet_depths_and_strides(ctx, oracle, treelet_log, length, stride):
-    count = 256 if treelet_log < 9 else 4096
+    count = 256 if treelet_log < 9 else (4096 if treelet_log < 12 else 32768)
     leaves = G.make_leaves(count, stride, length, salt=length + treelet_log)
     plan = azk.SHA3RawLeavesMerkleCommitPlan(ctx, count, stride, length, treelet_log=treelet_log)
     assert plan.commit(leaves) == oracle.merkle_root(leaves, count, stride, length)

@@ -71,7 +71,8 @@ def test_prover_matches_oracle(ctx, oracle, log_size, rounds, queries):
 
 
 @pytest.mark.parametrize("schedule", [dict(treelet_log=1, group_log=1, threads=128), dict(treelet_log=5, group_log=3, threads=256),
-                                      dict(treelet_log=11, group_log=11, threads=512), dict(treelet_log=8, group_log=2, threads=256)])
+                                      dict(treelet_log=11, group_log=11, threads=512), dict(treelet_log=8, group_log=2, threads=256),
+                                      dict(treelet_log=13, group_log=13, threads=256), dict(treelet_log=2, group_log=1, threads=512)])
 def test_prover_schedules_do_not_change_bytes(ctx, oracle, schedule):
     rng = np.random.default_rng(99)
     log_size, rounds = 15, 9
