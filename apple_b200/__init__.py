@@ -20,6 +20,7 @@ from .plans import (  # noqa: F401
     CircleCodewordPlan,
     CirclePCSFRIProver,
     Context,
+    ProofServer,
     KeccakF1600PermutationPlan,
     SHA3FixedOneBlockHashPlan,
     SHA3RawLeavesMerkleCommitPlan,
@@ -34,4 +35,5 @@ from .plans import (  # noqa: F401
     qm31_fold,
     qm31_merkle_fold_chain,
     qm31_transcript_challenges,
+    sumcheck_prove,
 )

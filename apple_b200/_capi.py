@@ -37,7 +37,8 @@ class Stats(ctypes.Structure):
 
 
 class Schedule(ctypes.Structure):
-    _fields_ = [("treelet_log", ctypes.c_uint32), ("group_log", ctypes.c_uint32), ("threads", ctypes.c_uint32), ("use_graph", ctypes.c_uint32)]
+    _fields_ = [("treelet_log", ctypes.c_uint32), ("group_log", ctypes.c_uint32), ("threads", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
+                ("layer_treelet", ctypes.c_uint8 * 32)]
 
 
 def library_path() -> str:
@@ -122,6 +123,24 @@ PROTOTYPES = {
     "azk_batch_work": (I32, [P, U64P, U64P, U64P, U32P]),
     "azk_batch_destroy": (None, [P]),
     "azk_probe_int_issue": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
+    "azk_sumcheck_prove": (I32, [P, P, U64, P, P, P, U32P, U32P, P, STATS]),
+    "azk_server_create": (I32, [P, U64, U32, SCHED, PP]),
+    "azk_server_submit_pcs": (I32, [P, U32, U32, U32, U32, P, U64, P, U64P]),
+    "azk_server_submit_sumcheck": (I32, [P, P, U64, U64P]),
+    "azk_server_poll": (I32, [P, U64, IP, ctypes.POINTER(ctypes.c_double), P, U64P]),
+    "azk_server_release": (I32, [P, U64]),
+    "azk_server_wait_all": (I32, [P]),
+    "azk_server_stats": (I32, [P, U64P, U64P, ctypes.POINTER(ctypes.c_double), U64P]),
+    "azk_server_destroy": (None, [P]),
+    "azk_tuner_time_tree": (I32, [P, U32, U32, U32, U32, U32, U32, U32, U32, ctypes.POINTER(ctypes.c_double)]),
+    "azk_mlp_create": (I32, [P, U32, P, U64, PP]),
+    "azk_mlp_param_count": (U64, [P]),
+    "azk_mlp_get_params": (I32, [P, P, U64]),
+    "azk_mlp_set_params": (I32, [P, P, U64]),
+    "azk_mlp_forward": (I32, [P, P, U64, P]),
+    "azk_mlp_gradients": (I32, [P, P, P, U64, ctypes.POINTER(ctypes.c_float), P]),
+    "azk_mlp_train": (I32, [P, P, P, U64, U32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+    "azk_mlp_destroy": (None, [P]),
 }
 
 

@@ -73,12 +73,24 @@ __host__ __device__ inline uint64_t inner_offset(uint32_t logn, uint32_t level) 
 // ---------------------------------------------------------------------------
 // FFT / fold jobs
 // ---------------------------------------------------------------------------
+// What the upload learned about one coefficient buffer (written on the device by
+// the input scan): `m31` = every coefficient below `count` has zero b, c, d limbs
+// (an M31 polynomial lifted to QM31); coefficients at index >= count are zero.
+// count == 0 means unknown (all N coefficients are read).
+struct InputInfo {
+  uint32_t m31;
+  uint32_t reserved;
+  uint64_t count;
+};
+
 struct FftJob {
   uint32_t logn;
-  uint32_t pass;       // this job's pass index (0 reads `in`; the last pass is the low stages)
-  const uint4* in;     // FFT-basis coefficients (read by the first pass)
-  uint4* out;          // codeword (bit-reversed order)
-  const uint32_t* tw;  // stage twiddles of the domain (N - 1 values)
+  uint32_t pass;             // this job's pass index (0 reads `in`; the last pass is the low stages)
+  const uint4* in;           // FFT-basis coefficients (read by the first pass)
+  uint4* out;                // codeword (bit-reversed order)
+  const uint32_t* tw;        // stage twiddles of the domain (N - 1 values)
+  uint32_t* narrow;          // N words of scratch between passes for M31 inputs (null: none)
+  const InputInfo* info;     // null: unknown input (QM31 arithmetic, all N coefficients read)
 };
 
 // Circle FFT pass geometry: the stages above bit 12 run first in chunks of at
@@ -185,6 +197,10 @@ cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, 
 cudaError_t launch_domain_tables(uint32_t logn, uint32_t* d_tw, uint32_t* d_inv, cudaStream_t s);
 cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
+// Canonicality gate over `count` QM31 coefficients; with `info`, also clears
+// info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
+// info = {1, 0, count} first).
+cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad, InputInfo* d_info, cudaStream_t s);
 cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s);
 cudaError_t launch_pcs_prefix(PcsInstance* d_inst, uint32_t ninst, cudaStream_t s);

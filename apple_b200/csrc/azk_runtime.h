@@ -104,6 +104,20 @@ struct DevBuf {
   ~DevBuf() { release(); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(p); }
 };
@@ -168,11 +182,15 @@ struct Sched {
   uint32_t group_log = 12;
   uint32_t threads = 256;
   bool graph = true;
+  uint8_t layer_tile[32] = {0};
 };
 Sched resolve_schedule(const azk_schedule* s);
-// Tile depth used for a tree of 2^logn leaves under a schedule.
+// Tile depth used for a tree of 2^logn leaves under a schedule (per-layer table
+// first, then the global depth), clamped to [1, logn].
 inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
-  uint32_t t = s.tile_log < logn ? s.tile_log : logn;
+  uint32_t t = (logn < 32 && s.layer_tile[logn]) ? s.layer_tile[logn] : s.tile_log;
+  if (t > logn) t = logn;
+  if (t == 0 && logn > 0) t = 1;
   return t;
 }
 

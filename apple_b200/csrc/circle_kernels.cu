@@ -80,46 +80,162 @@ __device__ __forceinline__ uint64_t fft_global_index(const FftPassGeom& g, uint6
   return (hi << (g.s_lo + g.m)) | ((uint64_t)row << g.s_lo) | (mid << g.c) | col;
 }
 
+// Shared-memory tile layout: the four limbs of the tile's QM31 values as four u32
+// arrays (an M31 tile uses only the first), then the tile's stage twiddles.  Stage
+// j of the pass (global stage s_lo + j) pairs local indices differing in bit j + c,
+// and its twiddle is tw[off(s) + (gi >> (s + 1))] = tw[off(s) + (hi << (m-1-j)) +
+// (row >> (j + 1))]: 2^(m-1-j) consecutive table entries per tile, staged at
+// stw + 2^m - 2^(m-j).
+__device__ __forceinline__ uint32_t fft_stw_offset(uint32_t m, uint32_t j) { return (1u << m) - (1u << (m - j)); }
+
+__device__ __forceinline__ void bfly_m31(uint32_t& l, uint32_t& r, uint32_t t) {
+  uint32_t rt = m31_mul(r, t);
+  uint32_t a = m31_add(l, rt);
+  r = m31_sub(l, rt);
+  l = a;
+}
+
+__device__ __forceinline__ void bfly_q(qm31& l, qm31& r, uint32_t t) {
+  qm31 rt = q_mul_m31(r, t);
+  qm31 a = q_add(l, rt);
+  r = q_sub(l, rt);
+  l = a;
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
-  extern __shared__ uint4 sv[];
+  extern __shared__ uint32_t fsm[];
   const uint2 w = work[blockIdx.x];
   const FftJob& job = jobs[w.x];
   const uint32_t logn = job.logn;
   const FftPassGeom g = fft_pass_geom(logn, job.pass);
   const uint32_t T = 1u << (g.m + g.c);
-  const uint4* src = job.pass == 0 ? job.in : job.out;
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) sv[L] = src[fft_global_index(g, w.y, L)];
+  const uint64_t N = 1ull << logn;
+  const bool first = job.pass == 0;
+  const bool last = job.pass == fft_high_chunks(logn);
+  const InputInfo* info = job.info;
+  const bool narrow = info != nullptr && job.narrow != nullptr && info->m31 != 0;
+  const uint64_t count = (info != nullptr && info->count != 0) ? info->count : N;
+  uint32_t* sa = fsm;
+  uint32_t* sb = sa + T;
+  uint32_t* sc = sb + T;
+  uint32_t* sd = sc + T;
+  uint32_t* stw = sd + T;
+
+  // this tile's twiddles, one coalesced run per stage
+  const uint32_t midbits = g.s_lo > g.c ? g.s_lo - g.c : 0;
+  const uint64_t hi = (uint64_t)w.y >> midbits;
+  for (uint32_t j = 0; j < g.m; j++) {
+    const uint32_t cnt = 1u << (g.m - 1 - j);
+    const uint32_t* src = job.tw + tw_offset(logn, g.s_lo + j) + (hi << (g.m - 1 - j));
+    uint32_t* dst = stw + fft_stw_offset(g.m, j);
+    for (uint32_t r = threadIdx.x; r < cnt; r += THREADS) dst[r] = __ldg(src + r);
+  }
+  // the tile (the first pass skips coefficients known to be zero)
+  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
+    const uint64_t gi = fft_global_index(g, w.y, L);
+    if (narrow) {
+      uint32_t v;
+      if (first)
+        v = gi < count ? __ldg(reinterpret_cast<const uint32_t*>(job.in) + 4 * gi) : 0u;
+      else
+        v = job.narrow[gi];
+      sa[L] = v;
+    } else {
+      uint4 v;
+      if (first)
+        v = gi < count ? __ldg(job.in + gi) : make_uint4(0u, 0u, 0u, 0u);
+      else
+        v = job.out[gi];
+      sa[L] = v.x;
+      sb[L] = v.y;
+      sc[L] = v.z;
+      sd[L] = v.w;
+    }
+  }
   __syncthreads();
-  for (int s = (int)(g.s_lo + g.m) - 1; s >= (int)g.s_lo; s--) {
-    const uint32_t p = (uint32_t)s - g.s_lo + g.c;
-    const uint64_t off = tw_offset(logn, (uint32_t)s);
-    for (uint32_t k = threadIdx.x; k < T / 2; k += THREADS) {
-      uint32_t L = ((k >> p) << (p + 1)) | (k & ((1u << p) - 1));
-      uint32_t R = L | (1u << p);
-      uint64_t gi = fft_global_index(g, w.y, L);
-      uint32_t t = __ldg(job.tw + off + (gi >> (s + 1)));
-      uint4 l = sv[L], r = sv[R];
-      qm31 rt = q_mul_m31(qm31{r.x, r.y, r.z, r.w}, t);
-      qm31 lv = qm31{l.x, l.y, l.z, l.w};
-      qm31 a = q_add(lv, rt), b = q_sub(lv, rt);
-      sv[L] = make_uint4(a.a, a.b, a.c, a.d);
-      sv[R] = make_uint4(b.a, b.b, b.c, b.d);
+
+  // stages two at a time (radix 4 in registers), then one more if m is odd
+  int j = (int)g.m - 1;
+  for (; j >= 1; j -= 2) {
+    const uint32_t p = (uint32_t)j + g.c;  // stage j pairs bit p, stage j-1 pairs bit p-1
+    const uint32_t* tw_j = stw + fft_stw_offset(g.m, (uint32_t)j);
+    const uint32_t* tw_j1 = stw + fft_stw_offset(g.m, (uint32_t)j - 1);
+    const uint32_t lowmask = (1u << (p - 1)) - 1;
+    for (uint32_t k = threadIdx.x; k < T / 4; k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << 2) | (k & lowmask);
+      const uint32_t e1 = e0 | (1u << (p - 1)), e2 = e0 | (1u << p), e3 = e2 | (1u << (p - 1));
+      const uint32_t row = e0 >> g.c;
+      const uint32_t t1 = tw_j[row >> (j + 1)];
+      const uint32_t t2a = tw_j1[row >> j], t2b = tw_j1[(row >> j) | 1u];
+      if (narrow) {
+        uint32_t v0 = sa[e0], v1 = sa[e1], v2 = sa[e2], v3 = sa[e3];
+        bfly_m31(v0, v2, t1);
+        bfly_m31(v1, v3, t1);
+        bfly_m31(v0, v1, t2a);
+        bfly_m31(v2, v3, t2b);
+        sa[e0] = v0;
+        sa[e1] = v1;
+        sa[e2] = v2;
+        sa[e3] = v3;
+      } else {
+        qm31 v0 = {sa[e0], sb[e0], sc[e0], sd[e0]}, v1 = {sa[e1], sb[e1], sc[e1], sd[e1]};
+        qm31 v2 = {sa[e2], sb[e2], sc[e2], sd[e2]}, v3 = {sa[e3], sb[e3], sc[e3], sd[e3]};
+        bfly_q(v0, v2, t1);
+        bfly_q(v1, v3, t1);
+        bfly_q(v0, v1, t2a);
+        bfly_q(v2, v3, t2b);
+        sa[e0] = v0.a, sb[e0] = v0.b, sc[e0] = v0.c, sd[e0] = v0.d;
+        sa[e1] = v1.a, sb[e1] = v1.b, sc[e1] = v1.c, sd[e1] = v1.d;
+        sa[e2] = v2.a, sb[e2] = v2.b, sc[e2] = v2.c, sd[e2] = v2.d;
+        sa[e3] = v3.a, sb[e3] = v3.b, sc[e3] = v3.c, sd[e3] = v3.d;
+      }
     }
     __syncthreads();
   }
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) job.out[fft_global_index(g, w.y, L)] = sv[L];
+  if (j == 0) {
+    const uint32_t p = g.c;
+    for (uint32_t k = threadIdx.x; k < T / 2; k += THREADS) {
+      const uint32_t L = ((k >> p) << (p + 1)) | (k & ((1u << p) - 1));
+      const uint32_t R = L | (1u << p);
+      const uint32_t t = stw[(L >> g.c) >> 1];
+      if (narrow) {
+        uint32_t l = sa[L], r = sa[R];
+        bfly_m31(l, r, t);
+        sa[L] = l;
+        sa[R] = r;
+      } else {
+        qm31 l = {sa[L], sb[L], sc[L], sd[L]}, r = {sa[R], sb[R], sc[R], sd[R]};
+        bfly_q(l, r, t);
+        sa[L] = l.a, sb[L] = l.b, sc[L] = l.c, sd[L] = l.d;
+        sa[R] = r.a, sb[R] = r.b, sc[R] = r.c, sd[R] = r.d;
+      }
+    }
+    __syncthreads();
+  }
+
+  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
+    const uint64_t gi = fft_global_index(g, w.y, L);
+    if (!narrow)
+      job.out[gi] = make_uint4(sa[L], sb[L], sc[L], sd[L]);
+    else if (last)
+      job.out[gi] = make_uint4(sa[L], 0u, 0u, 0u);
+    else
+      job.narrow[gi] = sa[L];
+  }
 }
 
-static constexpr size_t kFftSmem = (size_t)16 << kFftLowBits;  // 4096 QM31 values, 64 KiB
+// four limb arrays of 4096 values + 4095 staged twiddles
+static constexpr size_t kFftSmem = ((size_t)16 << kFftLowBits) + ((size_t)4 << kFftLowBits);
+static constexpr int kFftThreads = 512;
 
 cudaError_t prepare_fft_kernels() {
-  return cudaFuncSetAttribute(fft_pass_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmem);
+  return cudaFuncSetAttribute(fft_pass_kernel<kFftThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmem);
 }
 
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
-  fft_pass_kernel<256><<<nwork, 256, kFftSmem, s>>>(d_jobs, d_work);
+  fft_pass_kernel<kFftThreads><<<nwork, kFftThreads, kFftSmem, s>>>(d_jobs, d_work);
   return cudaGetLastError();
 }
 
@@ -502,6 +618,29 @@ __global__ void check_canonical_kernel(const uint32_t* __restrict__ w, uint64_t 
   bool bad = false;
   for (; i < n; i += (uint64_t)gridDim.x * blockDim.x) bad |= w[i] >= kP;
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+// Input scan of `count` QM31 coefficients: the canonicality gate, and whether any
+// b, c or d limb is nonzero (then the coefficients are not a lifted M31
+// polynomial and info->m31 is cleared).
+__global__ void scan_input_kernel(const uint4* __restrict__ in, uint64_t count, uint32_t* bad, InputInfo* info) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool b = false, upper = false;
+  for (; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 v = in[i];
+    b |= v.x >= kP || v.y >= kP || v.z >= kP || v.w >= kP;
+    upper |= (v.y | v.z | v.w) != 0;
+  }
+  if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+  if (info && __any_sync(0xffffffffu, upper) && (threadIdx.x & 31) == 0) atomicAnd(&info->m31, 0u);
+}
+
+cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad, InputInfo* d_info, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  uint64_t blocks = (count + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  scan_input_kernel<<<(unsigned)blocks, 256, 0, s>>>(d_in, count, d_bad, d_info);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_check_canonical(const uint32_t* d_words, uint64_t nwords, uint32_t* d_flag, cudaStream_t s) {

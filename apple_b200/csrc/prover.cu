@@ -9,9 +9,25 @@
 // and the whole superstep is a fixed launch sequence captured in a CUDA graph.
 // Plain form: the same kernels, launched instance after instance.
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
 
 #include "azk_field.cuh"
 #include "azk_runtime.h"
+
+namespace azk {
+struct SumcheckOut {
+  uint32_t claimed_sum;
+  uint32_t final_eval;
+  uint64_t digest[4];
+  uint32_t* r0;
+  uint32_t* r1;
+  uint32_t* challenges;
+};
+cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s);
+}  // namespace azk
 
 using namespace azk;
 
@@ -34,7 +50,7 @@ struct Engine {
   std::vector<uint64_t> off_input, off_layers, off_trees, off_tr, off_ch, off_cm, off_qp, off_claim, off_proof, off_cnt;
   std::vector<uint64_t> proof_len, proof_off;
   uint64_t proof_total = 0;
-  uint64_t off_inst = 0, off_flag = 0;
+  uint64_t off_inst = 0, off_flag = 0, off_info = 0;
 
   std::vector<PcsInstance> h_inst;
   // FFT
@@ -104,6 +120,24 @@ struct Engine {
 
   PcsInstance* d_inst() const { return arena.at<PcsInstance>(off_inst); }
   uint32_t* d_flag() const { return arena.at<uint32_t>(off_flag); }
+  InputInfo* d_info() const { return arena.at<InputInfo>(off_info); }
+
+  // Canonicality gate over the staged coefficients of every instance (counts[i]
+  // leading QM31 values; the rest are zero) and the FFT's input description:
+  // which instances are lifted M31 polynomials, how many coefficients are nonzero.
+  void scan_inputs(const std::vector<uint64_t>& counts) {
+    std::vector<InputInfo> h(cfg.size());
+    for (size_t i = 0; i < cfg.size(); i++) h[i] = InputInfo{1u, 0u, counts[i]};
+    AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s));
+    AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
+    for (size_t i = 0; i < cfg.size(); i++) AZK_CU(launch_scan_input(arena.at<uint4>(off_input[i]), counts[i], d_flag(), d_info() + i, s));
+    uint32_t f = 0;
+    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaStreamSynchronize(s));
+    layout(f == 0, "input contains a non-canonical field element");
+  }
+  // Inputs written by the caller through a device pointer: nothing known.
+  void forget_input(size_t i) { AZK_CU(cudaMemsetAsync(d_info() + i, 0, sizeof(InputInfo), s)); }
 
   void init(azk_ctx* c, const std::vector<InstanceCfg>& cf, const Sched& sc) {
     ctx = c;
@@ -146,6 +180,7 @@ struct Engine {
     for (size_t i = 0; i < n; i++) off_proof[i] = off_proofs + proof_off[i];
     off_inst = arena.reserve(sizeof(PcsInstance) * n);
     off_flag = arena.reserve(16);
+    off_info = arena.reserve(sizeof(InputInfo) * n);
     arena.commit("PCS.Arena");
     // counters and inputs start at zero
     AZK_CU(cudaMemsetAsync(arena.buf.p, 0, arena.used, s));
@@ -186,7 +221,8 @@ struct Engine {
     // ---- FFT ----
     std::vector<FftJob> tf;
     for (size_t i = 0; i < n; i++)
-      tf.push_back(FftJob{cfg[i].logn, 0, arena.at<uint4>(off_input[i]), arena.at<uint4>(off_layers[i]), h_inst[i].tw});
+      tf.push_back(FftJob{cfg[i].logn, 0, arena.at<uint4>(off_input[i]), arena.at<uint4>(off_layers[i]), h_inst[i].tw,
+                          arena.at<uint32_t>(off_trees[i]), d_info() + i});
     fft.build(tf);
     fft.upload(s);
 
@@ -538,7 +574,7 @@ azk_status azk_pcs_prover_prove_coefficients(azk_pcs_prover* p, const uint32_t* 
     uint4* in = e.arena.at<uint4>(e.off_input[0]);
     AZK_CU(cudaMemcpyAsync(in, coeffs, 16 * count, cudaMemcpyHostToDevice, e.s));
     if (count < N) AZK_CU(cudaMemsetAsync(in + count, 0, 16 * (N - count), e.s));
-    e.check_input_canonical(in, 4 * count);
+    e.scan_inputs({count});
     pcs_prove_common(p, true, pub, proof_out, false, proof_len, st, t);
   });
 }
@@ -553,9 +589,12 @@ azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* din, uin
     pcs_ensure_claimed(p, {});
     Engine& e = p->eng;
     const uint8_t* src = static_cast<const uint8_t*>(din) + in_off;
-    e.check_input_canonical(src, 4 * N);
     void* dst = is_coeffs ? (void*)e.arena.at<uint4>(e.off_input[0]) : (void*)e.h_inst[0].layers;
     AZK_CU(cudaMemcpyAsync(dst, src, 16 * N, cudaMemcpyDeviceToDevice, e.s));
+    if (is_coeffs)
+      e.scan_inputs({N});
+    else
+      e.check_input_canonical(dst, 4 * N);
     pcs_prove_common(p, is_coeffs != 0, pub, static_cast<uint8_t*>(dproof), true, proof_len, st, t);
   });
 }
@@ -617,6 +656,11 @@ azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* logs, 
 azk_status azk_batch_input(azk_batch* b, uint32_t i, void** dev) {
   return guarded(b ? b->ctx : nullptr, [&] {
     layout(b && dev && i < b->eng.cfg.size());
+    std::lock_guard<std::mutex> lk(b->mu);
+    // the caller writes this input directly: what the last upload learned about it
+    // no longer holds (the FFT reads all N coefficients with QM31 arithmetic)
+    b->eng.forget_input(i);
+    AZK_CU(cudaStreamSynchronize(b->eng.s));
     *dev = b->eng.arena.at<void>(b->eng.off_input[i]);
   });
 }
@@ -633,7 +677,8 @@ azk_status azk_batch_upload(azk_batch* b, const uint32_t* host, const uint64_t* 
       AZK_CU(cudaMemcpyAsync(in, host + 4 * offsets[i], 16 * counts[i], cudaMemcpyHostToDevice, e.s));
       if (counts[i] < N) AZK_CU(cudaMemsetAsync(in + counts[i], 0, 16 * (N - counts[i]), e.s));
     }
-    AZK_CU(cudaStreamSynchronize(e.s));
+    // every staged word must be canonical (QM31CanonicalityCheck.swift:11-117)
+    e.scan_inputs(std::vector<uint64_t>(counts, counts + e.cfg.size()));
   });
 }
 
@@ -714,5 +759,393 @@ azk_status azk_batch_work(azk_batch* b, uint64_t* tree_permutations, uint64_t* f
 }
 
 void azk_batch_destroy(azk_batch* b) { delete b; }
+
+}  // extern "C"
+
+// ===========================================================================
+// Continuous-batching server
+//
+// Jobs (Circle PCS commit-and-fold proofs and M31 multilinear sum-checks) enter
+// one FIFO queue.  `slots` worker threads each own a CUDA stream; a worker takes
+// the next queued job as soon as its device memory fits the HBM budget, so jobs
+// that arrive while others run join the device as slots and memory free up and
+// their kernels overlap with the running ones.
+//
+// Device memory is per worker and per job shape (a PCS engine or a sum-check
+// table set), kept after the job for the next job of that shape: no allocation
+// or free (each of which waits for the whole device) sits between jobs once the
+// shapes have been seen.  Every byte held, in use or cached, counts against the
+// budget; a worker whose next job does not fit first gives back its own cached
+// shapes, least recently used first.
+// ===========================================================================
+namespace {
+
+struct ServeJob {
+  uint64_t id = 0;
+  int kind = 0;  // 0 pcs, 1 sumcheck
+  uint32_t logn = 0, rounds = 0, queries = 0, log_blowup = 0;
+  std::vector<uint32_t> input;  // pcs: coefficient words; sumcheck: evaluations
+  uint64_t count = 0;           // pcs: coefficient count
+  uint8_t pub[32] = {0};
+  uint64_t bytes = 0;  // device memory of its shape
+  std::chrono::steady_clock::time_point submitted, started, finished;
+  int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
+  std::string error;
+  std::vector<uint8_t> result;
+};
+
+using ShapeKey = std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t>;
+
+ShapeKey shape_of(const ServeJob& j) { return std::make_tuple(j.kind, j.logn, j.rounds, j.queries, j.log_blowup); }
+
+struct SumcheckBufs {
+  DevBuf ev, scratch, rounds, out;
+};
+
+// Device memory of one job shape held by a worker.
+struct Resident {
+  std::unique_ptr<Engine> eng;
+  std::unique_ptr<SumcheckBufs> sc;
+  uint64_t bytes = 0;
+  uint64_t last_use = 0;
+};
+
+uint64_t pcs_shape_bytes(uint32_t logn, uint32_t rounds, uint32_t queries) {
+  uint64_t N = 1ull << logn;
+  // arena of one engine: input 16N, layers 32N, trees 64N, tree counters 2N,
+  // transcript and proof state; FFT work lists and slack rounded into 8N
+  return 120 * N + proof_total_bytes(logn, rounds, queries, 0, false) + (64ull << 10);
+}
+
+uint64_t sumcheck_shape_bytes(uint32_t logn) { return 8ull << logn | 4096; }
+
+}  // namespace
+
+struct azk_server {
+  azk_ctx* ctx;
+  Sched sched;
+  uint64_t budget;
+  uint32_t slots;
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::deque<std::shared_ptr<ServeJob>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<ServeJob>> jobs;
+  uint64_t next_id = 1;
+  uint64_t held = 0;  // device bytes held by all workers (in use and cached)
+  uint64_t running = 0;
+  uint64_t tick = 0;
+  bool stop = false;
+  std::vector<std::map<ShapeKey, Resident>> cache;  // per worker
+  std::vector<std::thread> workers;
+  uint64_t completed = 0, elems = 0;
+  std::chrono::steady_clock::time_point first_submit, last_finish;
+  bool any_submit = false;
+};
+
+namespace {
+
+void run_pcs(azk_server* sv, Resident& r, ServeJob& j) {
+  if (!r.eng) {
+    r.eng = std::make_unique<Engine>();
+    Sched sc = sv->sched;
+    sc.graph = false;
+    r.eng->init(sv->ctx, {InstanceCfg{j.logn, j.rounds, j.queries, j.log_blowup, 0, {}}}, sc);
+  }
+  Engine* e = r.eng.get();
+  uint64_t N = 1ull << j.logn;
+  uint4* in = e->arena.at<uint4>(e->off_input[0]);
+  AZK_CU(cudaMemcpyAsync(in, j.input.data(), 16 * j.count, cudaMemcpyHostToDevice, e->s));
+  if (j.count < N) AZK_CU(cudaMemsetAsync(in + j.count, 0, 16 * (N - j.count), e->s));
+  e->scan_inputs({j.count});
+  e->set_publics(j.pub);
+  Timer t;
+  e->run(true, true, nullptr, t);
+  j.result.resize(e->proof_len[0]);
+  AZK_CU(cudaMemcpyAsync(j.result.data(), e->h_inst[0].proof, e->proof_len[0], cudaMemcpyDeviceToHost, e->s));
+  AZK_CU(cudaStreamSynchronize(e->s));
+}
+
+// Sum-check of one table through reusable device buffers: evaluations upload,
+// one single-CTA kernel, results download.  Output words: claimed sum, final
+// evaluation, digest (8 words), sums at 0, sums at 1, challenges (rounds each).
+std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s) {
+  const uint64_t n = 1ull << logn;
+  if (!b.ev.p) {
+    b.ev.alloc(4 * n, "Sumcheck.Evals");
+    b.scratch.alloc(4 * n, "Sumcheck.Scratch");
+    b.rounds.alloc(12ull * logn + 64, "Sumcheck.Rounds");
+    b.out.alloc(sizeof(SumcheckOut), "Sumcheck.Out");
+  }
+  AZK_CU(cudaMemcpyAsync(b.ev.p, evals, 4 * n, cudaMemcpyHostToDevice, s));
+  SumcheckOut h{};
+  h.r0 = b.rounds.as<uint32_t>();
+  h.r1 = h.r0 + logn;
+  h.challenges = h.r1 + logn;
+  AZK_CU(cudaMemcpyAsync(b.out.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  AZK_CU(launch_sumcheck(b.ev.as<uint32_t>(), logn, b.scratch.as<uint32_t>(), b.out.as<SumcheckOut>(), s));
+  SumcheckOut r{};
+  std::vector<uint32_t> rounds(3 * logn);
+  AZK_CU(cudaMemcpyAsync(&r, b.out.p, sizeof(r), cudaMemcpyDeviceToHost, s));
+  AZK_CU(cudaMemcpyAsync(rounds.data(), b.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, s));
+  AZK_CU(cudaStreamSynchronize(s));
+  std::vector<uint32_t> words = {r.claimed_sum, r.final_eval};
+  for (int i = 0; i < 4; i++) {
+    words.push_back((uint32_t)r.digest[i]);
+    words.push_back((uint32_t)(r.digest[i] >> 32));
+  }
+  words.insert(words.end(), rounds.begin(), rounds.end());
+  return words;
+}
+
+void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j) {
+  if (!res.sc) res.sc = std::make_unique<SumcheckBufs>();
+  std::vector<uint32_t> words = sumcheck_run(*res.sc, j.input.data(), j.logn, s);
+  j.result.resize(4 * words.size());
+  std::memcpy(j.result.data(), words.data(), j.result.size());
+}
+
+// Called with the server lock held.  Takes the front job if its shape is cached
+// by this worker or its bytes fit the budget, evicting this worker's least
+// recently used shapes when that makes room.  Nothing is taken while the job
+// cannot fit; a job larger than the budget never enters the queue.
+std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
+  if (sv->queue.empty()) return nullptr;
+  auto& cache = sv->cache[w];
+  const auto& j = sv->queue.front();
+  ShapeKey key = shape_of(*j);
+  if (!cache.count(key)) {
+    while (sv->held + j->bytes > sv->budget && !cache.empty()) {
+      auto lru = cache.begin();
+      for (auto it = cache.begin(); it != cache.end(); ++it)
+        if (it->second.last_use < lru->second.last_use) lru = it;
+      sv->held -= lru->second.bytes;
+      cache.erase(lru);  // frees the device memory of that shape
+    }
+    if (sv->held + j->bytes > sv->budget) return nullptr;
+    Resident& r = cache[key];
+    r.bytes = j->bytes;
+    sv->held += j->bytes;
+  }
+  cache[key].last_use = ++sv->tick;
+  auto job = j;
+  sv->queue.pop_front();
+  sv->running++;
+  job->state = 1;
+  job->started = std::chrono::steady_clock::now();
+  return job;
+}
+
+void worker_loop(azk_server* sv, int w) {
+  cudaSetDevice(sv->ctx->device);
+  cudaStream_t s = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  for (;;) {
+    std::shared_ptr<ServeJob> job;
+    Resident* res = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      for (;;) {
+        if (sv->stop && sv->queue.empty()) break;
+        job = try_take(sv, w);
+        if (job) break;
+        sv->cv.wait(lk);
+      }
+      if (!job) break;
+      res = &sv->cache[w][shape_of(*job)];
+    }
+    try {
+      if (job->kind == 0)
+        run_pcs(sv, *res, *job);
+      else
+        run_sumcheck(*res, s, *job);
+      job->state = 2;
+    } catch (const Error& e) {
+      job->error = e.msg;
+      job->state = 3;
+    } catch (const std::exception& e) {
+      job->error = e.what();
+      job->state = 3;
+    }
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      job->finished = std::chrono::steady_clock::now();
+      job->input.clear();
+      job->input.shrink_to_fit();
+      if (job->state == 3) {  // drop the shape's memory: it may be in an unknown state
+        auto it = sv->cache[w].find(shape_of(*job));
+        if (it != sv->cache[w].end()) {
+          sv->held -= it->second.bytes;
+          sv->cache[w].erase(it);
+        }
+      }
+      sv->running--;
+      sv->completed++;
+      if (job->kind == 0 && job->state == 2) sv->elems += 1ull << job->logn;
+      sv->last_finish = job->finished;
+    }
+    sv->cv.notify_all();
+    sv->done_cv.notify_all();
+  }
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (auto& kv : sv->cache[w]) sv->held -= kv.second.bytes;
+    sv->cache[w].clear();
+  }
+  if (s) cudaStreamDestroy(s);
+}
+
+uint64_t submit(azk_server* sv, std::shared_ptr<ServeJob> j) {
+  std::lock_guard<std::mutex> lk(sv->mu);
+  require(j->bytes <= sv->budget, AZK_ERR_HBM_BUDGET,
+          "job needs " + std::to_string(j->bytes) + " device bytes, more than the server's HBM budget of " + std::to_string(sv->budget));
+  j->id = sv->next_id++;
+  j->submitted = std::chrono::steady_clock::now();
+  if (!sv->any_submit) {
+    sv->first_submit = j->submitted;
+    sv->any_submit = true;
+  }
+  sv->jobs[j->id] = j;
+  sv->queue.push_back(j);
+  sv->cv.notify_all();
+  return j->id;
+}
+
+}  // namespace
+
+extern "C" {
+
+azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evals, uint64_t count, uint32_t* sums0, uint32_t* sums1, uint32_t* challenges,
+                              uint32_t* claimed_sum, uint32_t* final_eval, uint8_t digest[32], azk_stats* st) {
+  return guarded(ctx, [&] {
+    layout(ctx && evals && sums0 && sums1 && challenges && claimed_sum && final_eval && digest);
+    // preconditions of M31MultilinearSumcheckProofBuilderV1.prove (SumcheckOracle.swift:803-807)
+    layout(count > 1 && is_pow2(count) && count <= (1ull << 28), "evaluation count must be a power of two greater than one");
+    for (uint64_t i = 0; i < count; i++) layout(evals[i] < kP, "input contains a non-canonical field element");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Timer t;
+    uint32_t logn = ilog2(count);
+    SumcheckBufs b;
+    std::vector<uint32_t> w = sumcheck_run(b, evals, logn, ctx->stream);
+    *claimed_sum = w[0];
+    *final_eval = w[1];
+    std::memcpy(digest, w.data() + 2, 32);
+    std::memcpy(sums0, w.data() + 10, 4ull * logn);
+    std::memcpy(sums1, w.data() + 10 + logn, 4ull * logn);
+    std::memcpy(challenges, w.data() + 10 + 2 * logn, 4ull * logn);
+    fill_stats(st, t, 0, 0.0);
+  });
+}
+
+azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t slots, const azk_schedule* schedule, azk_server** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && slots >= 1 && slots <= 64 && hbm_budget_bytes > 0);
+    auto sv = std::make_unique<azk_server>();
+    sv->ctx = ctx;
+    sv->sched = resolve_schedule(schedule);
+    sv->budget = hbm_budget_bytes;
+    sv->slots = slots;
+    sv->cache.resize(slots);
+    for (uint32_t w = 0; w < slots; w++) sv->workers.emplace_back(worker_loop, sv.get(), (int)w);
+    *out = sv.release();
+  });
+}
+
+azk_status azk_server_submit_pcs(azk_server* sv, uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t rounds, const uint32_t* coeffs,
+                                 uint64_t count, const uint8_t pub[32], uint64_t* job_id) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv && coeffs && pub && job_id);
+    validate_params(logn, log_blowup, queries, 0, rounds);
+    layout(count >= 1 && count <= (1ull << logn));
+    for (uint64_t i = 0; i < 4 * count; i++) layout(coeffs[i] < kP, "input contains a non-canonical field element");
+    auto j = std::make_shared<ServeJob>();
+    j->kind = 0;
+    j->logn = logn;
+    j->rounds = rounds;
+    j->queries = queries;
+    j->log_blowup = log_blowup;
+    j->input.assign(coeffs, coeffs + 4 * count);
+    j->count = count;
+    std::memcpy(j->pub, pub, 32);
+    j->bytes = pcs_shape_bytes(logn, rounds, queries);
+    *job_id = submit(sv, j);
+  });
+}
+
+azk_status azk_server_submit_sumcheck(azk_server* sv, const uint32_t* evals, uint64_t count, uint64_t* job_id) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv && evals && job_id);
+    // M31MultilinearSumcheckProofBuilderV1.prove preconditions (SumcheckOracle.swift:803-807)
+    layout(count > 1 && is_pow2(count) && count <= (1ull << 28));
+    for (uint64_t i = 0; i < count; i++) layout(evals[i] < kP, "input contains a non-canonical field element");
+    auto j = std::make_shared<ServeJob>();
+    j->kind = 1;
+    j->logn = ilog2(count);
+    j->input.assign(evals, evals + count);
+    j->bytes = sumcheck_shape_bytes(j->logn);
+    *job_id = submit(sv, j);
+  });
+}
+
+azk_status azk_server_poll(azk_server* sv, uint64_t id, int* state, double* latency_s, uint8_t* out, uint64_t* out_len) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv && state);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(id);
+    layout(it != sv->jobs.end(), "unknown job id");
+    ServeJob& j = *it->second;
+    *state = j.state;
+    if (j.state == 3) fail(AZK_ERR_COMMAND_EXECUTION_FAILED, j.error);
+    if (j.state == 2) {
+      if (latency_s) *latency_s = std::chrono::duration<double>(j.finished - j.submitted).count();
+      if (out_len) {
+        if (out) {
+          layout(*out_len >= j.result.size(), "result buffer too small");
+          std::memcpy(out, j.result.data(), j.result.size());
+        }
+        *out_len = j.result.size();
+      }
+    }
+  });
+}
+
+azk_status azk_server_release(azk_server* sv, uint64_t id) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv != nullptr);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(id);
+    layout(it != sv->jobs.end() && it->second->state >= 2, "job not finished");
+    sv->jobs.erase(it);
+  });
+}
+
+azk_status azk_server_wait_all(azk_server* sv) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv != nullptr);
+    std::unique_lock<std::mutex> lk(sv->mu);
+    sv->done_cv.wait(lk, [&] { return sv->queue.empty() && sv->running == 0; });
+  });
+}
+
+azk_status azk_server_stats(azk_server* sv, uint64_t* completed, uint64_t* elems, double* span_s, uint64_t* held) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv != nullptr);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (completed) *completed = sv->completed;
+    if (elems) *elems = sv->elems;
+    if (span_s) *span_s = sv->any_submit ? std::chrono::duration<double>(sv->last_finish - sv->first_submit).count() : 0.0;
+    if (held) *held = sv->held;
+  });
+}
+
+void azk_server_destroy(azk_server* sv) {
+  if (!sv) return;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  for (auto& t : sv->workers) t.join();
+  delete sv;
+}
 
 }  // extern "C"

@@ -2,6 +2,7 @@
 // Keccak-f batch, SHA3/Keccak batch hashing, raw/prehashed Merkle commitment,
 // Circle FFT codeword, single folds and fold chains.
 #include <algorithm>
+#include <cstdlib>
 
 #include "azk_field.cuh"
 #include "azk_runtime.h"
@@ -40,6 +41,10 @@ Sched azk::resolve_schedule(const azk_schedule* s) {
     if (s->group_log) r.group_log = s->group_log;
     if (s->threads) r.threads = s->threads;
     r.graph = s->use_graph != 0;
+    for (int i = 0; i < 32; i++) {
+      r.layer_tile[i] = s->layer_treelet[i];
+      require(r.layer_tile[i] <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "layer treelet depth must be in 0...13");
+    }
   }
   require(r.tile_log >= 1 && r.tile_log <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 1...13");
   if (r.group_log > r.tile_log) r.group_log = r.tile_log;
@@ -171,6 +176,12 @@ extern "C" {
 azk_status azk_ctx_create(int device, azk_ctx** out) {
   return guarded(nullptr, [&] {
     layout(out != nullptr);
+    // Streams beyond the device's hardware work queues share queues, and a long
+    // kernel then blocks unrelated streams behind it (the server runs one stream
+    // per worker).  The queue count is read when CUDA initialises, so this only
+    // takes effect when this library is the first CUDA user of the process, and
+    // never overrides a value the caller set.
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
       cudaGetLastError();

@@ -1,0 +1,248 @@
+// M31 multilinear sum-check prover on the device (M31MultilinearSumcheckProofBuilderV1,
+// SumcheckOracle.swift:797-868; statement digest :743-754; word digest :1288-1299;
+// transcript frames :1066-1106).
+//
+// Two launches per table.  The statement's word digest is one sequential sponge
+// over the table, so it runs as its own one-warp kernel (the state spread over
+// the warp's lanes) that holds almost nothing of an SM while other jobs' kernels
+// run beside it.  Then one
+// CTA proves the table: each round is a block reduction (sums of the even and odd
+// entries), a transcript round by thread 0 (round frame, challenge frame, squeeze
+// one word mod p) and a fold t'[i] = (1 - r) t[2i] + r t[2i+1].  A table of 2^20
+// words is 4 MiB, so each round is a few microseconds of one SM; keeping the rounds
+// in one CTA needs no grid-wide wait and lets many jobs share the GPU.
+#include "azk_field.cuh"
+#include "azk_internal.h"
+
+namespace azk {
+
+struct SumcheckOut {
+  uint32_t claimed_sum;
+  uint32_t final_eval;
+  uint64_t digest[4];
+  uint32_t* r0;          // rounds
+  uint32_t* r1;          // rounds
+  uint32_t* challenges;  // rounds
+};
+
+__device__ __forceinline__ uint32_t block_sum_m31(uint32_t v, uint32_t* red) {
+  // warp tree then one warp over the warp sums (values < 2^31, sums reduced each step)
+  for (int o = 16; o > 0; o >>= 1) v = m31_add(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint32_t w = 0;
+  if (threadIdx.x < 32) {
+    w = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0u;
+    for (int o = 16; o > 0; o >>= 1) w = m31_add(w, __shfl_down_sync(0xffffffffu, w, o));
+  }
+  __syncthreads();
+  return w;  // valid in thread 0
+}
+
+__device__ void sc_frame(FrameBuf& f, uint8_t type) {
+  const char dom[] = "AppleZKProver.M31MultilinearSumcheck";
+  f.n = 0;
+  fb_u32(f, 36);
+  fb_str(f, dom, 36);
+  fb_u32(f, 1);
+  fb_u8(f, type);
+}
+
+// ---------------------------------------------------------------------------
+// Keccak-f[1600] spread over one warp, for the statement digest: one sponge over
+// the whole table is a chain of ~30,000 dependent permutations, so what counts is
+// the latency of one permutation, not throughput.  Lane x + 5y (< 25) holds state
+// lane (x, y); lanes 25..31 shadow lane 0.  A round is three shuffle stages:
+//   1. the column parity C[x] (four shuffles) and, for pi, the source lane
+//      (xs, ys) whose value lands here: X = ys, Y = 2 xs + 3 ys (mod 5);
+//   2. C[xs - 1] and C[xs + 1], giving theta's D[xs], then rho's rotation of the
+//      source lane by its own offset;
+//   3. chi's two row neighbours; iota on lane 0.
+// ---------------------------------------------------------------------------
+__constant__ static const uint8_t kRhoOffsets[25] = {0,  1,  62, 28, 27, 36, 44, 6,  55, 20, 3,  10, 43,
+                                                     25, 39, 41, 45, 15, 21, 8,  18, 2,  61, 56, 14};
+
+__device__ __forceinline__ uint64_t rotl_var(uint64_t v, uint32_t r) {
+  uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+  if (r & 32u) {
+    uint32_t t = lo;
+    lo = hi;
+    hi = t;
+  }
+  const uint32_t m = r & 31u;
+  return ((uint64_t)__funnelshift_l(lo, hi, m) << 32) | __funnelshift_l(hi, lo, m);
+}
+
+struct WarpKeccak {
+  uint32_t col[4];     // the other four lanes of this lane's column
+  uint32_t src;        // pi source lane
+  uint32_t cm, cp;     // lanes of columns xs - 1 and xs + 1
+  uint32_t rho;        // rotation of the source lane
+  uint32_t n1, n2;     // chi neighbours (x + 1, y) and (x + 2, y)
+  bool lane0;
+
+  __device__ explicit WarpKeccak(uint32_t lane) {
+    const uint32_t t = lane < 25 ? lane : 0;
+    const uint32_t x = t % 5, y = t / 5;
+    for (uint32_t k = 1; k < 5; k++) col[k - 1] = x + 5 * ((y + k) % 5);
+    const uint32_t ys = x, xs = (((y + 15 - 3 * x) % 5) * 3) % 5;  // 2^-1 = 3 (mod 5)
+    src = xs + 5 * ys;
+    cm = (xs + 4) % 5;
+    cp = (xs + 1) % 5;
+    rho = kRhoOffsets[src];
+    n1 = (x + 1) % 5 + 5 * y;
+    n2 = (x + 2) % 5 + 5 * y;
+    lane0 = lane == 0;
+  }
+
+  __device__ __forceinline__ void permute(uint64_t& a) const {
+#pragma unroll 1
+    for (int r = 0; r < 24; r++) {
+      const uint64_t as = __shfl_sync(0xffffffffu, a, src);
+      const uint64_t c = a ^ __shfl_sync(0xffffffffu, a, col[0]) ^ __shfl_sync(0xffffffffu, a, col[1]) ^
+                         __shfl_sync(0xffffffffu, a, col[2]) ^ __shfl_sync(0xffffffffu, a, col[3]);
+      const uint64_t c_m = __shfl_sync(0xffffffffu, c, cm), c_p = __shfl_sync(0xffffffffu, c, cp);
+      const uint64_t b = rotl_var(as ^ c_m ^ rotl<1>(c_p), rho);
+      const uint64_t b1 = __shfl_sync(0xffffffffu, b, n1), b2 = __shfl_sync(0xffffffffu, b, n2);
+      a = b ^ (~b1 & b2);
+      if (lane0) a ^= kKeccakRC[r];
+    }
+  }
+};
+
+// Byte k of the framed word-digest input: u32 len || "AppleZKProver.M31Sumcheck.Words.V1"
+// || u32 1 || u64 count || words (little-endian) (SumcheckOracle.swift:1288-1299).
+__device__ __forceinline__ uint32_t digest_stream_byte(const uint32_t* words, uint64_t count, uint64_t k) {
+  const char dom[] = "AppleZKProver.M31Sumcheck.Words.V1";
+  if (k < 4) return (34u >> (8 * k)) & 0xFFu;
+  if (k < 38) return (uint8_t)dom[k - 4];
+  if (k < 42) return (1u >> (8 * (k - 38))) & 0xFFu;
+  if (k < 50) return (uint32_t)(count >> (8 * (k - 42))) & 0xFFu;
+  const uint64_t w = (k - 50) >> 2;
+  return (__ldg(words + w) >> (8 * ((k - 50) & 3))) & 0xFFu;
+}
+
+// Rate word `lane` (< 17) of the block starting at stream byte `pos` >= 136 when
+// the block lies inside the stream: after the 50-byte header every 8-byte word
+// starts 2 bytes into a table word, so it is assembled from three table words.
+__device__ __forceinline__ uint64_t digest_block_word(const uint32_t* words, uint64_t pos, uint32_t lane) {
+  const uint32_t* w = words + ((pos - 50) >> 2) + 2 * lane;
+  const uint64_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+  return (w0 >> 16) | (w1 << 16) | (w2 << 48);
+}
+
+// SHA3-256 of the framed table, by the whole warp; lanes 0..3 return the digest lanes.
+__device__ uint64_t digest_words_warp(const uint32_t* words, uint64_t count) {
+  const uint32_t lane = threadIdx.x & 31;
+  const WarpKeccak kf(lane);
+  const uint64_t total = 50 + 4 * count;
+  uint64_t a = 0;
+  uint64_t pos = 0;
+  if (total >= 136) {
+    // first block: header bytes then table bytes
+    if (lane < 17) {
+      uint64_t v = 0;
+      for (uint32_t b = 0; b < 8; b++) v |= (uint64_t)digest_stream_byte(words, count, 8 * lane + b) << (8 * b);
+      a ^= v;
+    }
+    pos = 136;
+    // full middle blocks, the next block's words loaded before this permutation
+    uint64_t next = (lane < 17 && pos + 136 <= total) ? digest_block_word(words, pos, lane) : 0;
+    kf.permute(a);
+    while (pos + 136 <= total) {
+      a ^= next;
+      const uint64_t npos = pos + 136;
+      next = (lane < 17 && npos + 136 <= total) ? digest_block_word(words, npos, lane) : 0;
+      kf.permute(a);
+      pos = npos;
+    }
+  }
+  // final block: tail bytes, suffix 0x06, 0x80 at the end of the rate
+  const uint64_t tail = total - pos;
+  if (lane < 17) {
+    uint64_t v = 0;
+    for (uint32_t b = 0; b < 8; b++) {
+      const uint64_t k = 8 * lane + b;
+      if (k < tail) v |= (uint64_t)digest_stream_byte(words, count, pos + k) << (8 * b);
+      if (k == tail) v |= (uint64_t)0x06 << (8 * b);
+    }
+    if (lane == 16) v ^= kPadEnd;
+    a ^= v;
+  }
+  kf.permute(a);
+  return a;
+}
+
+__global__ void __launch_bounds__(32) sumcheck_digest_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, SumcheckOut* __restrict__ out) {
+  const uint64_t d = digest_words_warp(evals, 1ull << log_n);
+  if (threadIdx.x < 4) out->digest[threadIdx.x] = d;
+}
+
+__global__ void __launch_bounds__(1024) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
+                                                        SumcheckOut* __restrict__ out) {
+  __shared__ uint32_t red[32];
+  __shared__ uint32_t s_ch;
+  const uint64_t n = 1ull << log_n;
+  // claimed sum
+  uint32_t acc = 0;
+  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) acc = m31_add(acc, evals[i]);
+  uint32_t total = block_sum_m31(acc, red);
+  if (threadIdx.x == 0) out->claimed_sum = total;
+  Transcript t;
+  if (threadIdx.x == 0) {
+    tr_reset(t);
+    FrameBuf f;
+    sc_frame(f, 0);
+    fb_u64(f, n);
+    fb_u32(f, log_n);
+    fb_u32(f, total);
+    for (int i = 0; i < 4; i++) fb_u64(f, out->digest[i]);
+    tr_absorb(t, f.b, f.n);
+  }
+  const uint32_t* cur = evals;
+  uint32_t* bufs[2] = {scratch, scratch + (n >> 1)};
+  for (uint32_t r = 0; r < log_n; r++) {
+    const uint64_t half = (n >> r) >> 1;
+    uint32_t z = 0, o = 0;
+    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
+      z = m31_add(z, cur[2 * i]);
+      o = m31_add(o, cur[2 * i + 1]);
+    }
+    uint32_t zs = block_sum_m31(z, red);
+    uint32_t os = block_sum_m31(o, red);
+    if (threadIdx.x == 0) {
+      out->r0[r] = zs;
+      out->r1[r] = os;
+      FrameBuf f;
+      sc_frame(f, 1);
+      fb_u32(f, r);
+      fb_u32(f, zs);
+      fb_u32(f, os);
+      tr_absorb(t, f.b, f.n);
+      sc_frame(f, 2);
+      fb_u32(f, r);
+      fb_u32(f, kP);
+      tr_absorb(t, f.b, f.n);
+      uint32_t c;
+      tr_squeeze_u32(t, 1, kP, &c);
+      out->challenges[r] = c;
+      s_ch = c;
+    }
+    __syncthreads();
+    const uint32_t c = s_ch;
+    const uint32_t omc = m31_sub(1, c);
+    uint32_t* nxt = bufs[r & 1];
+    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) nxt[i] = m31_add(m31_mul(omc, cur[2 * i]), m31_mul(c, cur[2 * i + 1]));
+    __syncthreads();
+    cur = nxt;
+  }
+  if (threadIdx.x == 0) out->final_eval = cur[0];
+}
+
+cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s) {
+  sumcheck_digest_kernel<<<1, 32, 0, s>>>(evals, log_n, out);
+  sumcheck_kernel<<<1, 1024, 0, s>>>(evals, log_n, scratch, out);
+  return cudaGetLastError();
+}
+
+}  // namespace azk

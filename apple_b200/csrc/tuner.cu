@@ -1,0 +1,373 @@
+// Autotuner measurements and the learned cost model's kernels.
+//
+// The reference races a handful of Merkle schedules behind a CPU gate and keeps
+// winners in SQLite (Planner/MetalProofPlanner.swift:20-615).  Here the tuner
+// times the commit kernel itself for any (layer size, leaf bytes, fold or not,
+// concurrent trees, treelet depth, group depth, threads) and a small MLP, trained
+// on those timings by the kernels below, predicts schedules for shapes it has not
+// timed.  Nothing here changes a result: schedules only reorder identical work.
+#include <algorithm>
+#include <random>
+
+#include "azk_field.cuh"
+#include "azk_runtime.h"
+
+using namespace azk;
+
+// ---------------------------------------------------------------------------
+// Timing one tree-kernel configuration
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void fill_random_kernel(uint32_t* w, uint64_t n, uint32_t seed, uint32_t nonzero) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t x = (uint32_t)(i * 0x9E3779B1u) ^ seed;
+  x ^= x >> 16;
+  x *= 0x85EBCA6Bu;
+  x ^= x >> 13;
+  x *= 0xC2B2AE35u;
+  x ^= x >> 16;
+  x &= 0x7FFFFFFFu;
+  if (x == kP) x = 0;
+  if (nonzero && x == 0) x = 1;
+  w[i] = x;
+}
+}  // namespace
+
+extern "C" azk_status azk_tuner_time_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent, uint32_t tile_log,
+                                          uint32_t group_log, uint32_t threads, uint32_t reps, double* seconds) {
+  return guarded(ctx, [&] {
+    layout(ctx && seconds && log_leaves >= 1 && log_leaves <= 24 && concurrent >= 1 && concurrent <= 4096 && reps >= 1);
+    layout(leaf_bytes == 16 || leaf_bytes == 64);
+    require(tile_log >= 1 && tile_log <= 13 && group_log >= 1 && (threads == 128 || threads == 256 || threads == 512),
+            AZK_ERR_INVALID_KERNEL_CONFIGURATION, "tile_log 1..13, group_log >= 1, threads 128/256/512");
+    const uint64_t n = 1ull << log_leaves;
+    layout(n * concurrent <= (1ull << 26), "at most 2^26 leaves in one timing");
+    AZK_CU(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const uint32_t tl = std::min(tile_log, log_leaves);
+    const uint32_t gl = std::max<uint32_t>(1, std::min(group_log, tl));
+    // 64-byte leaves: the same QM31 layer memory read as raw 64-byte leaves (4 QM31 each)
+    const uint64_t elems = leaf_bytes == 16 ? n : 4 * n;
+    DevBuf prev(16 * 2 * elems * concurrent, "Tuner.Prev"), out(16 * elems * concurrent, "Tuner.Out"), inv(4 * n + 16, "Tuner.Inv"),
+        ch(16, "Tuner.Challenge"), inner(32 * n * concurrent, "Tuner.Inner"), cnt(4 * tree_counter_count(log_leaves, 1) * concurrent, "Tuner.Counters"),
+        jobs(sizeof(TreeJob) * concurrent, "Tuner.Jobs");
+    auto fill = [&](DevBuf& b, uint32_t seed, uint32_t nz) {
+      uint64_t words = b.bytes / 4;
+      fill_random_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(b.as<uint32_t>(), words, seed, nz);
+      AZK_CU(cudaGetLastError());
+    };
+    fill(prev, 11, 0);
+    fill(out, 13, 0);
+    fill(inv, 17, 1);
+    fill(ch, 19, 0);
+    AZK_CU(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+    std::vector<TreeJob> hj(concurrent);
+    std::vector<uint2> work;
+    const uint32_t kind = leaf_bytes == 64 ? kLeafRaw : (fold ? kLeafFold : kLeafQM31);
+    for (uint32_t c = 0; c < concurrent; c++) {
+      TreeJob& j = hj[c];
+      j = TreeJob{};
+      j.logn = log_leaves;
+      j.kind = kind;
+      j.tile_log = tl;
+      j.group_log = gl;
+      if (kind == kLeafRaw) {
+        j.raw = reinterpret_cast<const uint8_t*>(out.as<uint4>() + c * elems);
+        j.stride = 64;
+        j.len = 64;
+        j.suffix = 0x06;
+        j.aligned8 = 1;
+      } else if (kind == kLeafQM31) {
+        j.layer = out.as<uint4>() + c * elems;
+      } else {
+        j.layer = prev.as<uint4>() + c * 2 * elems;
+        j.inv = inv.as<uint32_t>();
+        j.fold_ch = ch.as<uint32_t>();
+        j.out_layer = out.as<uint4>() + c * elems;
+      }
+      j.inner = inner.as<uint64_t>() + 4 * n * c;
+      j.counters = cnt.as<uint32_t>() + tree_counter_count(log_leaves, 1) * c;
+      j.root_action = kRootNone;
+      uint64_t tiles = 1ull << (log_leaves - tl);
+      for (uint64_t t = 0; t < tiles; t++) work.push_back(make_uint2(c, (uint32_t)t));
+    }
+    DevBuf dwork(work.size() * sizeof(uint2), "Tuner.Work");
+    AZK_CU(cudaMemcpyAsync(jobs.p, hj.data(), sizeof(TreeJob) * concurrent, cudaMemcpyHostToDevice, s));
+    AZK_CU(cudaMemcpyAsync(dwork.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    AZK_CU(launch_tree_jobs(jobs.as<TreeJob>(), dwork.as<uint2>(), (uint32_t)work.size(), tl, kind, threads, s));  // warm-up
+    std::vector<double> ts;
+    for (uint32_t r = 0; r < reps; r++) {
+      GpuTimer g(s);
+      AZK_CU(launch_tree_jobs(jobs.as<TreeJob>(), dwork.as<uint2>(), (uint32_t)work.size(), tl, kind, threads, s));
+      g.stop();
+      ts.push_back(g.seconds());
+    }
+    std::sort(ts.begin(), ts.end());
+    *seconds = ts[ts.size() / 2];
+  });
+}
+
+// ---------------------------------------------------------------------------
+// MLP cost model: fully connected, ReLU hidden layers, linear output, MSE loss,
+// full-batch Adam.  fp32 throughout; one thread per output element, so every
+// sum runs in a fixed order (results are reproducible run to run).
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void dense_forward(const float* __restrict__ x, const float* __restrict__ w, const float* __restrict__ b, float* __restrict__ z, uint32_t rows,
+                              uint32_t in, uint32_t out, int relu) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)rows * out) return;
+  uint32_t r = (uint32_t)(t / out), o = (uint32_t)(t % out);
+  float acc = b[o];
+  const float* xr = x + (uint64_t)r * in;
+  const float* wo = w + (uint64_t)o * in;
+  for (uint32_t i = 0; i < in; i++) acc = fmaf(xr[i], wo[i], acc);
+  z[t] = relu ? fmaxf(acc, 0.0f) : acc;
+}
+
+// dL/dy for MSE over `rows` samples (mean of squared errors), and per-sample
+// squared errors for the loss.
+__global__ void mse_grad(const float* __restrict__ y, const float* __restrict__ target, float* __restrict__ dy, float* __restrict__ sq, uint32_t rows) {
+  uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  float e = y[r] - target[r];
+  dy[r] = 2.0f * e / (float)rows;
+  sq[r] = e * e;
+}
+
+__global__ void sum_rows(const float* __restrict__ v, uint32_t rows, float* __restrict__ out) {
+  if (threadIdx.x || blockIdx.x) return;
+  float acc = 0.0f;
+  for (uint32_t r = 0; r < rows; r++) acc += v[r];
+  out[0] = acc / (float)rows;
+}
+
+// dX[r][i] = sum_o dZ[r][o] W[o][i], masked by ReLU'(activation of X) when mask != 0
+__global__ void dense_backward_input(const float* __restrict__ dz, const float* __restrict__ w, const float* __restrict__ xact, float* __restrict__ dx,
+                                     uint32_t rows, uint32_t in, uint32_t out) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)rows * in) return;
+  uint32_t r = (uint32_t)(t / in), i = (uint32_t)(t % in);
+  float acc = 0.0f;
+  for (uint32_t o = 0; o < out; o++) acc = fmaf(dz[(uint64_t)r * out + o], w[(uint64_t)o * in + i], acc);
+  dx[t] = xact[t] > 0.0f ? acc : 0.0f;
+}
+
+// dW[o][i] = sum_r dZ[r][o] X[r][i];  dB[o] = sum_r dZ[r][o]
+__global__ void dense_backward_params(const float* __restrict__ dz, const float* __restrict__ x, float* __restrict__ dw, float* __restrict__ db, uint32_t rows,
+                                      uint32_t in, uint32_t out) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t nw = (uint64_t)out * in;
+  if (t < nw) {
+    uint32_t o = (uint32_t)(t / in), i = (uint32_t)(t % in);
+    float acc = 0.0f;
+    for (uint32_t r = 0; r < rows; r++) acc = fmaf(dz[(uint64_t)r * out + o], x[(uint64_t)r * in + i], acc);
+    dw[t] = acc;
+  } else if (t < nw + out) {
+    uint32_t o = (uint32_t)(t - nw);
+    float acc = 0.0f;
+    for (uint32_t r = 0; r < rows; r++) acc += dz[(uint64_t)r * out + o];
+    db[o] = acc;
+  }
+}
+
+__global__ void adam_update(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v, uint64_t n, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float gi = g[i];
+  float mi = b1 * m[i] + (1.0f - b1) * gi;
+  float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace
+
+struct azk_mlp {
+  azk_ctx* ctx;
+  std::mutex mu;
+  cudaStream_t s = nullptr;
+  std::vector<uint32_t> dims;
+  std::vector<uint64_t> w_off, b_off;
+  uint64_t nparams = 0;
+  DevBuf params, grads, m, v;
+  uint64_t step = 0;
+  ~azk_mlp() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+namespace {
+unsigned blocks_for(uint64_t n) { return (unsigned)((n + 255) / 256); }
+
+struct MlpWork {
+  std::vector<DevBuf> acts;  // acts[0] = input, acts[l] = output of layer l
+  std::vector<DevBuf> dacts;
+  DevBuf target, dy, sq, loss;
+};
+
+void mlp_forward(azk_mlp* p, MlpWork& w, uint32_t rows) {
+  size_t L = p->dims.size() - 1;
+  for (size_t l = 0; l < L; l++) {
+    uint32_t in = p->dims[l], out = p->dims[l + 1];
+    dense_forward<<<blocks_for((uint64_t)rows * out), 256, 0, p->s>>>(w.acts[l].as<float>(), p->params.as<float>() + p->w_off[l],
+                                                                       p->params.as<float>() + p->b_off[l], w.acts[l + 1].as<float>(), rows, in, out,
+                                                                       l + 1 < L ? 1 : 0);
+    AZK_CU(cudaGetLastError());
+  }
+}
+
+void mlp_backward(azk_mlp* p, MlpWork& w, uint32_t rows) {
+  size_t L = p->dims.size() - 1;
+  mse_grad<<<blocks_for(rows), 256, 0, p->s>>>(w.acts[L].as<float>(), w.target.as<float>(), w.dacts[L].as<float>(), w.sq.as<float>(), rows);
+  AZK_CU(cudaGetLastError());
+  sum_rows<<<1, 1, 0, p->s>>>(w.sq.as<float>(), rows, w.loss.as<float>());
+  for (size_t l = L; l-- > 0;) {
+    uint32_t in = p->dims[l], out = p->dims[l + 1];
+    dense_backward_params<<<blocks_for((uint64_t)out * in + out), 256, 0, p->s>>>(w.dacts[l + 1].as<float>(), w.acts[l].as<float>(),
+                                                                                 p->grads.as<float>() + p->w_off[l], p->grads.as<float>() + p->b_off[l],
+                                                                                 rows, in, out);
+    AZK_CU(cudaGetLastError());
+    if (l > 0) {
+      dense_backward_input<<<blocks_for((uint64_t)rows * in), 256, 0, p->s>>>(w.dacts[l + 1].as<float>(), p->params.as<float>() + p->w_off[l],
+                                                                             w.acts[l].as<float>(), w.dacts[l].as<float>(), rows, in, out);
+      AZK_CU(cudaGetLastError());
+    }
+  }
+}
+
+void mlp_prepare(azk_mlp* p, MlpWork& w, const float* x, const float* y, uint32_t rows) {
+  size_t L = p->dims.size() - 1;
+  w.acts.resize(L + 1);
+  w.dacts.resize(L + 1);
+  for (size_t l = 0; l <= L; l++) {
+    w.acts[l].alloc(4ull * rows * p->dims[l], "MLP.Activations");
+    w.dacts[l].alloc(4ull * rows * p->dims[l], "MLP.Gradients");
+  }
+  AZK_CU(cudaMemcpyAsync(w.acts[0].p, x, 4ull * rows * p->dims[0], cudaMemcpyHostToDevice, p->s));
+  if (y) {
+    w.target.alloc(4ull * rows, "MLP.Target");
+    w.dy.alloc(4ull * rows, "MLP.dY");
+    w.sq.alloc(4ull * rows, "MLP.SquaredError");
+    w.loss.alloc(16, "MLP.Loss");
+    AZK_CU(cudaMemcpyAsync(w.target.p, y, 4ull * rows, cudaMemcpyHostToDevice, p->s));
+  }
+}
+}  // namespace
+
+extern "C" {
+
+azk_status azk_mlp_create(azk_ctx* ctx, uint32_t n_layers, const uint32_t* dims, uint64_t seed, azk_mlp** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && dims && out && n_layers >= 1 && n_layers <= 8);
+    for (uint32_t l = 0; l <= n_layers; l++) layout(dims[l] >= 1 && dims[l] <= 1024);
+    layout(dims[n_layers] == 1, "the cost model predicts one value per sample");
+    AZK_CU(cudaSetDevice(ctx->device));
+    auto p = std::make_unique<azk_mlp>();
+    p->ctx = ctx;
+    p->dims.assign(dims, dims + n_layers + 1);
+    for (uint32_t l = 0; l < n_layers; l++) {
+      p->w_off.push_back(p->nparams);
+      p->nparams += (uint64_t)dims[l] * dims[l + 1];
+      p->b_off.push_back(p->nparams);
+      p->nparams += dims[l + 1];
+    }
+    // He-style initialisation from a seeded host generator (deterministic)
+    std::vector<float> h(p->nparams, 0.0f);
+    std::mt19937_64 rng(seed);
+    for (uint32_t l = 0; l < n_layers; l++) {
+      std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / dims[l]));
+      for (uint64_t i = 0; i < (uint64_t)dims[l] * dims[l + 1]; i++) h[p->w_off[l] + i] = nd(rng);
+    }
+    p->params.alloc(4 * p->nparams, "MLP.Params");
+    p->grads.alloc(4 * p->nparams, "MLP.Grads");
+    p->m.alloc(4 * p->nparams, "MLP.AdamM");
+    p->v.alloc(4 * p->nparams, "MLP.AdamV");
+    AZK_CU(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking));
+    AZK_CU(cudaMemcpyAsync(p->params.p, h.data(), 4 * p->nparams, cudaMemcpyHostToDevice, p->s));
+    AZK_CU(cudaMemsetAsync(p->m.p, 0, 4 * p->nparams, p->s));
+    AZK_CU(cudaMemsetAsync(p->v.p, 0, 4 * p->nparams, p->s));
+    AZK_CU(cudaStreamSynchronize(p->s));
+    *out = p.release();
+  });
+}
+
+uint64_t azk_mlp_param_count(azk_mlp* p) { return p ? p->nparams : 0; }
+
+azk_status azk_mlp_get_params(azk_mlp* p, float* out, uint64_t count) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && out && count == p->nparams);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaMemcpyAsync(out, p->params.p, 4 * count, cudaMemcpyDeviceToHost, p->s));
+    AZK_CU(cudaStreamSynchronize(p->s));
+  });
+}
+
+azk_status azk_mlp_set_params(azk_mlp* p, const float* in, uint64_t count) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && in && count == p->nparams);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaMemcpyAsync(p->params.p, in, 4 * count, cudaMemcpyHostToDevice, p->s));
+    AZK_CU(cudaMemsetAsync(p->m.p, 0, 4 * count, p->s));
+    AZK_CU(cudaMemsetAsync(p->v.p, 0, 4 * count, p->s));
+    p->step = 0;
+    AZK_CU(cudaStreamSynchronize(p->s));
+  });
+}
+
+azk_status azk_mlp_forward(azk_mlp* p, const float* x, uint64_t rows, float* y) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && x && y && rows >= 1 && rows <= (1u << 22));
+    std::lock_guard<std::mutex> lk(p->mu);
+    MlpWork w;
+    mlp_prepare(p, w, x, nullptr, (uint32_t)rows);
+    mlp_forward(p, w, (uint32_t)rows);
+    AZK_CU(cudaMemcpyAsync(y, w.acts.back().p, 4 * rows, cudaMemcpyDeviceToHost, p->s));
+    AZK_CU(cudaStreamSynchronize(p->s));
+  });
+}
+
+azk_status azk_mlp_gradients(azk_mlp* p, const float* x, const float* y, uint64_t rows, float* loss, float* grads) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && x && y && rows >= 1 && rows <= (1u << 22));
+    std::lock_guard<std::mutex> lk(p->mu);
+    MlpWork w;
+    mlp_prepare(p, w, x, y, (uint32_t)rows);
+    mlp_forward(p, w, (uint32_t)rows);
+    mlp_backward(p, w, (uint32_t)rows);
+    if (loss) AZK_CU(cudaMemcpyAsync(loss, w.loss.p, 4, cudaMemcpyDeviceToHost, p->s));
+    if (grads) AZK_CU(cudaMemcpyAsync(grads, p->grads.p, 4 * p->nparams, cudaMemcpyDeviceToHost, p->s));
+    AZK_CU(cudaStreamSynchronize(p->s));
+  });
+}
+
+azk_status azk_mlp_train(azk_mlp* p, const float* x, const float* y, uint64_t rows, uint32_t steps, float lr, float* final_loss) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && x && y && rows >= 1 && rows <= (1u << 22) && steps >= 1);
+    std::lock_guard<std::mutex> lk(p->mu);
+    MlpWork w;
+    mlp_prepare(p, w, x, y, (uint32_t)rows);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (uint32_t it = 0; it < steps; it++) {
+      mlp_forward(p, w, (uint32_t)rows);
+      mlp_backward(p, w, (uint32_t)rows);
+      p->step++;
+      float c1 = 1.0f - std::pow(b1, (float)p->step), c2 = 1.0f - std::pow(b2, (float)p->step);
+      adam_update<<<blocks_for(p->nparams), 256, 0, p->s>>>(p->params.as<float>(), p->grads.as<float>(), p->m.as<float>(), p->v.as<float>(), p->nparams, lr, b1,
+                                                            b2, eps, c1, c2);
+      AZK_CU(cudaGetLastError());
+    }
+    mlp_forward(p, w, (uint32_t)rows);
+    mlp_backward(p, w, (uint32_t)rows);
+    if (final_loss) AZK_CU(cudaMemcpyAsync(final_loss, w.loss.p, 4, cudaMemcpyDeviceToHost, p->s));
+    AZK_CU(cudaStreamSynchronize(p->s));
+  });
+}
+
+void azk_mlp_destroy(azk_mlp* p) { delete p; }
+
+}  // extern "C"

@@ -362,7 +362,13 @@ def _sched(schedule):
     if isinstance(schedule, Schedule):
         return ctypes.byref(schedule)
     s = Schedule(schedule.get("treelet_log", 0), schedule.get("group_log", 0), schedule.get("threads", 0), schedule.get("use_graph", 1))
+    for lg, tl in dict(schedule.get("layer_treelet", {})).items():
+        s.layer_treelet[int(lg)] = int(tl)
+    _keep.append(s)
     return ctypes.byref(s)
+
+
+_keep = []  # Schedule structs passed by reference stay alive until the call returns
 
 
 class CirclePCSFRIProver(_Plan):
@@ -481,3 +487,88 @@ class BatchProver(_Plan):
         qp = np.empty(self.queries, np.uint32)
         self._check(lib().azk_batch_trace(self._h, index, _ptr(cm), _ptr(ch), _ptr(fl), _ptr(qp)))
         return [cm[32 * k:32 * k + 32].tobytes() for k in range(r)], ch, fl, [int(v) for v in qp]
+
+
+def sumcheck_prove(ctx: Context, evaluations) -> dict:
+    """M31MultilinearSumcheckProofBuilderV1.prove (SumcheckOracle.swift:797-868) on the device."""
+    ev = np.ascontiguousarray(evaluations, dtype=np.uint32).reshape(-1)
+    rounds = max(0, len(ev).bit_length() - 1)
+    r0, r1, ch = (np.zeros(max(1, rounds), np.uint32) for _ in range(3))
+    cs, fe = ctypes.c_uint32(), ctypes.c_uint32()
+    dg = np.zeros(32, np.uint8)
+    check(lib().azk_sumcheck_prove(ctx.handle, _ptr(ev), len(ev), _ptr(r0), _ptr(r1), _ptr(ch), ctypes.byref(cs), ctypes.byref(fe), _ptr(dg), None),
+          ctx.handle)
+    return {"r0": r0[:rounds], "r1": r1[:rounds], "challenges": ch[:rounds], "claimed_sum": cs.value, "final": fe.value,
+            "initial_digest": dg.tobytes()}
+
+
+def _sumcheck_words(words: np.ndarray) -> dict:
+    rounds = (len(words) - 10) // 3
+    return {"claimed_sum": int(words[0]), "final": int(words[1]), "initial_digest": words[2:10].tobytes(),
+            "r0": words[10:10 + rounds], "r1": words[10 + rounds:10 + 2 * rounds], "challenges": words[10 + 2 * rounds:10 + 3 * rounds]}
+
+
+class ProofServer:
+    """Continuous-batching server over one device (azk_server_*).
+
+    Jobs are queued in arrival order and admitted when a worker slot is free and
+    their device memory fits the HBM budget; a job larger than the whole budget
+    raises AZKError(hbmBudget) at submission.  `poll` returns None while a
+    job is queued or running, else (result, latency_seconds): proof bytes for a
+    PCS job, a dict like `sumcheck_prove`'s for a sum-check job."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int, slots: int = 4, schedule=None):
+        self.ctx = ctx
+        self._h = _vp()
+        self._kind = {}
+        check(lib().azk_server_create(ctx.handle, int(hbm_budget_bytes), int(slots), _sched(schedule), ctypes.byref(self._h)), ctx.handle)
+
+    def _check(self, rc):
+        check(rc, self.ctx.handle)
+
+    def submit_pcs(self, log_size: int, log_blowup: int, queries: int, rounds: int, coefficients, public_digest: bytes) -> int:
+        c = _q(coefficients)
+        pub = _u8(public_digest)
+        jid = ctypes.c_uint64()
+        self._check(lib().azk_server_submit_pcs(self._h, log_size, log_blowup, queries, rounds, _ptr(c), len(c), _ptr(pub), ctypes.byref(jid)))
+        self._kind[jid.value] = 0
+        return jid.value
+
+    def submit_sumcheck(self, evaluations) -> int:
+        ev = np.ascontiguousarray(evaluations, dtype=np.uint32).reshape(-1)
+        jid = ctypes.c_uint64()
+        self._check(lib().azk_server_submit_sumcheck(self._h, _ptr(ev), len(ev), ctypes.byref(jid)))
+        self._kind[jid.value] = 1
+        return jid.value
+
+    def poll(self, job_id: int, release: bool = True):
+        st, lat, n = ctypes.c_int(), ctypes.c_double(), ctypes.c_uint64()
+        self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), ctypes.byref(lat), None, ctypes.byref(n)))
+        if st.value != 2:
+            return None
+        out = np.empty(max(1, n.value), np.uint8)
+        self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), None, _ptr(out), ctypes.byref(n)))
+        if release:
+            self._check(lib().azk_server_release(self._h, job_id))
+        kind = self._kind.pop(job_id, 0) if release else self._kind.get(job_id, 0)
+        res = out[:n.value].tobytes() if kind == 0 else _sumcheck_words(out[:n.value].view(np.uint32))
+        return res, lat.value
+
+    def wait_all(self):
+        self._check(lib().azk_server_wait_all(self._h))
+
+    def stats(self) -> dict:
+        c, e, h, span = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
+        self._check(lib().azk_server_stats(self._h, ctypes.byref(c), ctypes.byref(e), ctypes.byref(span), ctypes.byref(h)))
+        return {"completed": c.value, "pcs_elements": e.value, "span_s": span.value, "held_bytes": h.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().azk_server_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

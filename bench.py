@@ -237,6 +237,112 @@ def run_reference(args, logs, rounds, counts, offsets, rows, pubs, world, rank, 
     print(json.dumps(line), flush=True)
 
 
+def serving_mix(n_jobs, seed, lo=12, hi=22, sumcheck_every=5):
+    """Job kinds and log sizes of the serving stream: commit-and-fold jobs with log
+    codeword sizes in [lo, hi], P(k) proportional to 2^-(k-lo)/2, and one M31
+    multilinear sum-check over 2^20 evaluations after every four of them."""
+    ks = np.arange(lo, hi + 1)
+    w = 2.0 ** (-(ks - lo) / 2.0)
+    cdf = np.cumsum(w / w.sum())
+    u = (splitmix64(seed, n_jobs) >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+    jobs = []
+    for i in range(n_jobs):
+        if i % sumcheck_every == sumcheck_every - 1:
+            jobs.append(("sc", 20))
+        else:
+            jobs.append(("pcs", int(ks[min(len(ks) - 1, int(np.searchsorted(cdf, u[i], side="right")))])))
+    return jobs
+
+
+def run_serving(azk, ctx, args):
+    """Continuous-batching server on the serving mix: a saturated backlog gives the
+    server's throughput on this mix; Poisson arrivals at `--serve-load` of it give
+    p50/p99 latency (completion - arrival).  Every job's bytes are those of the
+    same job alone (tests/test_gpu_server.py)."""
+    final_log, queries, blowup = args.final_log, 64, 2
+    rng_rows = {k: None for k in range(12, 23)}
+    for k in rng_rows:
+        r = np.zeros(((1 << k) >> 2, 4), np.uint32)
+        r[:, 0] = uniform_m31(SEED ^ (0x5E7 + k), len(r))
+        rng_rows[k] = r
+    sc_tables = [uniform_m31(SEED ^ (0x5C0 + i), 1 << 20) for i in range(2)]
+    pubs = public_digests(4096, SEED ^ 0x5E)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), slots=args.serve_slots,
+                             schedule=dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=0))
+
+    def submit(job, i):
+        kind, k = job
+        if kind == "sc":
+            return server.submit_sumcheck(sc_tables[i % 2])
+        return server.submit_pcs(k, blowup, queries, k - final_log, rng_rows[k], pubs[32 * (i % 4096):32 * (i % 4096) + 32])
+
+    def collect(ids):
+        server.wait_all()
+        return [server.poll(j) for j in ids]
+
+    # warm every worker's resident shapes: one burst of `slots` jobs per shape
+    t0 = time.perf_counter()
+    warm = []
+    for k in range(12, 23):
+        warm += [submit(("pcs", k), i) for i in range(args.serve_slots)]
+        collect(warm)
+        warm = []
+    collect([submit(("sc", 20), i) for i in range(args.serve_slots)])
+    t_warm = time.perf_counter() - t0
+
+    # saturated backlog: the server's throughput on this mix
+    mix = serving_mix(args.serve_backlog, SEED ^ 0xB1)
+    s0 = server.stats()
+    t0 = time.perf_counter()
+    ids = [submit(j, i) for i, j in enumerate(mix)]
+    res = collect(ids)
+    t_sat = time.perf_counter() - t0
+    s1 = server.stats()
+    sat_elems = s1["pcs_elements"] - s0["pcs_elements"]
+    sat_jobs_s = len(mix) / t_sat
+    sat_elems_s = sat_elems / t_sat
+
+    # Poisson arrivals at a fraction of that rate
+    lam = args.serve_load * sat_jobs_s
+    n = max(50, int(lam * args.serve_seconds))
+    mix = serving_mix(n, SEED ^ 0xA7)
+    gaps = -np.log1p(-((splitmix64(SEED ^ 0x9A, n) >> np.uint64(11)).astype(np.float64) / float(1 << 53))) / lam
+    arrivals = np.cumsum(gaps)
+    s0 = server.stats()
+    ids, lags = [], []
+    t0 = time.perf_counter()
+    for i, (job, at) in enumerate(zip(mix, arrivals)):
+        while True:
+            now = time.perf_counter() - t0
+            if now >= at:
+                break
+            if at - now > 2e-3:
+                time.sleep(at - now - 1e-3)
+        ids.append(submit(job, i))
+        lags.append(time.perf_counter() - t0 - at)
+    res = collect(ids)
+    t_run = time.perf_counter() - t0
+    s1 = server.stats()
+    lat = np.array([r[1] + lag for r, lag in zip(res, lags)])
+    kinds = np.array([j[0] for j in mix])
+    server.close()
+
+    def pct(v):
+        return {"p50_ms": float(np.percentile(v, 50) * 1e3), "p99_ms": float(np.percentile(v, 99) * 1e3), "jobs": int(len(v))} if len(v) else None
+
+    return {
+        "mix": "commit-and-fold jobs log U*[12,22] with P(k) ~ 2^-(k-12)/2 (blowup 4, fold to log 6, 64 queries) : "
+               "M31 multilinear sum-check over 2^20 evaluations = 4:1",
+        "slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb,
+        "saturated": {"jobs_per_s": sat_jobs_s, "elems_per_s": sat_elems_s, "jobs": args.serve_backlog, "seconds": t_sat},
+        "offered_load": args.serve_load, "arrival_rate_jobs_per_s": lam,
+        "throughput_elems_per_s": (s1["pcs_elements"] - s0["pcs_elements"]) / t_run, "jobs_per_s": len(mix) / t_run,
+        "latency_all": pct(lat), "latency_pcs": pct(lat[kinds == "pcs"]), "latency_sumcheck": pct(lat[kinds == "sc"]),
+        "submit_lag_p99_ms": float(np.percentile(lags, 99) * 1e3), "warmup_s": t_warm,
+        "held_gb": s1["held_bytes"] / 2**30,
+    }
+
+
 def plain_values_ok(v):
     return v is not None and v > 0
 
@@ -273,6 +379,13 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--cpu-budget-elems", type=int, default=1 << 21)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--e2e-pipeline", type=int, default=1)
+    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-backlog", type=int, default=1000)
+    ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
     args = ap.parse_args()
 
     world, rank, local, dist = dist_setup(args)
@@ -338,7 +451,45 @@ def main():
         azk._capi.check(azk.lib().azk_batch_download_proofs(batch._h, ctypes.c_void_p(proof_host.data_ptr()), batch.proof_total), ctx.handle)
         e2e_times.append(time.perf_counter() - t0)
     t_e2e = max_over_ranks(dist, statistics.median(e2e_times), local)
-    e2e_value = world * elems / t_e2e
+    e2e_serial = world * elems / t_e2e
+
+    # ---- pipelined end to end: two provers alternate, so one step's copies
+    # overlap the other's kernels (every step still uploads its inputs from
+    # pinned host memory and reads its proofs back) ----
+    e2e_pipe = None
+    if args.e2e_pipeline:
+        batch2 = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=sched)
+        batch2.upload(host_rows, offsets, counts)
+        batch2.prove(pubs)
+        proof_host2 = torch.empty(max(1, batch.proof_total), dtype=torch.uint8, pin_memory=True)
+        lanes = [(batch, proof_host), (batch2, proof_host2)]
+        per_lane = max(1, args.steps // 2)
+        errors = []
+
+        def lane(b, ph):
+            try:
+                for _ in range(per_lane):
+                    b.upload(host_rows, offsets, counts)
+                    b.prove(pubs)
+                    azk._capi.check(azk.lib().azk_batch_download_proofs(b._h, ctypes.c_void_p(ph.data_ptr()), b.proof_total), ctx.handle)
+            except Exception as exc:  # surfaced below
+                errors.append(exc)
+
+        barrier(dist)
+        t0 = time.perf_counter()
+        threads = [threading.Thread(target=lane, args=ln) for ln in lanes]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        t_pipe = time.perf_counter() - t0
+        if errors:
+            raise errors[0]
+        t_pipe = max_over_ranks(dist, t_pipe / (2 * per_lane), local)
+        e2e_pipe = world * elems / t_pipe
+        del batch2
+    e2e_value = e2e_pipe if e2e_pipe else e2e_serial
+    t_e2e_report = world * elems / e2e_value
 
     # ---- plain per-instance form, same instances ----
     plain_times = []
@@ -350,6 +501,7 @@ def main():
           file=sys.stderr, flush=True)
     plain_value = world * elems / t_plain if plain_times else None
 
+    proof_total = batch.proof_total
     # ---- rooflines ----
     int_ops = azk.probe_int_issue(ctx)
     perm_peak = int_ops / 4320.0
@@ -358,6 +510,13 @@ def main():
     hbm_gbs, hbm_kind = measured_peaks()
     fft_gbs = work["fft_bytes"] / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
     traffic = profile_traffic()
+
+    serving = None
+    if not args.no_serve and world == 1:
+        del batch
+        batch = None
+        serving = run_serving(azk, ctx, args)
+        print(f"[bench] serving {serving}", file=sys.stderr, flush=True)
 
     line = None
     if rank == 0:
@@ -374,7 +533,9 @@ def main():
             "dtype": "u32/u64 (M31/QM31 field, Keccak lanes)", "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": 1000 * t_plain if plain_values_ok(plain_value) else None,
                       "batched_over_plain": value / plain_value if plain_values_ok(plain_value) else None},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e_report,
+                    "mode": "two provers alternating (copies of one step overlap kernels of the other)" if e2e_pipe else "serial",
+                    "serial_value": e2e_serial, "serial_ms_per_step": 1000 * t_e2e},
             "roofline": {
                 "bound": "int32-issue", "kernel": "tree_tiles_kernel (fold + leaf hash + treelet + upper tree + transcript)",
                 "achieved": tree_rate / 1e9, "peak": perm_peak / 1e9, "unit": "Gperm/s", "frac": tree_rate / perm_peak if perm_peak else None,
@@ -392,7 +553,8 @@ def main():
             "gpu_launches": work["launches"] * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
-            "proof_bytes_per_step": batch.proof_total,
+            "proof_bytes_per_step": proof_total,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     del batch

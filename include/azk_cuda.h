@@ -195,6 +195,9 @@ typedef struct azk_schedule {
   uint32_t group_log;     /* upper-level group size (1..treelet_log); 0 = default */
   uint32_t threads;       /* threads per CTA for hashing kernels: 128, 256 or 512; 0 = default */
   uint32_t use_graph;     /* batched form: capture the superstep in a CUDA graph */
+  /* Per-layer override: layer_treelet[L] (nonzero) is the treelet depth for a
+   * committed layer of 2^L leaves; the autotuner fills this table. */
+  uint8_t layer_treelet[32];
 } azk_schedule;
 
 azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,
@@ -226,7 +229,10 @@ void azk_pcs_prover_destroy(azk_pcs_prover* p);
 azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* log_sizes, const uint32_t* rounds, uint32_t log_blowup,
                             uint32_t queries, const azk_schedule* schedule, azk_batch** out);
 /* Device pointer of instance i's coefficient input (N_i QM31); the caller may
- * fill it in place (resident input). */
+ * fill it in place (resident input).  Fetching the pointer drops what the last
+ * azk_batch_upload learned about that input (its nonzero prefix, whether it is a
+ * lifted M31 polynomial): fetch it again after every upload before writing
+ * through it. */
 azk_status azk_batch_input(azk_batch* b, uint32_t index, void** dev_input);
 /* Copy coefficients from the host: instance i's coefficient_counts[i] leading
  * values start at host_coefficients + 4 * offsets[i] (u32 words / 4). */
@@ -248,6 +254,64 @@ azk_status azk_batch_profile(azk_batch* b, double* seconds4);
  * single-pass FFT bytes, final-fold bytes, and kernel launches per superstep. */
 azk_status azk_batch_work(azk_batch* b, uint64_t* tree_permutations, uint64_t* fft_bytes, uint64_t* fold_bytes, uint32_t* launches);
 void azk_batch_destroy(azk_batch* b);
+
+/* ---- M31 multilinear sum-check (M31MultilinearSumcheckProofBuilderV1.prove,
+ * SumcheckOracle.swift:797-868) ----
+ * `count` (a power of two > 1) canonical M31 evaluations; writes the per-round
+ * sums over the even (sums0) and odd (sums1) entries, the transcript challenges
+ * (log2(count) each), the claimed sum, the final folded evaluation and the
+ * statement's word digest (SHA3-256 of the framed evaluations). */
+azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evaluations, uint64_t count, uint32_t* sums0, uint32_t* sums1, uint32_t* challenges,
+                              uint32_t* claimed_sum, uint32_t* final_evaluation, uint8_t digest[32], azk_stats* stats);
+
+/* ---- continuous-batching server (no counterpart in the reference) ----
+ * Jobs enter one FIFO queue; `slots` workers, each with its own CUDA stream, take
+ * the next job as soon as its device memory fits `hbm_budget_bytes`, so jobs that
+ * arrive while others run are admitted as slots and memory free up and their
+ * kernels overlap on the device.  A job larger than the whole budget is refused
+ * with AZK_ERR_HBM_BUDGET at submission.  Results equal those of the single-job
+ * entry points (each job's kernels are the same; only their overlap differs). */
+typedef struct azk_server azk_server;
+azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t slots, const azk_schedule* schedule, azk_server** out);
+/* Circle PCS proof from `count` leading FFT-basis coefficients (rest zero). */
+azk_status azk_server_submit_pcs(azk_server* sv, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t rounds, const uint32_t* coefficients,
+                                 uint64_t count, const uint8_t public_digest[32], uint64_t* job_id);
+/* M31 multilinear sum-check over `count` (power of two) evaluations
+ * (M31MultilinearSumcheckProofBuilderV1, SumcheckOracle.swift:797-868). */
+azk_status azk_server_submit_sumcheck(azk_server* sv, const uint32_t* evaluations, uint64_t count, uint64_t* job_id);
+/* state: 0 queued, 1 running, 2 done, 3 failed.  Done: latency = completion -
+ * submission; result = proof bytes (PCS) or u32 words {claimed sum, final
+ * evaluation, digest[8], sums at 0 [rounds], sums at 1 [rounds], challenges [rounds]}
+ * (sum-check); pass out = NULL to learn *out_len. */
+azk_status azk_server_poll(azk_server* sv, uint64_t job_id, int* state, double* latency_s, uint8_t* out, uint64_t* out_len);
+azk_status azk_server_release(azk_server* sv, uint64_t job_id);
+azk_status azk_server_wait_all(azk_server* sv);
+azk_status azk_server_stats(azk_server* sv, uint64_t* completed, uint64_t* elems, double* span_s, uint64_t* reserved_bytes);
+void azk_server_destroy(azk_server* sv);
+
+/* ---- autotuner and learned cost model (the reference's planner races a few
+ * Merkle schedules, Planner/MetalProofPlanner.swift:20-615; this replaces it) ---- */
+
+/* Median device time of one commit-kernel launch over `concurrent` independent
+ * trees of 2^log_leaves leaves: leaf_bytes 16 (QM31 leaves; fold != 0 computes
+ * each leaf as a fold of a previous layer first) or 64 (raw 64-byte leaves). */
+azk_status azk_tuner_time_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent, uint32_t tile_log,
+                               uint32_t group_log, uint32_t threads, uint32_t reps, double* seconds);
+
+typedef struct azk_mlp azk_mlp;
+/* Fully connected network dims[0] -> ... -> dims[n_layers] (= 1), ReLU hidden
+ * layers, fp32, trained on the device by hand-written forward/backward/Adam kernels. */
+azk_status azk_mlp_create(azk_ctx* ctx, uint32_t n_layers, const uint32_t* dims, uint64_t seed, azk_mlp** out);
+uint64_t azk_mlp_param_count(azk_mlp* mlp);
+/* Parameters: per layer, weights [out][in] then biases [out]. */
+azk_status azk_mlp_get_params(azk_mlp* mlp, float* params, uint64_t count);
+azk_status azk_mlp_set_params(azk_mlp* mlp, const float* params, uint64_t count);
+azk_status azk_mlp_forward(azk_mlp* mlp, const float* x, uint64_t rows, float* y);
+/* Mean-squared-error loss and its gradient with respect to every parameter. */
+azk_status azk_mlp_gradients(azk_mlp* mlp, const float* x, const float* y, uint64_t rows, float* loss, float* grads);
+/* `steps` full-batch Adam steps (lr, betas 0.9/0.999); returns the final loss. */
+azk_status azk_mlp_train(azk_mlp* mlp, const float* x, const float* y, uint64_t rows, uint32_t steps, float lr, float* final_loss);
+void azk_mlp_destroy(azk_mlp* mlp);
 
 #ifdef __cplusplus
 }

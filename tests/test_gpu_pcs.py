@@ -155,3 +155,63 @@ def test_batch_graph_replay_and_plain_agree(ctx):
     assert b.proofs() == first
     b.prove(pubs, plain=True)
     assert b.proofs() == first
+
+
+def test_batch_upload_rejects_non_canonical(ctx):
+    logs = [10, 11]
+    flat, offs, cnts = _batch_inputs(logs, 3)
+    b = azk.BatchProver(ctx, logs, [4, 5], 2, 8)
+    b.upload(flat, offs, cnts)
+    bad = flat.copy()
+    bad[offs[1] + cnts[1] - 1, 2] = G.P
+    with pytest.raises(azk.AZKError) as e:
+        b.upload(bad, offs, cnts)
+    assert e.value.name == "invalidInputLayout"
+
+
+@pytest.mark.parametrize("log_size,count_log,rounds", [(5, 3, 2), (12, 10, 6), (13, 11, 7), (16, 14, 9), (20, 18, 14), (23, 21, 17)])
+def test_lifted_m31_coefficients_match_oracle(ctx, oracle, log_size, count_log, rounds):
+    """Coefficients with zero b, c, d limbs and a zero tail take the FFT's M31 path
+    (one limb between passes, tail reads skipped); proofs stay the oracle's."""
+    rng = np.random.default_rng(log_size * 3 + 1)
+    count = 1 << count_log
+    coeffs = np.zeros((count, 4), np.uint32)
+    coeffs[:, 0] = rng.integers(0, G.P, size=count, dtype=np.uint32)
+    pub = rng.integers(0, 256, size=32, dtype=np.uint8).tobytes()
+    p = azk.CirclePCSFRIProver(ctx, log_size, 2, 8, rounds)
+    proof = p.prove_coefficients(coeffs, pub)
+    full = np.zeros((1 << log_size, 4), np.uint32)
+    full[:count] = coeffs
+    ev = oracle.fft_evaluate(log_size, full)
+    assert proof == oracle.prove(log_size, ev, 2, 8, pub, rounds).proof
+    # one nonzero upper limb anywhere switches the same prover back to QM31 arithmetic
+    coeffs[count - 1, 3] = 5
+    full[:count] = coeffs
+    proof = p.prove_coefficients(coeffs, pub)
+    assert proof == oracle.prove(log_size, oracle.fft_evaluate(log_size, full), 2, 8, pub, rounds).proof
+
+
+def test_batch_mixes_m31_and_qm31_instances(ctx, oracle):
+    logs = [14, 13, 9, 15]
+    rounds = [lg - 6 for lg in logs]
+    rng = np.random.default_rng(21)
+    flat, offs, cnts = _batch_inputs(logs, 9)
+    flat[offs[0]:offs[0] + cnts[0], 1:] = 0   # instance 0: lifted M31
+    flat[offs[2]:offs[2] + cnts[2], 1:] = 0   # instance 2: lifted M31 (single pass)
+    b = azk.BatchProver(ctx, logs, rounds, 2, 8)
+    b.upload(flat, offs, cnts)
+    pubs = rng.integers(0, 256, size=32 * len(logs), dtype=np.uint8).tobytes()
+    b.prove(pubs)
+    proofs = b.proofs()
+    for i, lg in enumerate(logs):
+        full = np.zeros((1 << lg, 4), np.uint32)
+        full[:cnts[i]] = flat[offs[i]:offs[i] + cnts[i]]
+        assert proofs[i] == oracle.prove(lg, oracle.fft_evaluate(lg, full), 2, 8, pubs[32 * i:32 * i + 32], rounds[i]).proof, i
+    # writing through the input pointer makes the batch forget the upload's description
+    import ctypes
+    ptr = b.input_pointer(0)
+    full = rng.integers(0, G.P, size=(1 << logs[0], 4), dtype=np.uint32)
+    azk._capi.check(azk.lib().azk_buf_upload(ctx.handle, ctypes.c_void_p(ptr), 0, full.ctypes.data, full.nbytes), ctx.handle)
+    b.prove(pubs)
+    want = oracle.prove(logs[0], oracle.fft_evaluate(logs[0], full), 2, 8, pubs[:32], rounds[0]).proof
+    assert b.proofs()[0] == want

@@ -1,0 +1,107 @@
+"""GPU: the continuous-batching server returns, for every job of a mixed stream
+(Circle PCS proofs of uneven sizes and M31 multilinear sum-checks), exactly the
+result the same job gives alone, admits jobs under its HBM budget and refuses a
+job larger than the budget."""
+import time
+
+import numpy as np
+import pytest
+
+import apple_b200 as azk
+
+pytestmark = pytest.mark.gpu
+P = (1 << 31) - 1
+
+
+def _pcs_job(rng, log_size):
+    rounds = min(8, log_size)
+    count = 1 << (log_size - 2)
+    coeffs = rng.integers(0, P, (count, 4), dtype=np.uint32)
+    pub = rng.integers(0, 256, 32, dtype=np.uint8).tobytes()
+    return dict(kind="pcs", log_size=log_size, rounds=rounds, queries=32, coeffs=coeffs, pub=pub)
+
+
+def _wait(server, ids, timeout=120.0):
+    out, t0 = {}, time.time()
+    while len(out) < len(ids):
+        for j in ids:
+            if j not in out:
+                r = server.poll(j)
+                if r is not None:
+                    out[j] = r
+        assert time.time() - t0 < timeout
+        time.sleep(0.001)
+    return out
+
+
+def test_mixed_stream_matches_alone(ctx, oracle):
+    rng = np.random.default_rng(0x5E4)
+    jobs = []
+    for k in range(20):
+        if k % 5 == 4:
+            jobs.append(dict(kind="sc", ev=rng.integers(0, P, 1 << int(rng.integers(10, 17)), dtype=np.uint32)))
+        else:
+            jobs.append(_pcs_job(rng, int(rng.integers(10, 19))))
+    server = azk.ProofServer(ctx, hbm_budget_bytes=8 << 30, slots=4)
+    ids = []
+    for j in jobs:
+        if j["kind"] == "pcs":
+            ids.append(server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]))
+        else:
+            ids.append(server.submit_sumcheck(j["ev"]))
+    res = _wait(server, ids)
+    server.wait_all()
+    st = server.stats()
+    assert st["completed"] == len(jobs)
+    server.close()
+    for j, i in zip(jobs, ids):
+        got, lat = res[i]
+        assert lat > 0
+        if j["kind"] == "pcs":
+            alone = azk.CirclePCSFRIProver(ctx, j["log_size"], 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])
+            assert got == alone
+            assert oracle.verify(got, j["pub"])
+        else:
+            alone = azk.sumcheck_prove(ctx, j["ev"])
+            for key in ("claimed_sum", "final", "initial_digest"):
+                assert got[key] == alone[key]
+            for key in ("r0", "r1", "challenges"):
+                assert np.array_equal(got[key], alone[key])
+
+
+def test_pcs_job_matches_oracle_proof(ctx, oracle):
+    rng = np.random.default_rng(7)
+    j = _pcs_job(rng, 12)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=1 << 30, slots=2)
+    jid = server.submit_pcs(12, 2, j["queries"], j["rounds"], j["coeffs"], j["pub"])
+    (proof, _), = _wait(server, [jid]).values()
+    server.close()
+    full = np.zeros((1 << 12, 4), np.uint32)
+    full[:len(j["coeffs"])] = j["coeffs"]
+    ev = oracle.fft_evaluate(12, full)
+    assert proof == oracle.prove(12, ev, 2, j["queries"], j["pub"], j["rounds"]).proof
+
+
+def test_budget_admission_and_refusal(ctx):
+    rng = np.random.default_rng(11)
+    # one log-16 PCS shape is about 7.5 MiB: a 12 MiB budget runs one at a time
+    server = azk.ProofServer(ctx, hbm_budget_bytes=12 << 20, slots=4)
+    with pytest.raises(azk.AZKError) as e:
+        server.submit_pcs(20, 2, 32, 8, rng.integers(0, P, (16, 4), dtype=np.uint32), bytes(32))
+    assert e.value.name == "hbmBudget"
+    jobs = [_pcs_job(rng, 16) for _ in range(6)]
+    ids = [server.submit_pcs(16, 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]) for j in jobs]
+    res = _wait(server, ids)
+    assert server.stats()["held_bytes"] <= 12 << 20
+    server.close()
+    for j, i in zip(jobs, ids):
+        assert res[i][0] == azk.CirclePCSFRIProver(ctx, 16, 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])
+
+
+def test_bad_jobs_are_refused_at_submission(ctx):
+    server = azk.ProofServer(ctx, hbm_budget_bytes=1 << 30, slots=1)
+    with pytest.raises(azk.AZKError):
+        server.submit_sumcheck(np.zeros(3, np.uint32))
+    with pytest.raises(azk.AZKError):
+        server.submit_pcs(10, 2, 8, 4, np.full((4, 4), P, np.uint32), bytes(32))
+    server.close()
