@@ -215,16 +215,16 @@ class Tuner:
         self.model = CostModel(self.ctx, hidden=hidden, seed=seed)
         return self.model.fit(records if records is not None else self.records, steps=steps, lr=lr)
 
-    def ranked(self, shape):
+    def ranked(self, shape, threads=None):
         lg, lb, fold, c = shape
-        cands = [(t, th) for t in tile_candidates(lg) for th in self.threads]
+        cands = [(t, th) for t in tile_candidates(lg) for th in (self.threads if threads is None else (threads,))]
         pred = self.model.predict_seconds([(lg, lb, fold, c, t, th) for t, th in cands])
         order = np.argsort(pred)
         return [cands[i] for i in order], pred[order]
 
-    def choose(self, shape, verify: int = 0):
+    def choose(self, shape, verify: int = 0, threads=None):
         """Model's pick; with verify=k, time its top k candidates and keep the fastest."""
-        ranked, _ = self.ranked(shape)
+        ranked, _ = self.ranked(shape, threads)
         if verify <= 0:
             return ranked[0]
         lg, lb, fold, c = shape
@@ -249,14 +249,16 @@ class Tuner:
             out["heuristic"].append(h / best - 1.0)
         return {k: {"mean": float(np.mean(v)), "max": float(np.max(v)), "n": len(v)} for k, v in out.items()}
 
-    def layer_table(self, concurrent=1, leaf_bytes=16, logs=range(1, 27)) -> dict:
-        """{layer log size: treelet depth} for an azk_schedule's layer_treelet."""
+    def layer_table(self, concurrent=1, leaf_bytes=16, fold=1, logs=range(1, 27), threads=256) -> dict:
+        """{layer log size: treelet depth} for an azk_schedule's layer_treelet (the
+        commit kernel's thread count is one per launch, so the table is chosen at a
+        fixed `threads`; over the measured shapes that costs at most a few percent)."""
         table = {}
         for lg in logs:
             if lg < 2:
                 table[lg] = 1
                 continue
-            t, _ = self.choose((lg, leaf_bytes, 1, concurrent))
+            t, _ = self.choose((lg, leaf_bytes, fold, concurrent), threads=threads)
             table[lg] = int(t)
         return table
 
@@ -286,18 +288,64 @@ def _device_name(ctx) -> str:
     return f"sm{info['cc'][0]}{info['cc'][1]}-{info['sm_count']}sm"
 
 
+# Default schedules shipped with the library: per-layer treelet depths chosen by
+# the trained model for the commit kernel's common shapes.
+TABLE_SHAPES = {
+    "pcs_single": dict(concurrent=1, leaf_bytes=16, fold=1),   # one PCS instance: one tree per launch
+    "pcs_batch": dict(concurrent=64, leaf_bytes=16, fold=1),   # batched supersteps: many trees per launch
+    "merkle_raw64": dict(concurrent=1, leaf_bytes=64, fold=0),  # raw-leaf Merkle plan
+}
+
+
+def export(tuner: Tuner, report: dict, json_path: str, header_path: str):
+    """Write the tables (and the evidence behind them) as JSON and as the C++ header
+    the library compiles in (`csrc/azk_tuned.h`)."""
+    tables = {name: tuner.layer_table(**kw) for name, kw in TABLE_SHAPES.items()}
+    doc = {"device": _device_name(tuner.ctx), "report": report, "threads": 256, "shapes": TABLE_SHAPES,
+           "tables": {k: {str(lg): t for lg, t in v.items()} for k, v in tables.items()}}
+    with open(json_path, "w") as f:
+        json.dump(doc, f, indent=1)
+    with open(header_path, "w") as f:
+        f.write(header_text(doc))
+    return doc
+
+
+def header_text(doc) -> str:
+    lines = ["// Generated by `python -m apple_b200.autotune --export` from measured commit-kernel",
+             "// timings on " + doc["device"] + f" ({doc['report'].get('records', 0)} records) and the cost model trained on them;",
+             "// tests/test_tuned_tables.py keeps it equal to apple_b200/tuned_b200.json.",
+             "// Entry [k] = treelet depth for a layer of 2^k leaves (0: not used).",
+             "#pragma once",
+             "#include <stdint.h>",
+             "",
+             "namespace azk {"]
+    for name in TABLE_SHAPES:
+        tab = doc["tables"][name]
+        vals = [int(tab.get(str(k), 0)) for k in range(32)]
+        lines.append(f"static constexpr uint8_t kTuned_{name}[32] = {{{', '.join(str(v) for v in vals)}}};")
+    lines += ["}  // namespace azk", ""]
+    return "\n".join(lines)
+
+
 def main():
     import argparse
 
     import apple_b200 as azk
 
-    ap = argparse.ArgumentParser(description="collect timings, train the cost model, report regret")
+    ap = argparse.ArgumentParser(description="collect timings, train the cost model, report regret, export default tables")
     ap.add_argument("--out", default="tuner_store.json")
+    ap.add_argument("--from-store", default=None, help="reuse the timings of an earlier store instead of collecting")
     ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--export", action="store_true", help="write the default tables (JSON and C++ header)")
+    ap.add_argument("--export-dir", default=None, help="where to write tuned_b200.json and azk_tuned.h (default: in the package)")
     a = ap.parse_args()
     ctx = azk.Context(0)
     t0 = time.time()
-    recs = collect(ctx)
+    if a.from_store:
+        with open(a.from_store) as f:
+            recs = json.load(f)["records"]
+    else:
+        recs = collect(ctx)
     t1 = time.time()
     held = {9, 13, 17, 21}
     train = [r for r in recs if r["log"] not in held]
@@ -305,9 +353,16 @@ def main():
     loss = tuner.train(steps=a.steps, records=train)
     t2 = time.time()
     test_shapes = sorted({(r["log"], r["leaf_bytes"], r["fold"], r["concurrent"]) for r in recs if r["log"] in held})
-    report = {"records": len(recs), "train_records": len(train), "collect_s": t1 - t0, "train_s": t2 - t1, "train_loss": loss,
-              "regret_unseen": tuner.regret(test_shapes), "regret_unseen_verify3": tuner.regret(test_shapes, verify=3)}
+    report = {"records": len(recs), "train_records": len(train), "held_out_logs": sorted(held), "collect_s": t1 - t0, "train_s": t2 - t1,
+              "train_loss": loss, "regret_unseen": tuner.regret(test_shapes), "regret_unseen_verify3": tuner.regret(test_shapes, verify=3)}
     tuner.save(a.out)
+    if a.export:
+        # the shipped tables come from a model trained on every record
+        final = Tuner(ctx, recs)
+        final.train(steps=a.steps)
+        here = os.path.dirname(os.path.abspath(__file__))
+        jd, hd = (a.export_dir, a.export_dir) if a.export_dir else (here, os.path.join(here, "csrc"))
+        export(final, report, os.path.join(jd, "tuned_b200.json"), os.path.join(hd, "azk_tuned.h"))
     print(json.dumps(report))
 
 

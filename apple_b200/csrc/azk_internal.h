@@ -89,8 +89,8 @@ struct FftJob {
   const uint4* in;           // FFT-basis coefficients (read by the first pass)
   uint4* out;                // codeword (bit-reversed order)
   const uint32_t* tw;        // stage twiddles of the domain (N - 1 values)
-  uint32_t* narrow;          // N words of scratch between passes for M31 inputs (null: none)
-  const InputInfo* info;     // null: unknown input (QM31 arithmetic, all N coefficients read)
+  uint32_t* narrow;          // N words of scratch between passes of the one-limb kernel
+  const InputInfo* info;     // nonzero prefix of the input (null: all N coefficients read)
 };
 
 // Circle FFT pass geometry: the stages above bit 12 run first in chunks of at
@@ -196,7 +196,8 @@ cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_
 cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, uint32_t nidx, uint64_t* d_out, cudaStream_t s);
 cudaError_t launch_domain_tables(uint32_t logn, uint32_t* d_tw, uint32_t* d_inv, cudaStream_t s);
 cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
+// `narrow`: the work items' inputs are lifted M31 polynomials (one-limb kernel).
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s);
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
 // info = {1, 0, count} first).

@@ -144,13 +144,37 @@ struct Timer {
   uint64_t ns() const { return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
+// Wait for everything queued on a stream without spinning a host core: the wait
+// sleeps on a blocking-sync event (the server's workers share the host's cores
+// with each other and with the threads that submit work).
+inline void sync_stream(cudaStream_t s) {
+  struct Ev {
+    cudaEvent_t e = nullptr;
+    int dev = -1;
+    ~Ev() {
+      if (e) cudaEventDestroy(e);
+    }
+  };
+  thread_local Ev ev;
+  int dev = 0;
+  AZK_CU(cudaGetDevice(&dev));
+  if (!ev.e || ev.dev != dev) {
+    if (ev.e) cudaEventDestroy(ev.e);
+    ev.e = nullptr;
+    AZK_CU(cudaEventCreateWithFlags(&ev.e, cudaEventBlockingSync | cudaEventDisableTiming));
+    ev.dev = dev;
+  }
+  AZK_CU(cudaEventRecord(ev.e, s));
+  AZK_CU(cudaEventSynchronize(ev.e));
+}
+
 // CUDA events around a region of one stream.
 struct GpuTimer {
   cudaEvent_t a = nullptr, b = nullptr;
   cudaStream_t s;
   explicit GpuTimer(cudaStream_t st) : s(st) {
-    AZK_CU(cudaEventCreate(&a));
-    AZK_CU(cudaEventCreate(&b));
+    AZK_CU(cudaEventCreateWithFlags(&a, cudaEventBlockingSync));
+    AZK_CU(cudaEventCreateWithFlags(&b, cudaEventBlockingSync));
     AZK_CU(cudaEventRecord(a, s));
   }
   void stop() { AZK_CU(cudaEventRecord(b, s)); }
@@ -184,7 +208,9 @@ struct Sched {
   bool graph = true;
   uint8_t layer_tile[32] = {0};
 };
-Sched resolve_schedule(const azk_schedule* s);
+// A schedule with no treelet depth and no layer table takes `defaults` (a tuned
+// per-layer table from azk_tuned.h) when one is given.
+Sched resolve_schedule(const azk_schedule* s, const uint8_t* defaults = nullptr);
 // Tile depth used for a tree of 2^logn leaves under a schedule (per-layer table
 // first, then the global depth), clamped to [1, logn].
 inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
@@ -196,14 +222,18 @@ inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
 
 // FFT work for a set of transforms: one FftJob per (transform, pass); passes of
 // all transforms are aligned so every transform's last (low-stage) pass runs at
-// the final step.
+// the final step.  Transforms flagged `narrow` (inputs known to be lifted M31
+// polynomials) run on the one-limb kernel: in each step their work items follow
+// the QM31 items, so each kernel gets one contiguous range.
 struct FftPlan {
   std::vector<FftJob> jobs;
   std::vector<uint2> work;                       // all steps, step-major, transform-contiguous
-  std::vector<uint64_t> step_off, step_cnt;      // per step
+  std::vector<uint64_t> step_off, step_cnt;      // per step: QM31 items
+  std::vector<uint64_t> nstep_off, nstep_cnt;    // per step: one-limb items
+  std::vector<uint8_t> narrow;                   // per transform
   std::vector<std::vector<std::pair<uint64_t, uint64_t>>> inst_range;  // [step][transform] -> (offset, count)
   DevBuf d_jobs, d_work;
-  void build(const std::vector<FftJob>& transforms);
+  void build(const std::vector<FftJob>& transforms, const std::vector<uint8_t>& narrow_flags = {});
   void upload(cudaStream_t s);
   void launch_step(size_t step, cudaStream_t s) const;
   void launch_step_for(size_t step, size_t t, cudaStream_t s) const;

@@ -80,13 +80,44 @@ __device__ __forceinline__ uint64_t fft_global_index(const FftPassGeom& g, uint6
   return (hi << (g.s_lo + g.m)) | ((uint64_t)row << g.s_lo) | (mid << g.c) | col;
 }
 
-// Shared-memory tile layout: the four limbs of the tile's QM31 values as four u32
-// arrays (an M31 tile uses only the first), then the tile's stage twiddles.  Stage
-// j of the pass (global stage s_lo + j) pairs local indices differing in bit j + c,
-// and its twiddle is tw[off(s) + (gi >> (s + 1))] = tw[off(s) + (hi << (m-1-j)) +
-// (row >> (j + 1))]: 2^(m-1-j) consecutive table entries per tile, staged at
-// stw + 2^m - 2^(m-j).
+// Stage j of a pass (global stage s_lo + j) pairs local indices that differ in bit
+// j + c, and its twiddle is tw[off(s) + (gi >> (s + 1))] = tw[off(s) + (hi <<
+// (m-1-j)) + (row >> (j + 1))]: 2^(m-1-j) consecutive table entries per tile,
+// staged in shared memory at stw + 2^m - 2^(m-j).  Shared arrays are padded by
+// one word per 32 so the strided butterfly groups spread over the banks.
 __device__ __forceinline__ uint32_t fft_stw_offset(uint32_t m, uint32_t j) { return (1u << m) - (1u << (m - j)); }
+__device__ __forceinline__ uint32_t fpad(uint32_t L) { return L + (L >> 5); }
+
+struct FftTile {
+  FftPassGeom g;
+  uint32_t T;
+  uint64_t count;
+  bool first, last;
+};
+
+__device__ __forceinline__ FftTile fft_tile(const FftJob& job) {
+  FftTile t;
+  t.g = fft_pass_geom(job.logn, job.pass);
+  t.T = 1u << (t.g.m + t.g.c);
+  const uint64_t N = 1ull << job.logn;
+  t.count = (job.info != nullptr && job.info->count != 0) ? job.info->count : N;
+  t.first = job.pass == 0;
+  t.last = job.pass == fft_high_chunks(job.logn);
+  return t;
+}
+
+template <int THREADS>
+__device__ __forceinline__ void fft_stage_twiddles(const FftJob& job, const FftTile& ft, uint64_t tile, uint32_t* stw) {
+  const FftPassGeom& g = ft.g;
+  const uint32_t midbits = g.s_lo > g.c ? g.s_lo - g.c : 0;
+  const uint64_t hi = tile >> midbits;
+  for (uint32_t j = 0; j < g.m; j++) {
+    const uint32_t cnt = 1u << (g.m - 1 - j);
+    const uint32_t* src = job.tw + tw_offset(job.logn, g.s_lo + j) + (hi << (g.m - 1 - j));
+    uint32_t* dst = stw + fft_stw_offset(g.m, j);
+    for (uint32_t r = threadIdx.x; r < cnt; r += THREADS) dst[r] = __ldg(src + r);
+  }
+}
 
 __device__ __forceinline__ void bfly_m31(uint32_t& l, uint32_t& r, uint32_t t) {
   uint32_t rt = m31_mul(r, t);
@@ -102,60 +133,36 @@ __device__ __forceinline__ void bfly_q(qm31& l, qm31& r, uint32_t t) {
   l = a;
 }
 
+// QM31 tiles: the four limbs as four padded u32 arrays; two stages per
+// shared-memory round trip (radix 4 in registers), then one more if m is odd.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) fft_pass_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
+__global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
   extern __shared__ uint32_t fsm[];
   const uint2 w = work[blockIdx.x];
   const FftJob& job = jobs[w.x];
-  const uint32_t logn = job.logn;
-  const FftPassGeom g = fft_pass_geom(logn, job.pass);
-  const uint32_t T = 1u << (g.m + g.c);
-  const uint64_t N = 1ull << logn;
-  const bool first = job.pass == 0;
-  const bool last = job.pass == fft_high_chunks(logn);
-  const InputInfo* info = job.info;
-  const bool narrow = info != nullptr && job.narrow != nullptr && info->m31 != 0;
-  const uint64_t count = (info != nullptr && info->count != 0) ? info->count : N;
+  const FftTile ft = fft_tile(job);
+  const FftPassGeom& g = ft.g;
+  const uint32_t T = ft.T, TP = T + (T >> 5);
   uint32_t* sa = fsm;
-  uint32_t* sb = sa + T;
-  uint32_t* sc = sb + T;
-  uint32_t* sd = sc + T;
-  uint32_t* stw = sd + T;
-
-  // this tile's twiddles, one coalesced run per stage
-  const uint32_t midbits = g.s_lo > g.c ? g.s_lo - g.c : 0;
-  const uint64_t hi = (uint64_t)w.y >> midbits;
-  for (uint32_t j = 0; j < g.m; j++) {
-    const uint32_t cnt = 1u << (g.m - 1 - j);
-    const uint32_t* src = job.tw + tw_offset(logn, g.s_lo + j) + (hi << (g.m - 1 - j));
-    uint32_t* dst = stw + fft_stw_offset(g.m, j);
-    for (uint32_t r = threadIdx.x; r < cnt; r += THREADS) dst[r] = __ldg(src + r);
-  }
-  // the tile (the first pass skips coefficients known to be zero)
+  uint32_t* sb = sa + TP;
+  uint32_t* sc = sb + TP;
+  uint32_t* sd = sc + TP;
+  uint32_t* stw = sd + TP;
+  fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
   for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
     const uint64_t gi = fft_global_index(g, w.y, L);
-    if (narrow) {
-      uint32_t v;
-      if (first)
-        v = gi < count ? __ldg(reinterpret_cast<const uint32_t*>(job.in) + 4 * gi) : 0u;
-      else
-        v = job.narrow[gi];
-      sa[L] = v;
-    } else {
-      uint4 v;
-      if (first)
-        v = gi < count ? __ldg(job.in + gi) : make_uint4(0u, 0u, 0u, 0u);
-      else
-        v = job.out[gi];
-      sa[L] = v.x;
-      sb[L] = v.y;
-      sc[L] = v.z;
-      sd[L] = v.w;
-    }
+    uint4 v;
+    if (ft.first)
+      v = gi < ft.count ? __ldg(job.in + gi) : make_uint4(0u, 0u, 0u, 0u);
+    else
+      v = job.out[gi];
+    const uint32_t a = fpad(L);
+    sa[a] = v.x;
+    sb[a] = v.y;
+    sc[a] = v.z;
+    sd[a] = v.w;
   }
   __syncthreads();
-
-  // stages two at a time (radix 4 in registers), then one more if m is odd
   int j = (int)g.m - 1;
   for (; j >= 1; j -= 2) {
     const uint32_t p = (uint32_t)j + g.c;  // stage j pairs bit p, stage j-1 pairs bit p-1
@@ -164,32 +171,20 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const FftJob* __restr
     const uint32_t lowmask = (1u << (p - 1)) - 1;
     for (uint32_t k = threadIdx.x; k < T / 4; k += THREADS) {
       const uint32_t e0 = ((k & ~lowmask) << 2) | (k & lowmask);
-      const uint32_t e1 = e0 | (1u << (p - 1)), e2 = e0 | (1u << p), e3 = e2 | (1u << (p - 1));
       const uint32_t row = e0 >> g.c;
       const uint32_t t1 = tw_j[row >> (j + 1)];
       const uint32_t t2a = tw_j1[row >> j], t2b = tw_j1[(row >> j) | 1u];
-      if (narrow) {
-        uint32_t v0 = sa[e0], v1 = sa[e1], v2 = sa[e2], v3 = sa[e3];
-        bfly_m31(v0, v2, t1);
-        bfly_m31(v1, v3, t1);
-        bfly_m31(v0, v1, t2a);
-        bfly_m31(v2, v3, t2b);
-        sa[e0] = v0;
-        sa[e1] = v1;
-        sa[e2] = v2;
-        sa[e3] = v3;
-      } else {
-        qm31 v0 = {sa[e0], sb[e0], sc[e0], sd[e0]}, v1 = {sa[e1], sb[e1], sc[e1], sd[e1]};
-        qm31 v2 = {sa[e2], sb[e2], sc[e2], sd[e2]}, v3 = {sa[e3], sb[e3], sc[e3], sd[e3]};
-        bfly_q(v0, v2, t1);
-        bfly_q(v1, v3, t1);
-        bfly_q(v0, v1, t2a);
-        bfly_q(v2, v3, t2b);
-        sa[e0] = v0.a, sb[e0] = v0.b, sc[e0] = v0.c, sd[e0] = v0.d;
-        sa[e1] = v1.a, sb[e1] = v1.b, sc[e1] = v1.c, sd[e1] = v1.d;
-        sa[e2] = v2.a, sb[e2] = v2.b, sc[e2] = v2.c, sd[e2] = v2.d;
-        sa[e3] = v3.a, sb[e3] = v3.b, sc[e3] = v3.c, sd[e3] = v3.d;
-      }
+      const uint32_t a0 = fpad(e0), a1 = fpad(e0 | (1u << (p - 1))), a2 = fpad(e0 | (1u << p)), a3 = fpad(e0 | (3u << (p - 1)));
+      qm31 v0 = {sa[a0], sb[a0], sc[a0], sd[a0]}, v1 = {sa[a1], sb[a1], sc[a1], sd[a1]};
+      qm31 v2 = {sa[a2], sb[a2], sc[a2], sd[a2]}, v3 = {sa[a3], sb[a3], sc[a3], sd[a3]};
+      bfly_q(v0, v2, t1);
+      bfly_q(v1, v3, t1);
+      bfly_q(v0, v1, t2a);
+      bfly_q(v2, v3, t2b);
+      sa[a0] = v0.a, sb[a0] = v0.b, sc[a0] = v0.c, sd[a0] = v0.d;
+      sa[a1] = v1.a, sb[a1] = v1.b, sc[a1] = v1.c, sd[a1] = v1.d;
+      sa[a2] = v2.a, sb[a2] = v2.b, sc[a2] = v2.c, sd[a2] = v2.d;
+      sa[a3] = v3.a, sb[a3] = v3.b, sc[a3] = v3.c, sd[a3] = v3.d;
     }
     __syncthreads();
   }
@@ -197,45 +192,149 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const FftJob* __restr
     const uint32_t p = g.c;
     for (uint32_t k = threadIdx.x; k < T / 2; k += THREADS) {
       const uint32_t L = ((k >> p) << (p + 1)) | (k & ((1u << p) - 1));
-      const uint32_t R = L | (1u << p);
       const uint32_t t = stw[(L >> g.c) >> 1];
-      if (narrow) {
-        uint32_t l = sa[L], r = sa[R];
-        bfly_m31(l, r, t);
-        sa[L] = l;
-        sa[R] = r;
-      } else {
-        qm31 l = {sa[L], sb[L], sc[L], sd[L]}, r = {sa[R], sb[R], sc[R], sd[R]};
-        bfly_q(l, r, t);
-        sa[L] = l.a, sb[L] = l.b, sc[L] = l.c, sd[L] = l.d;
-        sa[R] = r.a, sb[R] = r.b, sc[R] = r.c, sd[R] = r.d;
-      }
+      const uint32_t aL = fpad(L), aR = fpad(L | (1u << p));
+      qm31 l = {sa[aL], sb[aL], sc[aL], sd[aL]}, r = {sa[aR], sb[aR], sc[aR], sd[aR]};
+      bfly_q(l, r, t);
+      sa[aL] = l.a, sb[aL] = l.b, sc[aL] = l.c, sd[aL] = l.d;
+      sa[aR] = r.a, sb[aR] = r.b, sc[aR] = r.c, sd[aR] = r.d;
     }
     __syncthreads();
   }
-
   for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
-    const uint64_t gi = fft_global_index(g, w.y, L);
-    if (!narrow)
-      job.out[gi] = make_uint4(sa[L], sb[L], sc[L], sd[L]);
-    else if (last)
-      job.out[gi] = make_uint4(sa[L], 0u, 0u, 0u);
-    else
-      job.narrow[gi] = sa[L];
+    const uint32_t a = fpad(L);
+    job.out[fft_global_index(g, w.y, L)] = make_uint4(sa[a], sb[a], sc[a], sd[a]);
   }
 }
 
-// four limb arrays of 4096 values + 4095 staged twiddles
-static constexpr size_t kFftSmem = ((size_t)16 << kFftLowBits) + ((size_t)4 << kFftLowBits);
-static constexpr int kFftThreads = 512;
-
-cudaError_t prepare_fft_kernels() {
-  return cudaFuncSetAttribute(fft_pass_kernel<kFftThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmem);
+// One-limb tiles for inputs that are lifted M31 polynomials (b = c = d = 0 in
+// every coefficient, so in every intermediate value): the first pass reads the
+// a limbs of the nonzero prefix, passes exchange one word per element through
+// `narrow`, and the last pass writes the QM31 codeword (a, 0, 0, 0).  Three stages
+// per shared-memory round trip (radix 8 in registers).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  extern __shared__ uint32_t nsm[];
+  const uint2 w = work[blockIdx.x];
+  const FftJob& job = jobs[w.x];
+  const FftTile ft = fft_tile(job);
+  const FftPassGeom& g = ft.g;
+  const uint32_t T = ft.T;
+  uint32_t* sv = nsm;
+  uint32_t* stw = sv + T + (T >> 5);
+  fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
+  const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
+  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
+    const uint64_t gi = fft_global_index(g, w.y, L);
+    uint32_t v;
+    if (ft.first)
+      v = gi < ft.count ? __ldg(in_a + 4 * gi) : 0u;
+    else
+      v = job.narrow[gi];
+    sv[fpad(L)] = v;
+  }
+  __syncthreads();
+  int j = (int)g.m - 1;
+  for (; j >= 2; j -= 3) {
+    const uint32_t p = (uint32_t)j + g.c;  // stages j, j-1, j-2 pair bits p, p-1, p-2
+    const uint32_t* tw0 = stw + fft_stw_offset(g.m, (uint32_t)j);
+    const uint32_t* tw1 = stw + fft_stw_offset(g.m, (uint32_t)j - 1);
+    const uint32_t* tw2 = stw + fft_stw_offset(g.m, (uint32_t)j - 2);
+    const uint32_t lowmask = (1u << (p - 2)) - 1;
+    for (uint32_t k = threadIdx.x; k < T / 8; k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << 3) | (k & lowmask);
+      const uint32_t row = e0 >> g.c;
+      uint32_t a[8], v[8];
+#pragma unroll
+      for (uint32_t b = 0; b < 8; b++) {
+        a[b] = fpad(e0 | ((b >> 2) << p) | (((b >> 1) & 1u) << (p - 1)) | ((b & 1u) << (p - 2)));
+        v[b] = sv[a[b]];
+      }
+      const uint32_t t0 = tw0[row >> (j + 1)];
+      const uint32_t r1 = row >> j, r2 = row >> (j - 1);
+      const uint32_t t1a = tw1[r1], t1b = tw1[r1 | 1u];
+      const uint32_t t2a = tw2[r2], t2b = tw2[r2 | 1u], t2c = tw2[r2 | 2u], t2d = tw2[r2 | 3u];
+      bfly_m31(v[0], v[4], t0);
+      bfly_m31(v[1], v[5], t0);
+      bfly_m31(v[2], v[6], t0);
+      bfly_m31(v[3], v[7], t0);
+      bfly_m31(v[0], v[2], t1a);
+      bfly_m31(v[1], v[3], t1a);
+      bfly_m31(v[4], v[6], t1b);
+      bfly_m31(v[5], v[7], t1b);
+      bfly_m31(v[0], v[1], t2a);
+      bfly_m31(v[2], v[3], t2b);
+      bfly_m31(v[4], v[5], t2c);
+      bfly_m31(v[6], v[7], t2d);
+#pragma unroll
+      for (uint32_t b = 0; b < 8; b++) sv[a[b]] = v[b];
+    }
+    __syncthreads();
+  }
+  if (j == 1) {
+    const uint32_t p = 1u + g.c;
+    const uint32_t* tw0 = stw + fft_stw_offset(g.m, 1);
+    const uint32_t lowmask = (1u << (p - 1)) - 1;
+    for (uint32_t k = threadIdx.x; k < T / 4; k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << 2) | (k & lowmask);
+      const uint32_t row = e0 >> g.c;
+      const uint32_t t1 = tw0[row >> 2];
+      const uint32_t t2a = stw[row >> 1], t2b = stw[(row >> 1) | 1u];
+      const uint32_t a0 = fpad(e0), a1 = fpad(e0 | (1u << (p - 1))), a2 = fpad(e0 | (1u << p)), a3 = fpad(e0 | (3u << (p - 1)));
+      uint32_t v0 = sv[a0], v1 = sv[a1], v2 = sv[a2], v3 = sv[a3];
+      bfly_m31(v0, v2, t1);
+      bfly_m31(v1, v3, t1);
+      bfly_m31(v0, v1, t2a);
+      bfly_m31(v2, v3, t2b);
+      sv[a0] = v0;
+      sv[a1] = v1;
+      sv[a2] = v2;
+      sv[a3] = v3;
+    }
+    __syncthreads();
+  } else if (j == 0) {
+    const uint32_t p = g.c;
+    for (uint32_t k = threadIdx.x; k < T / 2; k += THREADS) {
+      const uint32_t L = ((k >> p) << (p + 1)) | (k & ((1u << p) - 1));
+      const uint32_t t = stw[(L >> g.c) >> 1];
+      const uint32_t aL = fpad(L), aR = fpad(L | (1u << p));
+      uint32_t l = sv[aL], r = sv[aR];
+      bfly_m31(l, r, t);
+      sv[aL] = l;
+      sv[aR] = r;
+    }
+    __syncthreads();
+  }
+  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
+    const uint64_t gi = fft_global_index(g, w.y, L);
+    const uint32_t v = sv[fpad(L)];
+    if (ft.last)
+      job.out[gi] = make_uint4(v, 0u, 0u, 0u);
+    else
+      job.narrow[gi] = v;
+  }
 }
 
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s) {
+// tiles of at most 4096 values (+ one pad word per 32) and 4095 staged twiddles
+static constexpr uint32_t kFftTileMax = 1u << kFftLowBits;
+static constexpr uint32_t kFftTilePadded = kFftTileMax + (kFftTileMax >> 5);
+static constexpr size_t kFftSmemQ = (size_t)4 * (4 * kFftTilePadded + kFftTileMax);
+static constexpr size_t kFftSmemM31 = (size_t)4 * (kFftTilePadded + kFftTileMax);
+static constexpr int kFftThreadsQ = 512;
+static constexpr int kFftThreadsM31 = 256;
+
+cudaError_t prepare_fft_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(fft_pass_q_kernel<kFftThreadsQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemQ);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fft_pass_m31_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemM31);
+}
+
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
-  fft_pass_kernel<kFftThreads><<<nwork, kFftThreads, kFftSmem, s>>>(d_jobs, d_work);
+  if (narrow)
+    fft_pass_m31_kernel<kFftThreadsM31><<<nwork, kFftThreadsM31, kFftSmemM31, s>>>(d_jobs, d_work);
+  else
+    fft_pass_q_kernel<kFftThreadsQ><<<nwork, kFftThreadsQ, kFftSmemQ, s>>>(d_jobs, d_work);
   return cudaGetLastError();
 }
 

@@ -16,6 +16,7 @@
 
 #include "azk_field.cuh"
 #include "azk_runtime.h"
+#include "azk_tuned.h"
 
 namespace azk {
 struct SumcheckOut {
@@ -55,6 +56,8 @@ struct Engine {
   std::vector<PcsInstance> h_inst;
   // FFT
   FftPlan fft;
+  std::vector<FftJob> fft_transforms;
+  std::vector<uint8_t> fft_narrow;  // per instance: input known to be a lifted M31 polynomial
   // rounds: tree step k (kind QM31 at k == 0, fold+hash after), final folds at step k
   std::vector<TreeJob> tree_jobs;
   std::vector<uint2> tree_work;
@@ -133,11 +136,32 @@ struct Engine {
     for (size_t i = 0; i < cfg.size(); i++) AZK_CU(launch_scan_input(arena.at<uint4>(off_input[i]), counts[i], d_flag(), d_info() + i, s));
     uint32_t f = 0;
     AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s));
+    sync_stream(s);
     layout(f == 0, "input contains a non-canonical field element");
+    std::vector<uint8_t> narrow(cfg.size());
+    for (size_t i = 0; i < cfg.size(); i++) narrow[i] = h[i].m31 ? 1 : 0;
+    set_fft_narrow(narrow);
   }
   // Inputs written by the caller through a device pointer: nothing known.
-  void forget_input(size_t i) { AZK_CU(cudaMemsetAsync(d_info() + i, 0, sizeof(InputInfo), s)); }
+  void forget_input(size_t i) {
+    AZK_CU(cudaMemsetAsync(d_info() + i, 0, sizeof(InputInfo), s));
+    std::vector<uint8_t> narrow = fft_narrow;
+    narrow[i] = 0;
+    set_fft_narrow(narrow);
+  }
+  // Which instances run the one-limb FFT kernel; a change rebuilds the FFT work
+  // lists and drops the captured graph (it is captured again on the next run).
+  void set_fft_narrow(const std::vector<uint8_t>& narrow) {
+    if (narrow == fft_narrow) return;
+    sync_stream(s);
+    fft_narrow = narrow;
+    fft.build(fft_transforms, fft_narrow);
+    fft.upload(s);
+    sync_stream(s);
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
 
   void init(azk_ctx* c, const std::vector<InstanceCfg>& cf, const Sched& sc) {
     ctx = c;
@@ -223,7 +247,9 @@ struct Engine {
     for (size_t i = 0; i < n; i++)
       tf.push_back(FftJob{cfg[i].logn, 0, arena.at<uint4>(off_input[i]), arena.at<uint4>(off_layers[i]), h_inst[i].tw,
                           arena.at<uint32_t>(off_trees[i]), d_info() + i});
-    fft.build(tf);
+    fft_transforms = tf;
+    fft_narrow.assign(n, 0);
+    fft.build(tf, fft_narrow);
     fft.upload(s);
 
     // ---- rounds ----
@@ -301,7 +327,7 @@ struct Engine {
     up(d_tree_work, tree_work.data(), tree_work.size() * sizeof(uint2), "PCS.TreeWork");
     up(d_fold_jobs, fold_jobs.data(), fold_jobs.size() * sizeof(FoldJob), "PCS.FoldJobs");
     up(d_fold_work, fold_work.data(), fold_work.size() * sizeof(uint2), "PCS.FoldWork");
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     // algorithmic work: leaf + parent permutations and 3 transcript absorbs per
     // committed layer; FFT single-pass bytes (16N in, 16N out, 4(N-1) twiddles);
     // final fold bytes (16 in + 8 out + 2 twiddle per input element)
@@ -391,7 +417,7 @@ struct Engine {
       AZK_CU(launch_pcs_grind(d_inst(), i, start, chunk, found.as<unsigned long long>(), s));
       uint64_t nonce = ~0ull;
       AZK_CU(cudaMemcpyAsync(&nonce, found.p, 8, cudaMemcpyDeviceToHost, s));
-      AZK_CU(cudaStreamSynchronize(s));
+      sync_stream(s);
       if (nonce != ~0ull) {
         h_inst[i].nonce = nonce;
         h_inst[i].has_nonce = 1;
@@ -449,7 +475,7 @@ struct Engine {
     AZK_CU(launch_check_canonical(static_cast<const uint32_t*>(dptr), words, d_flag(), s));
     uint32_t f = 0;
     AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     layout(f == 0, "input contains a non-canonical field element");
   }
 
@@ -460,7 +486,7 @@ struct Engine {
     if (fl)
       AZK_CU(cudaMemcpyAsync(fl, h_inst[i].layers + layer_offset(c2.logn, c2.rounds), 16ull << (c2.logn - c2.rounds), cudaMemcpyDeviceToHost, s));
     if (qp) AZK_CU(cudaMemcpyAsync(qp, arena.at<uint8_t>(off_qp[i]), 4ull * c2.queries, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
   }
 };
 
@@ -507,7 +533,7 @@ azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t logn, uint32_t log_blowu
     p->queries = queries;
     p->log_blowup = log_blowup;
     p->grinding = grinding;
-    Sched sc = resolve_schedule(schedule);
+    Sched sc = resolve_schedule(schedule, kTuned_pcs_single);
     sc.graph = false;
     p->eng.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
     *out = p.release();
@@ -538,7 +564,7 @@ static void pcs_prove_common(azk_pcs_prover* p, bool coeffs, const uint8_t pub[3
     AZK_CU(cudaMemcpyAsync(proof_out, e.h_inst[0].proof, len, cudaMemcpyDeviceToDevice, e.s));
   else
     AZK_CU(cudaMemcpyAsync(proof_out, e.h_inst[0].proof, len, cudaMemcpyDeviceToHost, e.s));
-  AZK_CU(cudaStreamSynchronize(e.s));
+  sync_stream(e.s);
   fill_stats(st, t, sub, gs);
 }
 
@@ -617,7 +643,7 @@ azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint3
     uint64_t N = 1ull << logn;
     Timer t;
     Engine e;
-    Sched sc;
+    Sched sc = resolve_schedule(nullptr, kTuned_pcs_single);
     sc.graph = false;
     e.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
     AZK_CU(cudaMemcpyAsync(e.h_inst[0].layers, ev, 16 * N, cudaMemcpyHostToDevice, e.s));
@@ -648,7 +674,7 @@ azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* logs, 
     }
     auto b = std::make_unique<azk_batch>();
     b->ctx = ctx;
-    b->eng.init(ctx, cf, resolve_schedule(schedule));
+    b->eng.init(ctx, cf, resolve_schedule(schedule, kTuned_pcs_batch));
     *out = b.release();
   });
 }
@@ -660,7 +686,7 @@ azk_status azk_batch_input(azk_batch* b, uint32_t i, void** dev) {
     // the caller writes this input directly: what the last upload learned about it
     // no longer holds (the FFT reads all N coefficients with QM31 arithmetic)
     b->eng.forget_input(i);
-    AZK_CU(cudaStreamSynchronize(b->eng.s));
+    sync_stream(b->eng.s);
     *dev = b->eng.arena.at<void>(b->eng.off_input[i]);
   });
 }
@@ -691,7 +717,7 @@ azk_status azk_batch_prove(azk_batch* b, const uint8_t* pubs, int plain, azk_sta
     e.set_publics(pubs);
     uint64_t sub = 0;
     double gs = e.run(true, plain != 0, &sub, t);
-    AZK_CU(cudaStreamSynchronize(e.s));
+    sync_stream(e.s);
     fill_stats(st, t, sub, gs);
   });
 }
@@ -719,7 +745,7 @@ azk_status azk_batch_download_proofs(azk_batch* b, uint8_t* out, uint64_t cap) {
       AZK_CU(cudaMemcpyAsync(out + pos, e.h_inst[i].proof, e.proof_len[i], cudaMemcpyDeviceToHost, e.s));
       pos += e.proof_len[i];
     }
-    AZK_CU(cudaStreamSynchronize(e.s));
+    sync_stream(e.s);
   });
 }
 
@@ -743,7 +769,7 @@ azk_status azk_batch_profile(azk_batch* b, double* seconds4) {
   return guarded(b ? b->ctx : nullptr, [&] {
     layout(b && seconds4);
     std::lock_guard<std::mutex> lk(b->mu);
-    AZK_CU(cudaStreamSynchronize(b->eng.s));
+    sync_stream(b->eng.s);
     b->eng.profile(seconds4);
   });
 }
@@ -844,7 +870,29 @@ struct azk_server {
 
 namespace {
 
-void run_pcs(azk_server* sv, Resident& r, ServeJob& j) {
+// Page-locked host staging of one worker: job inputs and results cross PCIe from
+// here (copies from pageable memory go through the driver's own staging, which
+// serialises the workers' copies).
+struct Staging {
+  uint8_t* p = nullptr;
+  size_t n = 0;
+  uint8_t* ensure(size_t bytes) {
+    if (bytes > n) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      n = 0;
+      size_t want = std::max<size_t>(bytes, 1 << 20);
+      AZK_CU(cudaHostAlloc(reinterpret_cast<void**>(&p), want, cudaHostAllocDefault));
+      n = want;
+    }
+    return p;
+  }
+  ~Staging() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st) {
   if (!r.eng) {
     r.eng = std::make_unique<Engine>();
     Sched sc = sv->sched;
@@ -853,22 +901,28 @@ void run_pcs(azk_server* sv, Resident& r, ServeJob& j) {
   }
   Engine* e = r.eng.get();
   uint64_t N = 1ull << j.logn;
+  const uint64_t in_bytes = 16 * j.count, proof = e->proof_len[0];
+  uint8_t* pin = st.ensure(std::max<uint64_t>(in_bytes, proof) + 64);
+  std::memcpy(pin, j.input.data(), in_bytes);
   uint4* in = e->arena.at<uint4>(e->off_input[0]);
-  AZK_CU(cudaMemcpyAsync(in, j.input.data(), 16 * j.count, cudaMemcpyHostToDevice, e->s));
+  AZK_CU(cudaMemcpyAsync(in, pin, in_bytes, cudaMemcpyHostToDevice, e->s));
   if (j.count < N) AZK_CU(cudaMemsetAsync(in + j.count, 0, 16 * (N - j.count), e->s));
   e->scan_inputs({j.count});
   e->set_publics(j.pub);
   Timer t;
   e->run(true, true, nullptr, t);
-  j.result.resize(e->proof_len[0]);
-  AZK_CU(cudaMemcpyAsync(j.result.data(), e->h_inst[0].proof, e->proof_len[0], cudaMemcpyDeviceToHost, e->s));
-  AZK_CU(cudaStreamSynchronize(e->s));
+  AZK_CU(cudaMemcpyAsync(pin, e->h_inst[0].proof, proof, cudaMemcpyDeviceToHost, e->s));
+  sync_stream(e->s);
+  j.result.assign(pin, pin + proof);
 }
 
 // Sum-check of one table through reusable device buffers: evaluations upload,
 // one single-CTA kernel, results download.  Output words: claimed sum, final
 // evaluation, digest (8 words), sums at 0, sums at 1, challenges (rounds each).
-std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s) {
+// `evals` and `pin` (>= 4n + sizeof(SumcheckOut) + 12 log n bytes) may be the same
+// page-locked buffer: the evaluations are consumed by the upload before the
+// results land.
+std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s, uint8_t* pin) {
   const uint64_t n = 1ull << logn;
   if (!b.ev.p) {
     b.ev.alloc(4 * n, "Sumcheck.Evals");
@@ -877,17 +931,20 @@ std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint3
     b.out.alloc(sizeof(SumcheckOut), "Sumcheck.Out");
   }
   AZK_CU(cudaMemcpyAsync(b.ev.p, evals, 4 * n, cudaMemcpyHostToDevice, s));
-  SumcheckOut h{};
-  h.r0 = b.rounds.as<uint32_t>();
-  h.r1 = h.r0 + logn;
-  h.challenges = h.r1 + logn;
-  AZK_CU(cudaMemcpyAsync(b.out.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  SumcheckOut* h = reinterpret_cast<SumcheckOut*>(pin + align_up(4 * n, 64));
+  uint32_t* rounds_h = reinterpret_cast<uint32_t*>(h + 1);
+  SumcheckOut ptrs{};
+  ptrs.r0 = b.rounds.as<uint32_t>();
+  ptrs.r1 = ptrs.r0 + logn;
+  ptrs.challenges = ptrs.r1 + logn;
+  *h = ptrs;
+  AZK_CU(cudaMemcpyAsync(b.out.p, h, sizeof(SumcheckOut), cudaMemcpyHostToDevice, s));
   AZK_CU(launch_sumcheck(b.ev.as<uint32_t>(), logn, b.scratch.as<uint32_t>(), b.out.as<SumcheckOut>(), s));
-  SumcheckOut r{};
-  std::vector<uint32_t> rounds(3 * logn);
-  AZK_CU(cudaMemcpyAsync(&r, b.out.p, sizeof(r), cudaMemcpyDeviceToHost, s));
-  AZK_CU(cudaMemcpyAsync(rounds.data(), b.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, s));
-  AZK_CU(cudaStreamSynchronize(s));
+  AZK_CU(cudaMemcpyAsync(h, b.out.p, sizeof(SumcheckOut), cudaMemcpyDeviceToHost, s));
+  AZK_CU(cudaMemcpyAsync(rounds_h, b.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, s));
+  sync_stream(s);
+  const SumcheckOut r = *h;
+  std::vector<uint32_t> rounds(rounds_h, rounds_h + 3 * logn);
   std::vector<uint32_t> words = {r.claimed_sum, r.final_eval};
   for (int i = 0; i < 4; i++) {
     words.push_back((uint32_t)r.digest[i]);
@@ -897,9 +954,13 @@ std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint3
   return words;
 }
 
-void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j) {
+uint64_t sumcheck_pinned_bytes(uint32_t logn) { return align_up(4ull << logn, 64) + sizeof(SumcheckOut) + 12ull * logn + 64; }
+
+void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j, Staging& st) {
   if (!res.sc) res.sc = std::make_unique<SumcheckBufs>();
-  std::vector<uint32_t> words = sumcheck_run(*res.sc, j.input.data(), j.logn, s);
+  uint8_t* pin = st.ensure(sumcheck_pinned_bytes(j.logn));
+  std::memcpy(pin, j.input.data(), 4ull << j.logn);
+  std::vector<uint32_t> words = sumcheck_run(*res.sc, reinterpret_cast<const uint32_t*>(pin), j.logn, s, pin);
   j.result.resize(4 * words.size());
   std::memcpy(j.result.data(), words.data(), j.result.size());
 }
@@ -937,8 +998,13 @@ std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
 
 void worker_loop(azk_server* sv, int w) {
   cudaSetDevice(sv->ctx->device);
+  // sum-check jobs are one long chain of dependent permutations: their stream gets
+  // the device's highest priority, so their blocks are placed first
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   cudaStream_t s = nullptr;
-  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio_hi);
+  Staging staging;
   for (;;) {
     std::shared_ptr<ServeJob> job;
     Resident* res = nullptr;
@@ -955,9 +1021,9 @@ void worker_loop(azk_server* sv, int w) {
     }
     try {
       if (job->kind == 0)
-        run_pcs(sv, *res, *job);
+        run_pcs(sv, *res, *job, staging);
       else
-        run_sumcheck(*res, s, *job);
+        run_sumcheck(*res, s, *job, staging);
       job->state = 2;
     } catch (const Error& e) {
       job->error = e.msg;
@@ -1025,7 +1091,10 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evals, uint64_t coun
     Timer t;
     uint32_t logn = ilog2(count);
     SumcheckBufs b;
-    std::vector<uint32_t> w = sumcheck_run(b, evals, logn, ctx->stream);
+    Staging staging;
+    uint8_t* pin = staging.ensure(sumcheck_pinned_bytes(logn));
+    std::memcpy(pin, evals, 4ull << logn);
+    std::vector<uint32_t> w = sumcheck_run(b, reinterpret_cast<const uint32_t*>(pin), logn, ctx->stream, pin);
     *claimed_sum = w[0];
     *final_eval = w[1];
     std::memcpy(digest, w.data() + 2, 32);
@@ -1041,7 +1110,9 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     layout(ctx && out && slots >= 1 && slots <= 64 && hbm_budget_bytes > 0);
     auto sv = std::make_unique<azk_server>();
     sv->ctx = ctx;
-    sv->sched = resolve_schedule(schedule);
+    // many jobs share the device at once, so the throughput table (many trees per
+    // launch) fits better than the single-tree latency table
+    sv->sched = resolve_schedule(schedule, kTuned_pcs_batch);
     sv->budget = hbm_budget_bytes;
     sv->slots = slots;
     sv->cache.resize(slots);

@@ -6,6 +6,7 @@
 
 #include "azk_field.cuh"
 #include "azk_runtime.h"
+#include "azk_tuned.h"
 
 using namespace azk;
 
@@ -30,12 +31,13 @@ const azk_ctx::Domain& azk::domain_tables(azk_ctx* ctx, uint32_t logn) {
   AZK_CU(cudaMalloc(&d.tw, 4 * (n - 1 + 1)));
   AZK_CU(cudaMalloc(&d.inv, 4 * (n - 1 + 1)));
   AZK_CU(launch_domain_tables(logn, d.tw, d.inv, ctx->stream));
-  AZK_CU(cudaStreamSynchronize(ctx->stream));
+  sync_stream(ctx->stream);
   return ctx->domains.emplace(logn, d).first->second;
 }
 
-Sched azk::resolve_schedule(const azk_schedule* s) {
+Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults) {
   Sched r;
+  bool any_layer = false;
   if (s) {
     if (s->treelet_log) r.tile_log = s->treelet_log;
     if (s->group_log) r.group_log = s->group_log;
@@ -43,9 +45,12 @@ Sched azk::resolve_schedule(const azk_schedule* s) {
     r.graph = s->use_graph != 0;
     for (int i = 0; i < 32; i++) {
       r.layer_tile[i] = s->layer_treelet[i];
+      any_layer |= r.layer_tile[i] != 0;
       require(r.layer_tile[i] <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "layer treelet depth must be in 0...13");
     }
   }
+  if (defaults && !any_layer && !(s && s->treelet_log))
+    for (int i = 0; i < 32; i++) r.layer_tile[i] = defaults[i] <= 13 ? defaults[i] : 13;
   require(r.tile_log >= 1 && r.tile_log <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 1...13");
   if (r.group_log > r.tile_log) r.group_log = r.tile_log;
   require(r.group_log >= 1, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "group_log must be >= 1");
@@ -56,13 +61,17 @@ Sched azk::resolve_schedule(const azk_schedule* s) {
 // ---------------------------------------------------------------------------
 // FFT plans
 // ---------------------------------------------------------------------------
-void FftPlan::build(const std::vector<FftJob>& transforms) {
+void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uint8_t>& narrow_flags) {
   jobs.clear();
   work.clear();
+  narrow.assign(transforms.size(), 0);
+  for (size_t i = 0; i < transforms.size() && i < narrow_flags.size(); i++) narrow[i] = narrow_flags[i] ? 1 : 0;
   uint32_t max_passes = 0;
   for (auto& t : transforms) max_passes = std::max(max_passes, fft_high_chunks(t.logn) + 1);
   step_off.assign(max_passes, 0);
   step_cnt.assign(max_passes, 0);
+  nstep_off.assign(max_passes, 0);
+  nstep_cnt.assign(max_passes, 0);
   inst_range.assign(max_passes, std::vector<std::pair<uint64_t, uint64_t>>(transforms.size(), {0, 0}));
   std::vector<std::vector<uint32_t>> job_at(max_passes, std::vector<uint32_t>(transforms.size(), UINT32_MAX));
   for (size_t i = 0; i < transforms.size(); i++) {
@@ -75,15 +84,17 @@ void FftPlan::build(const std::vector<FftJob>& transforms) {
     }
   }
   for (uint32_t step = 0; step < max_passes; step++) {
-    step_off[step] = work.size();
-    for (size_t i = 0; i < transforms.size(); i++) {
-      uint32_t jid = job_at[step][i];
-      if (jid == UINT32_MAX) continue;
-      uint64_t tiles = fft_pass_tiles(jobs[jid].logn, jobs[jid].pass);
-      inst_range[step][i] = {work.size(), tiles};
-      for (uint64_t t = 0; t < tiles; t++) work.push_back(make_uint2(jid, (uint32_t)t));
+    for (int part = 0; part < 2; part++) {
+      (part ? nstep_off : step_off)[step] = work.size();
+      for (size_t i = 0; i < transforms.size(); i++) {
+        uint32_t jid = job_at[step][i];
+        if (jid == UINT32_MAX || narrow[i] != part) continue;
+        uint64_t tiles = fft_pass_tiles(jobs[jid].logn, jobs[jid].pass);
+        inst_range[step][i] = {work.size(), tiles};
+        for (uint64_t t = 0; t < tiles; t++) work.push_back(make_uint2(jid, (uint32_t)t));
+      }
+      (part ? nstep_cnt : step_cnt)[step] = work.size() - (part ? nstep_off : step_off)[step];
     }
-    step_cnt[step] = work.size() - step_off[step];
   }
 }
 void FftPlan::upload(cudaStream_t s) {
@@ -93,11 +104,12 @@ void FftPlan::upload(cudaStream_t s) {
   if (!work.empty()) AZK_CU(cudaMemcpyAsync(d_work.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
 }
 void FftPlan::launch_step(size_t step, cudaStream_t s) const {
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + step_off[step], (uint32_t)step_cnt[step], s));
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + step_off[step], (uint32_t)step_cnt[step], false, s));
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + nstep_off[step], (uint32_t)nstep_cnt[step], true, s));
 }
 void FftPlan::launch_step_for(size_t step, size_t t, cudaStream_t s) const {
   auto r = inst_range[step][t];
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, s));
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, narrow[t] != 0, s));
 }
 
 // ---------------------------------------------------------------------------
@@ -381,7 +393,7 @@ azk_status azk_keccakf_plan_permute(azk_keccakf_plan* p, const void* host_states
     AZK_CU(cudaMemcpyAsync(p->in.p, host_states, p->count * p->in_stride, cudaMemcpyHostToDevice, p->s));
     keccakf_run(p, p->in.as<uint8_t>(), p->out.as<uint8_t>(), nullptr, t);
     AZK_CU(cudaMemcpyAsync(host_out, p->out.p, p->count * p->out_stride, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     if (st) { st->cpu_wall_s = t.seconds(); st->gpu_s = 0; st->cpu_submit_ns = 0; }
   });
 }
@@ -401,7 +413,7 @@ azk_status azk_keccakf_plan_clear(azk_keccakf_plan* p) {
     std::lock_guard<std::mutex> lk(p->mu);
     AZK_CU(cudaMemsetAsync(p->in.p, 0, p->in.bytes, p->s));
     AZK_CU(cudaMemsetAsync(p->out.p, 0, p->out.bytes, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 void azk_keccakf_plan_destroy(azk_keccakf_plan* p) { delete p; }
@@ -444,7 +456,7 @@ azk_status azk_hash_plan_hash(azk_hash_plan* p, const void* msgs, void* digests,
                              p->threads, p->s));
     uint64_t sub = t.ns();
     AZK_CU(cudaMemcpyAsync(digests, p->out.p, p->count * p->out_stride, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     fill_stats(st, t, sub, 0);
   });
 }
@@ -469,7 +481,7 @@ azk_status azk_hash_plan_clear(azk_hash_plan* p) {
     std::lock_guard<std::mutex> lk(p->mu);
     AZK_CU(cudaMemsetAsync(p->in.p, 0, p->in.bytes, p->s));
     AZK_CU(cudaMemsetAsync(p->out.p, 0, p->out.bytes, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 void azk_hash_plan_destroy(azk_hash_plan* p) { delete p; }
@@ -491,7 +503,8 @@ azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t count, uint64_t stride,
     p->stride = stride;
     p->length = length;
     p->logn = ilog2(count);
-    uint32_t tl = treelet_log ? treelet_log : 12;
+    // default depth: the tuned table for one raw-leaf tree of this size
+    uint32_t tl = treelet_log ? treelet_log : (p->logn < 32 && kTuned_merkle_raw64[p->logn] ? kTuned_merkle_raw64[p->logn] : 12);
     if (tl > p->logn) tl = p->logn;
     if (tl == 0 && p->logn > 0) tl = 1;
     p->tile_log = tl;
@@ -522,7 +535,7 @@ azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t count, uint64_t stride,
     j.counters = p->counters.as<uint32_t>();
     j.root_out = p->root.as<uint64_t>();
     j.root_action = kRootNone;
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     *out = p.release();
   });
 }
@@ -536,7 +549,7 @@ static void merkle_commit_dev(azk_merkle_plan* p, const uint8_t* dleaves, uint8_
   uint64_t sub = t.ns();
   g.stop();
   AZK_CU(cudaMemcpyAsync(root_out, p->root.p, 32, cudaMemcpyDeviceToHost, p->s));
-  AZK_CU(cudaStreamSynchronize(p->s));
+  sync_stream(p->s);
   p->committed = true;
   fill_stats(st, t, sub, g.seconds());
 }
@@ -567,7 +580,7 @@ static void merkle_gather(azk_merkle_plan* p, const uint64_t* idx, uint64_t n, u
   AZK_CU(cudaMemcpyAsync(p->idx.p, idx, n * 8, cudaMemcpyHostToDevice, p->s));
   AZK_CU(launch_gather_openings(p->job.as<TreeJob>(), p->idx.as<uint64_t>(), (uint32_t)n, p->paths.as<uint64_t>(), p->s));
   AZK_CU(cudaMemcpyAsync(out, p->paths.p, n * p->logn * 32, cudaMemcpyDeviceToHost, p->s));
-  AZK_CU(cudaStreamSynchronize(p->s));
+  sync_stream(p->s);
 }
 
 azk_status azk_merkle_plan_open(azk_merkle_plan* p, const void* leaves, uint64_t index, uint8_t* leaf_out, uint8_t* sib_out, uint8_t root[32],
@@ -611,7 +624,7 @@ azk_status azk_merkle_plan_clear(azk_merkle_plan* p) {
     std::lock_guard<std::mutex> lk(p->mu);
     for (DevBuf* b : {&p->leaves, &p->leaf_digests, &p->inner, &p->root})
       AZK_CU(cudaMemsetAsync(b->p, 0, b->bytes, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     p->committed = false;
   });
 }
@@ -654,7 +667,7 @@ azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* digests, uint64
     AZK_CU(launch_tree_jobs(jb.as<TreeJob>(), dw.as<uint2>(), (uint32_t)tiles, tl, kLeafDigest, 256, s));
     g.stop();
     AZK_CU(cudaMemcpyAsync(root, r.p, 32, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -668,7 +681,7 @@ azk_status azk_circle_domain_points(azk_ctx* ctx, uint32_t logn, uint32_t* xy) {
     DevBuf d(8 * n, "CircleDomain.Points");
     AZK_CU(launch_domain_points(logn, d.as<uint32_t>(), ctx->stream));
     AZK_CU(cudaMemcpyAsync(xy, d.p, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
-    AZK_CU(cudaStreamSynchronize(ctx->stream));
+    sync_stream(ctx->stream);
   });
 }
 
@@ -708,7 +721,7 @@ azk_status azk_codeword_plan_create(azk_ctx* ctx, uint32_t logn, azk_codeword_pl
     FftJob j{logn, 0, p->coeff.as<uint4>(), p->out.as<uint4>(), d.tw};
     p->fft.build({j});
     p->fft.upload(p->s);
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     *out = p.release();
   });
 }
@@ -746,7 +759,7 @@ azk_status azk_codeword_plan_execute(azk_codeword_plan* p, const uint32_t* coeff
     if (count < n) AZK_CU(cudaMemsetAsync(p->coeff.as<uint4>() + count, 0, 16 * (n - count), p->s));
     codeword_run(p, p->coeff.as<uint4>(), p->out.as<uint4>(), nullptr, t);
     AZK_CU(cudaMemcpyAsync(codeword, p->out.p, 16 * n, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     fill_stats(st, t, 0, 0);
   });
 }
@@ -768,7 +781,7 @@ azk_status azk_codeword_plan_execute_resident(azk_codeword_plan* p, const void* 
     Timer t;
     codeword_run(p, reinterpret_cast<const uint4*>(static_cast<const uint8_t*>(din) + in_off),
                  reinterpret_cast<uint4*>(static_cast<uint8_t*>(dout) + out_off), st, t);
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 void azk_codeword_plan_destroy(azk_codeword_plan* p) { delete p; }
@@ -798,7 +811,7 @@ azk_status azk_qm31_fold(azk_ctx* ctx, const uint32_t* ev, uint64_t n, const uin
     AZK_CU(launch_fold_qm31_inv(de.as<uint4>(), di.as<uint4>(), dc.as<uint32_t>(), dout.as<uint4>(), n / 2, s));
     g.stop();
     AZK_CU(cudaMemcpyAsync(out, dout.p, 8 * n, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -838,7 +851,7 @@ azk_status azk_circle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint32_t* ev
       AZK_CU(launch_fold_jobs(djobs.as<FoldJob>(), dwork.as<uint2>() + ranges[r].first, (uint32_t)ranges[r].second, s));
     g.stop();
     AZK_CU(cudaMemcpyAsync(out, layers.as<uint4>() + layer_offset(logn, rounds), 16 * (n >> rounds), cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -906,7 +919,7 @@ azk_status azk_qm31_merkle_fold_chain(azk_ctx* ctx, const uint32_t* ev, uint64_t
     AZK_CU(cudaMemcpyAsync(final_out, layers.as<uint4>() + layer_offset(logn, rounds), 16 * (n >> rounds), cudaMemcpyDeviceToHost, s));
     if (commitments_out) AZK_CU(cudaMemcpyAsync(commitments_out, dcm.p, 32ull * rounds, cudaMemcpyDeviceToHost, s));
     if (ch_out) AZK_CU(cudaMemcpyAsync(ch_out, dch.p, 16ull * rounds, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -927,7 +940,7 @@ azk_status azk_qm31_transcript_challenges(azk_ctx* ctx, uint64_t input_count, co
     AZK_CU(launch_qm31_transcript_prefix(tr.as<Transcript>(), input_count, rounds, s));
     AZK_CU(launch_transcript_rounds_given(tr.as<Transcript>(), kRootQM31Round, roots.as<uint64_t>(), rounds, input_count, dch.as<uint32_t>(), s));
     AZK_CU(cudaMemcpyAsync(ch_out, dch.p, 16ull * rounds, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
   });
 }
 
@@ -939,7 +952,7 @@ azk_status azk_probe_int_issue(azk_ctx* ctx, double* ops_per_second) {
     DevBuf sink(16, "Probe.Sink");
     double ops = 0;
     AZK_CU(launch_int_issue_probe(ctx->sm_count, s, sink.as<uint32_t>(), &ops, nullptr));  // warm-up
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
     double best = 0;
     for (int rep = 0; rep < 5; rep++) {
       GpuTimer g(s);
@@ -961,7 +974,7 @@ azk_status azk_check_canonical(azk_ctx* ctx, const void* dwords, uint64_t nwords
     AZK_CU(cudaMemsetAsync(f.p, 0, 4, s));
     AZK_CU(launch_check_canonical(static_cast<const uint32_t*>(dwords), nwords, f.as<uint32_t>(), s));
     AZK_CU(cudaMemcpyAsync(flag_out, f.p, 4, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaStreamSynchronize(s));
+    sync_stream(s);
   });
 }
 

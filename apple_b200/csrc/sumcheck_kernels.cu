@@ -178,7 +178,9 @@ __global__ void __launch_bounds__(32) sumcheck_digest_kernel(const uint32_t* __r
   if (threadIdx.x < 4) out->digest[threadIdx.x] = d;
 }
 
-__global__ void __launch_bounds__(1024) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
+// 512 threads at <= 64 registers: half an SM's register file, so a rounds kernel
+// finds room beside the other jobs' kernels instead of waiting for an empty SM.
+__global__ void __launch_bounds__(512, 2) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
                                                         SumcheckOut* __restrict__ out) {
   __shared__ uint32_t red[32];
   __shared__ uint32_t s_ch;
@@ -241,7 +243,7 @@ __global__ void __launch_bounds__(1024) sumcheck_kernel(const uint32_t* __restri
 
 cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s) {
   sumcheck_digest_kernel<<<1, 32, 0, s>>>(evals, log_n, out);
-  sumcheck_kernel<<<1, 1024, 0, s>>>(evals, log_n, scratch, out);
+  sumcheck_kernel<<<1, 512, 0, s>>>(evals, log_n, scratch, out);
   return cudaGetLastError();
 }
 

@@ -291,7 +291,7 @@ azk_status azk_mlp_create(azk_ctx* ctx, uint32_t n_layers, const uint32_t* dims,
     AZK_CU(cudaMemcpyAsync(p->params.p, h.data(), 4 * p->nparams, cudaMemcpyHostToDevice, p->s));
     AZK_CU(cudaMemsetAsync(p->m.p, 0, 4 * p->nparams, p->s));
     AZK_CU(cudaMemsetAsync(p->v.p, 0, 4 * p->nparams, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
     *out = p.release();
   });
 }
@@ -303,7 +303,7 @@ azk_status azk_mlp_get_params(azk_mlp* p, float* out, uint64_t count) {
     layout(p && out && count == p->nparams);
     std::lock_guard<std::mutex> lk(p->mu);
     AZK_CU(cudaMemcpyAsync(out, p->params.p, 4 * count, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 
@@ -315,7 +315,7 @@ azk_status azk_mlp_set_params(azk_mlp* p, const float* in, uint64_t count) {
     AZK_CU(cudaMemsetAsync(p->m.p, 0, 4 * count, p->s));
     AZK_CU(cudaMemsetAsync(p->v.p, 0, 4 * count, p->s));
     p->step = 0;
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 
@@ -327,7 +327,7 @@ azk_status azk_mlp_forward(azk_mlp* p, const float* x, uint64_t rows, float* y) 
     mlp_prepare(p, w, x, nullptr, (uint32_t)rows);
     mlp_forward(p, w, (uint32_t)rows);
     AZK_CU(cudaMemcpyAsync(y, w.acts.back().p, 4 * rows, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 
@@ -341,7 +341,7 @@ azk_status azk_mlp_gradients(azk_mlp* p, const float* x, const float* y, uint64_
     mlp_backward(p, w, (uint32_t)rows);
     if (loss) AZK_CU(cudaMemcpyAsync(loss, w.loss.p, 4, cudaMemcpyDeviceToHost, p->s));
     if (grads) AZK_CU(cudaMemcpyAsync(grads, p->grads.p, 4 * p->nparams, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 
@@ -364,7 +364,7 @@ azk_status azk_mlp_train(azk_mlp* p, const float* x, const float* y, uint64_t ro
     mlp_forward(p, w, (uint32_t)rows);
     mlp_backward(p, w, (uint32_t)rows);
     if (final_loss) AZK_CU(cudaMemcpyAsync(final_loss, w.loss.p, 4, cudaMemcpyDeviceToHost, p->s));
-    AZK_CU(cudaStreamSynchronize(p->s));
+    sync_stream(p->s);
   });
 }
 

@@ -92,13 +92,68 @@ def run(which, log_count, reps=5):
         perms = sum(2 * ((1 << lg) >> k) - 1 + 3 for k in range(16))
         emit({"what": "circle pcs prove log 22 (FFT + 16 rounds + 64 queries + proof bytes), single instance", "seconds": t,
               "elems_per_s": (1 << lg) / t, "perms_per_s": perms / t, "wall_s": prover.last_stats.cpu_wall_s})
+    if "fold" in which:
+        # QM31 fold of 2^log values with QM31 inverse points: 16n read + 8n inverse
+        # read + 8n write bytes (n inputs), one launch
+        import ctypes
+
+        ev = np.zeros((n, 4), np.uint32)
+        ev[:] = rng.integers(0, 2**31 - 1, size=ev.shape, dtype=np.uint32)
+        inv = rng.integers(1, 2**31 - 1, size=(n // 2, 4), dtype=np.uint32)
+        ch = np.array([[11, 13, 17, 19]], np.uint32)
+        res = np.empty((n // 2, 4), np.uint32)
+        ts = []
+        for _ in range(reps + 1):
+            st = azk.Stats()
+            azk._capi.check(azk.lib().azk_qm31_fold(ctx.handle, ev.ctypes.data, n, inv.ctypes.data, ch.ctypes.data, res.ctypes.data, ctypes.byref(st)),
+                            ctx.handle)
+            ts.append(st.gpu_s)
+        t = statistics.median(ts[1:])
+        hbm, kind = _hbm_peak()
+        emit({"what": "qm31 fold (QM31 inverse points)", "count": n, "seconds": t, "hbm_gbs": 32 * n / t / 1e9, "frac_hbm": 32 * n / t / 1e9 / hbm,
+              "peak_source": kind})
+    if "fft" in which:
+        # Circle FFT stage of a batch of 16 log-22 instances (blowup 4): lifted M31
+        # coefficients (one-limb path) and full QM31 coefficients
+        lg, cnt = 22, 16
+        rows = (1 << lg) >> 2
+        for label, limbs in (("lifted M31", 1), ("QM31", 4)):
+            flat = np.zeros((rows * cnt, 4), np.uint32)
+            flat[:, :limbs] = rng.integers(0, 2**31 - 1, size=(rows * cnt, limbs), dtype=np.uint32)
+            b = azk.BatchProver(ctx, [lg] * cnt, [lg - 6] * cnt, 2, 64)
+            b.upload(flat, [rows * i for i in range(cnt)], [rows] * cnt)
+            pubs = bytes(32 * cnt)
+            b.prove(pubs)
+            b.set_profiling(True)
+            fs = []
+            for _ in range(reps):
+                b.prove(pubs)
+                fs.append(b.profile()["fft_s"])
+            t = statistics.median(fs)
+            N = (1 << lg) * cnt
+            alg = 16 * N + 16 * N + 4 * N
+            hbm, kind = _hbm_peak()
+            emit({"what": f"circle fft 16 x log 22, {label} coefficients", "seconds": t, "elems_per_s": N / t, "hbm_gbs": alg / t / 1e9,
+                  "frac_hbm": alg / t / 1e9 / hbm, "algorithmic": "16N read + 16N write + 4N twiddles", "peak_source": kind})
+            del b
     ctx.close()
     return out
 
 
+def _hbm_peak():
+    import json
+    import os
+
+    try:
+        with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--which", default="perm,sha3,merkle,prove")
+    ap.add_argument("--which", default="perm,sha3,merkle,prove,fold,fft")
     ap.add_argument("--log", type=int, default=24)
     ap.add_argument("--reps", type=int, default=5)
     a = ap.parse_args()

@@ -135,6 +135,15 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def tuned_tables():
+    """The tuned per-layer treelet tables the library was built with (apple_b200/tuned_b200.json)."""
+    try:
+        with open(os.path.join(ROOT, "apple_b200", "tuned_b200.json")) as f:
+            return {k: {int(lg): int(t) for lg, t in v.items()} for k, v in json.load(f)["tables"].items()}
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -254,11 +263,12 @@ def serving_mix(n_jobs, seed, lo=12, hi=22, sumcheck_every=5):
     return jobs
 
 
-def run_serving(azk, ctx, args):
-    """Continuous-batching server on the serving mix: a saturated backlog gives the
+def run_serving(azk, ctx, args, batched_jobs_per_s):
+    """Continuous-batching server on the serving mix.  A saturated backlog gives the
     server's throughput on this mix; Poisson arrivals at `--serve-load` of it give
-    p50/p99 latency (completion - arrival).  Every job's bytes are those of the
-    same job alone (tests/test_gpu_server.py)."""
+    p50/p99 latency (completion - arrival).  The batched superstep's jobs/s (the
+    512-instance leg, larger jobs on average) is reported beside it.  Every job's
+    bytes are those of the same job alone (tests/test_gpu_server.py)."""
     final_log, queries, blowup = args.final_log, 64, 2
     rng_rows = {k: None for k in range(12, 23)}
     for k in rng_rows:
@@ -302,8 +312,8 @@ def run_serving(azk, ctx, args):
     sat_jobs_s = len(mix) / t_sat
     sat_elems_s = sat_elems / t_sat
 
-    # Poisson arrivals at a fraction of that rate
-    lam = args.serve_load * sat_jobs_s
+    # Poisson arrivals
+    lam = args.serve_rate if args.serve_rate > 0 else args.serve_load * sat_jobs_s
     n = max(50, int(lam * args.serve_seconds))
     mix = serving_mix(n, SEED ^ 0xA7)
     gaps = -np.log1p(-((splitmix64(SEED ^ 0x9A, n) >> np.uint64(11)).astype(np.float64) / float(1 << 53))) / lam
@@ -335,7 +345,9 @@ def run_serving(azk, ctx, args):
                "M31 multilinear sum-check over 2^20 evaluations = 4:1",
         "slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb,
         "saturated": {"jobs_per_s": sat_jobs_s, "elems_per_s": sat_elems_s, "jobs": args.serve_backlog, "seconds": t_sat},
-        "offered_load": args.serve_load, "arrival_rate_jobs_per_s": lam,
+        "arrival_rate_jobs_per_s": lam,
+        "arrival_rule": f"{args.serve_load} x saturated server jobs/s" if args.serve_rate <= 0 else "fixed",
+        "batched_superstep_jobs_per_s": batched_jobs_per_s,
         "throughput_elems_per_s": (s1["pcs_elements"] - s0["pcs_elements"]) / t_run, "jobs_per_s": len(mix) / t_run,
         "latency_all": pct(lat), "latency_pcs": pct(lat[kinds == "pcs"]), "latency_sumcheck": pct(lat[kinds == "sc"]),
         "submit_lag_p99_ms": float(np.percentile(lags, 99) * 1e3), "warmup_s": t_warm,
@@ -357,7 +369,9 @@ def config_block(args, logs):
                     f"16-B QM31 leaves, fold to log {args.final_log}, 64 queries, proof bytes on device",
         "instances": len(logs),
         "total_codeword_elems": int(sum(1 << lg for lg in logs)),
-        "schedule": {"treelet_log": args.treelet_log, "group_log": args.group_log, "threads": args.threads, "graph": True},
+        "schedule": ({"treelet_log": args.treelet_log, "group_log": args.group_log, "threads": args.threads, "graph": True} if args.treelet_log else
+                     {"treelet": "tuned per-layer table (cost model over measured timings, csrc/azk_tuned.h pcs_batch)", "group_log": args.group_log,
+                      "threads": args.threads, "graph": True}),
         "l2": "inputs larger than L2 (codewords and trees of one superstep are several GB)",
         "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))} (no data-path collective)",
     }
@@ -373,7 +387,8 @@ def main():
     ap.add_argument("--lo", type=int, default=10)
     ap.add_argument("--hi", type=int, default=22)
     ap.add_argument("--final-log", type=int, default=6)
-    ap.add_argument("--treelet-log", type=int, default=12)
+    ap.add_argument("--treelet-log", type=int, default=0, help="fixed treelet depth (0: the library's tuned per-layer table)")
+    ap.add_argument("--compare-schedules", type=int, default=1)
     ap.add_argument("--group-log", type=int, default=12)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=1)
@@ -385,7 +400,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-backlog", type=int, default=1000)
     ap.add_argument("--serve-load", type=float, default=0.8)
-    ap.add_argument("--serve-seconds", type=float, default=8.0)
+    ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="fixed arrival rate (jobs/s) instead of the load rule")
     args = ap.parse_args()
 
     world, rank, local, dist = dist_setup(args)
@@ -401,7 +417,12 @@ def main():
     import apple_b200 as azk
 
     ctx = azk.Context(local)
-    sched = dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1)
+    # schedule: the library's tuned per-layer table for batched supersteps unless a
+    # fixed treelet depth is asked for
+    if args.treelet_log:
+        sched = dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1)
+    else:
+        sched = dict(group_log=args.group_log, threads=args.threads, use_graph=1)
     batch = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=sched)
     work = batch.work()
     elems = int(sum(1 << lg for lg in logs))
@@ -487,21 +508,44 @@ def main():
             raise errors[0]
         t_pipe = max_over_ranks(dist, t_pipe / (2 * per_lane), local)
         e2e_pipe = world * elems / t_pipe
-        del batch2
+        del batch2, lanes, threads
     e2e_value = e2e_pipe if e2e_pipe else e2e_serial
     t_e2e_report = world * elems / e2e_value
 
-    # ---- plain per-instance form, same instances ----
+    proof_total = batch.proof_total
+
+    # ---- the same superstep with one fixed treelet depth everywhere (the schedule
+    # without the tuner), and the plain per-instance form on its own best schedule
+    # (the single-instance tuned table) ----
+    untuned_value = None
+    if args.compare_schedules and not args.treelet_log:
+        del batch
+        batch = None
+        bu = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=dict(treelet_log=12, group_log=12, threads=256, use_graph=1))
+        bu.upload(host_rows, offsets, counts)
+        bu.prove(pubs)
+        ut = [bu.prove(pubs).gpu_s for _ in range(2)]
+        untuned_value = world * elems / max_over_ranks(dist, statistics.median(ut), local)
+        del bu
     plain_times = []
-    for _ in range(args.plain_steps):
-        st = batch.prove(pubs, plain=True)
-        plain_times.append(st.gpu_s)
+    if args.plain_steps:
+        tables = tuned_tables()
+        psched = dict(layer_treelet=tables["pcs_single"], group_log=args.group_log, threads=args.threads, use_graph=0) if tables and not args.treelet_log \
+            else sched
+        if batch is not None:
+            del batch
+            batch = None
+        bp = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=psched)
+        bp.upload(host_rows, offsets, counts)
+        for _ in range(args.plain_steps):
+            st = bp.prove(pubs, plain=True)
+            plain_times.append(st.gpu_s)
+        del bp
     t_plain = max_over_ranks(dist, statistics.median(plain_times), local) if plain_times else float("nan")
     print(f"[bench] plain: {[round(1000 * g, 2) for g in plain_times]} ms, e2e {[round(1000 * g, 2) for g in e2e_times]} ms, profile {prof}",
           file=sys.stderr, flush=True)
     plain_value = world * elems / t_plain if plain_times else None
 
-    proof_total = batch.proof_total
     # ---- rooflines ----
     int_ops = azk.probe_int_issue(ctx)
     perm_peak = int_ops / 4320.0
@@ -513,9 +557,7 @@ def main():
 
     serving = None
     if not args.no_serve and world == 1:
-        del batch
-        batch = None
-        serving = run_serving(azk, ctx, args)
+        serving = run_serving(azk, ctx, args, len(logs) * args.steps / t_dev)
         print(f"[bench] serving {serving}", file=sys.stderr, flush=True)
 
     line = None
@@ -532,7 +574,10 @@ def main():
             "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/u64 (M31/QM31 field, Keccak lanes)", "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": 1000 * t_plain if plain_values_ok(plain_value) else None,
-                      "batched_over_plain": value / plain_value if plain_values_ok(plain_value) else None},
+                      "batched_over_plain": value / plain_value if plain_values_ok(plain_value) else None,
+                      "schedule": "tuned single-instance per-layer table" if (tuned_tables() and not args.treelet_log) else "same as batched"},
+            "untuned": {"value": untuned_value, "unit": UNIT, "schedule": "treelet depth 12 on every layer",
+                        "tuned_over_untuned": value / untuned_value if untuned_value else None},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e_report,
                     "mode": "two provers alternating (copies of one step overlap kernels of the other)" if e2e_pipe else "serial",
                     "serial_value": e2e_serial, "serial_ms_per_step": 1000 * t_e2e},
@@ -557,7 +602,6 @@ def main():
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    del batch
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
