@@ -19,6 +19,7 @@ from .plans import (  # noqa: F401
     BatchProver,
     CircleCodewordPlan,
     CirclePCSFRIProver,
+    CircleWitnessToFFTBasisPlan,
     Context,
     ProofServer,
     KeccakF1600PermutationPlan,

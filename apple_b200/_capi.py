@@ -112,6 +112,7 @@ PROTOTYPES = {
     "azk_pcs_prover_trace": (I32, [P, P, P, P, P]),
     "azk_pcs_prover_destroy": (None, [P]),
     "azk_batch_create": (I32, [P, U32, P, P, U32, U32, SCHED, PP]),
+    "azk_batch_create_leaves": (I32, [P, U32, P, P, U32, U32, U32, SCHED, PP]),
     "azk_batch_input": (I32, [P, U32, PP]),
     "azk_batch_upload": (I32, [P, P, P, P]),
     "azk_batch_prove": (I32, [P, P, I32, STATS]),
@@ -124,6 +125,10 @@ PROTOTYPES = {
     "azk_batch_destroy": (None, [P]),
     "azk_probe_int_issue": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
     "azk_sumcheck_prove": (I32, [P, P, U64, P, P, P, U32P, U32P, P, STATS]),
+    "azk_witness_plan_create": (I32, [P, U32, PP]),
+    "azk_witness_plan_execute": (I32, [P, P, U64, P, U64, P, STATS]),
+    "azk_witness_plan_execute_resident": (I32, [P, P, U64, U64, P, U64, U64, P, U64, STATS]),
+    "azk_witness_plan_destroy": (None, [P]),
     "azk_server_create": (I32, [P, U64, U32, SCHED, PP]),
     "azk_server_submit_pcs": (I32, [P, U32, U32, U32, U32, P, U64, P, U64P]),
     "azk_server_submit_sumcheck": (I32, [P, P, U64, U64P]),

@@ -22,6 +22,8 @@ enum LeafKind : uint32_t {
   kLeafQM31 = 1,    // 16-byte little-endian QM31 values
   kLeafFold = 2,    // fold of a previous QM31 layer, then hashed (layer written out)
   kLeafDigest = 3,  // prehashed 32-byte digests
+  kLeafQM31x4 = 4,  // 64-byte leaves of 4 consecutive QM31 values
+  kLeafFoldx4 = 5,  // fold of a previous layer into 4 values per 64-byte leaf, then hashed
 };
 
 enum RootAction : uint32_t {
@@ -196,6 +198,13 @@ cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_
 cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, uint32_t nidx, uint64_t* d_out, cudaStream_t s);
 cudaError_t launch_domain_tables(uint32_t logn, uint32_t* d_tw, uint32_t* d_inv, cudaStream_t s);
 cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
+// Witness columns -> FFT basis (witness_kernels.cu): factorial tables of n
+// entries (seg: ceil(n/1024) words of scratch), then the transform of two columns
+// of count_x / count_y monomial coefficients into 2n interleaved QM31.
+cudaError_t launch_witness_tables(uint64_t n, uint32_t* fact, uint32_t* seg, uint32_t* ifact, uint32_t* scale, cudaStream_t s);
+cudaError_t launch_witness_transform(const uint4* x, uint64_t count_x, const uint4* y, uint64_t count_y, uint64_t n, const uint32_t* ifact,
+                                     const uint32_t* scale, uint4* ax, uint4* ay, uint4* cx, uint4* cy, uint4* out, cudaStream_t s);
+
 // `narrow`: the work items' inputs are lifted M31 polynomials (one-limb kernel).
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s);
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears

@@ -1,6 +1,7 @@
 // SHA3 Merkle commitment kernels: fused leaf hashing + shared-memory treelets +
 // last-arriver upper levels, for raw leaves, prehashed digests, QM31 layers and
-// fold-then-hash layers (reference: MerkleCommitter.swift:526-1063 and the Metal
+// fold-then-hash layers with 16-byte leaves of one QM31 value or 64-byte leaves of
+// four (reference: MerkleCommitter.swift:526-1063 and the Metal
 // kernels HashMerkleKernels.metal:1064-1292; oracle MerkleOracle.swift:4-141).
 //
 // Tree layout: level 0 (leaf digests) optional; levels >= 1 in `inner`, level l
@@ -116,6 +117,26 @@ __device__ __forceinline__ uint32_t leaf_setup(const TreeJob& job, uint64_t leaf
     a[2] = 0x06;
     a[16] = kPadEnd;
     return 1;
+  } else if constexpr (KIND == kLeafQM31x4 || KIND == kLeafFoldx4) {
+    // leaf = values 4*leaf .. 4*leaf+3 (64 bytes, 8 lanes)
+#pragma unroll
+    for (uint32_t m = 0; m < 4; m++) {
+      const uint64_t e = 4 * leaf + m;
+      uint4 v;
+      if constexpr (KIND == kLeafQM31x4) {
+        v = __ldg(job.layer + e);
+      } else {
+        uint4 p = __ldg(job.layer + 2 * e), q = __ldg(job.layer + 2 * e + 1);
+        qm31 r = fri_fold_pair(qm31{p.x, p.y, p.z, p.w}, qm31{q.x, q.y, q.z, q.w}, __ldg(job.inv + e), qm31{ch[0], ch[1], ch[2], ch[3]});
+        v = make_uint4(r.a, r.b, r.c, r.d);
+        job.out_layer[e] = v;
+      }
+      a[2 * m] = (uint64_t)v.x | ((uint64_t)v.y << 32);
+      a[2 * m + 1] = (uint64_t)v.z | ((uint64_t)v.w << 32);
+    }
+    a[8] = 0x06;
+    a[16] = kPadEnd;
+    return 1;
   } else {
     xor_message(a, job.raw + leaf * job.stride, job.len, job.aligned8 != 0);
     if (job.len == 136) return 2;
@@ -223,7 +244,7 @@ __device__ __forceinline__ void tree_tile_body(const TreeJob& job, const uint64_
   uint64_t* bufB = sm + 4 * Q;   // Q/2 digests
 
   uint32_t ch[4] = {0, 0, 0, 0};
-  if constexpr (KIND == kLeafFold) {
+  if constexpr (KIND == kLeafFold || KIND == kLeafFoldx4) {
     if (threadIdx.x < 4) s_ch[threadIdx.x] = __ldcg(job.fold_ch + threadIdx.x);
     __syncthreads();
 #pragma unroll
@@ -297,6 +318,8 @@ cudaError_t prepare_tree_kernels() {
   if (e == cudaSuccess) e = prepare_kind<kLeafQM31>();
   if (e == cudaSuccess) e = prepare_kind<kLeafFold>();
   if (e == cudaSuccess) e = prepare_kind<kLeafDigest>();
+  if (e == cudaSuccess) e = prepare_kind<kLeafQM31x4>();
+  if (e == cudaSuccess) e = prepare_kind<kLeafFoldx4>();
   return e;
 }
 
@@ -321,6 +344,8 @@ cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_
     case kLeafQM31: return launch_kind<kLeafQM31>(d_jobs, d_work, nwork, max_tile_log, threads, s);
     case kLeafFold: return launch_kind<kLeafFold>(d_jobs, d_work, nwork, max_tile_log, threads, s);
     case kLeafDigest: return launch_kind<kLeafDigest>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafQM31x4: return launch_kind<kLeafQM31x4>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafFoldx4: return launch_kind<kLeafFoldx4>(d_jobs, d_work, nwork, max_tile_log, threads, s);
     default: return cudaErrorInvalidValue;
   }
 }

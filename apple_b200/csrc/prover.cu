@@ -37,6 +37,7 @@ namespace {
 struct InstanceCfg {
   uint32_t logn, rounds, queries, log_blowup, grinding;
   std::vector<uint64_t> claimed;
+  uint32_t leaf_values = 1;  // QM31 values per Merkle leaf: 1 (16-byte leaves) or 4 (64-byte leaves)
 };
 
 struct Engine {
@@ -55,6 +56,7 @@ struct Engine {
 
   std::vector<PcsInstance> h_inst;
   // FFT
+  uint32_t leaf_values = 1;  // all instances of an engine share the leaf size
   FftPlan fft;
   std::vector<FftJob> fft_transforms;
   std::vector<uint8_t> fft_narrow;  // per instance: input known to be a lifted M31 polynomial
@@ -170,7 +172,11 @@ struct Engine {
     AZK_CU(cudaSetDevice(ctx->device));
     AZK_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     size_t n = cfg.size();
+    leaf_values = cfg.empty() ? 1 : cfg[0].leaf_values;
     for (auto& i : cfg) {
+      layout(i.leaf_values == leaf_values && (leaf_values == 1 || leaf_values == 4), "all instances of a batch share one leaf size (16 or 64 bytes)");
+      // a 64-byte leaf holds 4 values: every committed layer needs at least 4
+      layout(leaf_values == 1 || i.logn >= i.rounds + 1, "64-byte leaves need at least 4 values in every committed layer");
       rmax = std::max(rmax, i.rounds);
       qmax = std::max(qmax, i.queries);
       any_grinding |= i.grinding > 0;
@@ -192,7 +198,7 @@ struct Engine {
       off_qp[i] = arena.reserve(4ull * c2.queries);
       off_claim[i] = arena.reserve(8ull * c2.claimed.size());
       off_cnt[i] = arena.reserve(4 * tree_counter_count(c2.logn, 1));
-      proof_len[i] = proof_total_bytes(c2.logn, c2.rounds, c2.queries, (uint32_t)c2.claimed.size(), c2.grinding > 0);
+      proof_len[i] = c2.leaf_values == 1 ? proof_total_bytes(c2.logn, c2.rounds, c2.queries, (uint32_t)c2.claimed.size(), c2.grinding > 0) : 0;
     }
     uint64_t pbase = arena.reserve(0);
     arena.used = pbase;
@@ -270,12 +276,13 @@ struct Engine {
         const auto& c2 = cfg[i];
         if (k >= c2.rounds) continue;
         const PcsInstance& I = h_inst[i];
-        uint32_t lg = c2.logn - k;
+        // leaves of layer k: 2^(logn - k) values, one or four per leaf
+        uint32_t lg = c2.logn - k - (leaf_values == 4 ? 2 : 0);
         uint32_t tl = tree_tile_log(sched, lg);
         if (tl == 0 && lg > 0) tl = 1;
         TreeJob j{};
         j.logn = lg;
-        j.kind = k == 0 ? kLeafQM31 : kLeafFold;
+        j.kind = tree_kind(k);
         j.tile_log = tl;
         j.group_log = std::max<uint32_t>(1, std::min(sched.group_log, tl));
         if (k == 0) {
@@ -345,10 +352,13 @@ struct Engine {
     ensure_events(fft.step_cnt.size() + 2 * rmax + 8);
   }
 
+  uint32_t tree_kind(uint32_t k) const {
+    if (leaf_values == 4) return k == 0 ? kLeafQM31x4 : kLeafFoldx4;
+    return k == 0 ? kLeafQM31 : kLeafFold;
+  }
   void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt) {
     if (!cnt) return;
-    AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], k == 0 ? kLeafQM31 : kLeafFold,
-                            sched.threads, s));
+    AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], tree_kind(k), sched.threads, s));
   }
   void launch_fold_range(uint64_t off, uint64_t cnt) {
     if (!cnt) return;
@@ -384,7 +394,11 @@ struct Engine {
     AZK_CU(launch_pcs_finalize(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
     prof_end();
   }
+  // Proof bytes exist only for 16-byte leaves (the reference's verifier opens one
+  // QM31 value per leaf); a 64-byte-leaf chain ends with its final layer.
+  bool has_proofs() const { return leaf_values == 1; }
   void enqueue_tail_batched() {
+    if (!has_proofs()) return;
     prof_begin(3);
     AZK_CU(launch_pcs_queries(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
     AZK_CU(launch_pcs_emit(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), qmax, s));
@@ -401,6 +415,7 @@ struct Engine {
       if (k == cfg[i].rounds) launch_fold_range(fstep_inst[k][i].first, fstep_inst[k][i].second);
     }
     AZK_CU(launch_pcs_finalize(d_inst(), id, 1, s));
+    if (!has_proofs()) return;
     grind_instance(i);
     AZK_CU(launch_pcs_queries(d_inst(), id, 1, s));
     AZK_CU(launch_pcs_emit(d_inst(), id, 1, cfg[i].queries, s));
@@ -663,20 +678,26 @@ azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint3
 }
 
 // ---- batch ----
-azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* logs, const uint32_t* rounds, uint32_t log_blowup, uint32_t queries,
-                            const azk_schedule* schedule, azk_batch** out) {
+azk_status azk_batch_create_leaves(azk_ctx* ctx, uint32_t count, const uint32_t* logs, const uint32_t* rounds, uint32_t log_blowup, uint32_t queries,
+                                   uint32_t leaf_bytes, const azk_schedule* schedule, azk_batch** out) {
   return guarded(ctx, [&] {
     layout(ctx && out && logs && rounds && count >= 1);
+    layout(leaf_bytes == 16 || leaf_bytes == 64, "leaf_bytes must be 16 (one QM31 per leaf) or 64 (four)");
     std::vector<InstanceCfg> cf;
     for (uint32_t i = 0; i < count; i++) {
       validate_params(logs[i], log_blowup, queries, 0, rounds[i]);
-      cf.push_back(InstanceCfg{logs[i], rounds[i], queries, log_blowup, 0, {}});
+      cf.push_back(InstanceCfg{logs[i], rounds[i], queries, log_blowup, 0, {}, leaf_bytes / 16});
     }
     auto b = std::make_unique<azk_batch>();
     b->ctx = ctx;
     b->eng.init(ctx, cf, resolve_schedule(schedule, kTuned_pcs_batch));
     *out = b.release();
   });
+}
+
+azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* logs, const uint32_t* rounds, uint32_t log_blowup, uint32_t queries,
+                            const azk_schedule* schedule, azk_batch** out) {
+  return azk_batch_create_leaves(ctx, count, logs, rounds, log_blowup, queries, 16, schedule, out);
 }
 
 azk_status azk_batch_input(azk_batch* b, uint32_t i, void** dev) {
@@ -739,6 +760,7 @@ azk_status azk_batch_download_proofs(azk_batch* b, uint8_t* out, uint64_t cap) {
     layout(b && out);
     std::lock_guard<std::mutex> lk(b->mu);
     Engine& e = b->eng;
+    layout(e.has_proofs(), "a 64-byte-leaf batch produces commitments, challenges and final layers (azk_batch_trace), not proof bytes");
     uint64_t pos = 0;
     for (size_t i = 0; i < e.cfg.size(); i++) {
       layout(pos + e.proof_len[i] <= cap, "proof buffer too small");
@@ -1110,9 +1132,10 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     layout(ctx && out && slots >= 1 && slots <= 64 && hbm_budget_bytes > 0);
     auto sv = std::make_unique<azk_server>();
     sv->ctx = ctx;
-    // many jobs share the device at once, so the throughput table (many trees per
-    // launch) fits better than the single-tree latency table
-    sv->sched = resolve_schedule(schedule, kTuned_pcs_batch);
+    // each job is one instance: the single-tree table (measured on the serving mix:
+    // the lowest latency per job at a throughput equal to the batch table's within
+    // run-to-run spread)
+    sv->sched = resolve_schedule(schedule, kTuned_pcs_single);
     sv->budget = hbm_budget_bytes;
     sv->slots = slots;
     sv->cache.resize(slots);

@@ -786,6 +786,103 @@ azk_status azk_codeword_plan_execute_resident(azk_codeword_plan* p, const void* 
 }
 void azk_codeword_plan_destroy(azk_codeword_plan* p) { delete p; }
 
+}  // extern "C"
+
+// ---- witness columns -> FFT basis (CircleWitnessToFFTBasisPlanV1) ----
+struct azk_witness_plan {
+  azk_ctx* ctx;
+  std::mutex mu;
+  cudaStream_t s = nullptr;
+  uint32_t logn;
+  uint64_t n;  // coefficient capacity = half the domain
+  DevBuf fact, seg, ifact, scale, ax, ay, cx, cy, xin, yin, out, flag;
+  ~azk_witness_plan() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+static void witness_run(azk_witness_plan* p, const uint4* x, uint64_t nx, const uint4* y, uint64_t ny, uint4* out, azk_stats* st, const Timer& t) {
+  // canonicality of both columns (CircleWitnessFFTBasis.swift:374-385)
+  AZK_CU(cudaMemsetAsync(p->flag.p, 0, 4, p->s));
+  if (nx) AZK_CU(launch_check_canonical(reinterpret_cast<const uint32_t*>(x), 4 * nx, p->flag.as<uint32_t>(), p->s));
+  if (ny) AZK_CU(launch_check_canonical(reinterpret_cast<const uint32_t*>(y), 4 * ny, p->flag.as<uint32_t>(), p->s));
+  uint32_t bad = 0;
+  AZK_CU(cudaMemcpyAsync(&bad, p->flag.p, 4, cudaMemcpyDeviceToHost, p->s));
+  sync_stream(p->s);
+  layout(bad == 0, "witness coefficients contain a non-canonical field element");
+  GpuTimer g(p->s);
+  AZK_CU(launch_witness_transform(x, nx, y, ny, p->n, p->ifact.as<uint32_t>(), p->scale.as<uint32_t>(), p->ax.as<uint4>(), p->ay.as<uint4>(),
+                                  p->cx.as<uint4>(), p->cy.as<uint4>(), out, p->s));
+  g.stop();
+  fill_stats(st, t, 0, g.seconds());
+}
+
+extern "C" {
+
+azk_status azk_witness_plan_create(azk_ctx* ctx, uint32_t log_size, azk_witness_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && log_size >= 1 && log_size <= 22);
+    AZK_CU(cudaSetDevice(ctx->device));
+    auto p = std::make_unique<azk_witness_plan>();
+    p->ctx = ctx;
+    p->logn = log_size;
+    p->n = 1ull << (log_size - 1);
+    p->s = new_stream();
+    const uint64_t n = p->n;
+    p->fact.alloc(4 * n, "Witness.Factorials");
+    p->seg.alloc(4 * ((n + 1023) / 1024), "Witness.Segments");
+    p->ifact.alloc(4 * n, "Witness.InverseFactorials");
+    p->scale.alloc(4 * n, "Witness.Scale");
+    for (DevBuf* b : {&p->ax, &p->ay, &p->cx, &p->cy, &p->xin, &p->yin}) b->alloc(16 * n, "Witness.Scratch");
+    p->out.alloc(32 * n, "Witness.Output");
+    p->flag.alloc(16, "Witness.Flag");
+    AZK_CU(launch_witness_tables(n, p->fact.as<uint32_t>(), p->seg.as<uint32_t>(), p->ifact.as<uint32_t>(), p->scale.as<uint32_t>(), p->s));
+    sync_stream(p->s);
+    *out = p.release();
+  });
+}
+
+// Host columns x, y of monomial coefficients (QM31) -> 2 * capacity interleaved
+// FFT-basis coefficients [x0, y0, x1, y1, ...].
+azk_status azk_witness_plan_execute(azk_witness_plan* p, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny, uint32_t* out,
+                                    azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && out && (x || !nx) && (y || !ny));
+    // CircleWitnessFFTBasis.swift:349-353
+    layout(nx <= p->n && ny <= p->n && nx + ny > 0);
+    std::lock_guard<std::mutex> lk(p->mu);
+    Timer t;
+    if (nx) AZK_CU(cudaMemcpyAsync(p->xin.p, x, 16 * nx, cudaMemcpyHostToDevice, p->s));
+    if (ny) AZK_CU(cudaMemcpyAsync(p->yin.p, y, 16 * ny, cudaMemcpyHostToDevice, p->s));
+    witness_run(p, p->xin.as<uint4>(), nx, p->yin.as<uint4>(), ny, p->out.as<uint4>(), st, t);
+    AZK_CU(cudaMemcpyAsync(out, p->out.p, 32 * p->n, cudaMemcpyDeviceToHost, p->s));
+    sync_stream(p->s);
+  });
+}
+
+// executeResident (CircleWitnessFFTBasis.swift:320-428): device columns and a
+// device output of 2 * capacity QM31 that must not overlap either column.
+azk_status azk_witness_plan_execute_resident(azk_witness_plan* p, const void* dx, uint64_t x_off, uint64_t nx, const void* dy, uint64_t y_off, uint64_t ny,
+                                             void* dout, uint64_t out_off, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && dout && (dx || !nx) && (dy || !ny));
+    layout(nx <= p->n && ny <= p->n && nx + ny > 0);
+    layout(x_off % 16 == 0 && y_off % 16 == 0 && out_off % 16 == 0);
+    const uint8_t* xb = static_cast<const uint8_t*>(dx) + x_off;
+    const uint8_t* yb = static_cast<const uint8_t*>(dy) + y_off;
+    uint8_t* ob = static_cast<uint8_t*>(dout) + out_off;
+    const uint64_t ob_len = 32 * p->n;
+    auto overlap = [&](const uint8_t* a, uint64_t alen) { return alen && a < ob + ob_len && ob < a + alen; };
+    layout(!overlap(xb, 16 * nx) && !overlap(yb, 16 * ny), "the output range overlaps a witness column");
+    std::lock_guard<std::mutex> lk(p->mu);
+    Timer t;
+    witness_run(p, reinterpret_cast<const uint4*>(xb), nx, reinterpret_cast<const uint4*>(yb), ny, reinterpret_cast<uint4*>(ob), st, t);
+    sync_stream(p->s);
+  });
+}
+
+void azk_witness_plan_destroy(azk_witness_plan* p) { delete p; }
+
 // ---- folds ----
 static void check_qm31(const uint32_t* v, uint64_t words) {
   for (uint64_t i = 0; i < words; i++) layout(v[i] < kP);

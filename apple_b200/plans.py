@@ -297,6 +297,34 @@ class CircleCodewordPlan(_Plan):
         return st
 
 
+class CircleWitnessToFFTBasisPlan(_Plan):
+    """CircleWitnessToFFTBasisPlanV1 (CircleWitnessFFTBasis.swift:226-590): monomial
+    witness columns -> interleaved Circle FFT-basis coefficients, on the device."""
+
+    _destroy = "azk_witness_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int):
+        super().__init__(ctx)
+        self.log_size = log_size
+        self._check(lib().azk_witness_plan_create(ctx.handle, log_size, ctypes.byref(self._h)))
+
+    def execute(self, x_coefficients, y_coefficients=()) -> np.ndarray:
+        x = _q(x_coefficients) if len(x_coefficients) else np.zeros((0, 4), np.uint32)
+        y = _q(y_coefficients) if len(y_coefficients) else np.zeros((0, 4), np.uint32)
+        out = np.empty((1 << self.log_size, 4), np.uint32)
+        st = Stats()
+        self._check(lib().azk_witness_plan_execute(self._h, _ptr(x) if len(x) else None, len(x), _ptr(y) if len(y) else None, len(y), _ptr(out),
+                                                   ctypes.byref(st)))
+        self.last_stats = st
+        return out
+
+    def execute_resident(self, dev_x, x_count, dev_y, y_count, dev_out, x_offset=0, y_offset=0, out_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_witness_plan_execute_resident(self._h, dev_x, x_offset, x_count, dev_y, y_offset, y_count, dev_out, out_offset,
+                                                            ctypes.byref(st)))
+        return st
+
+
 def qm31_fold(ctx: Context, evaluations, inverse_points, challenge) -> np.ndarray:
     """QM31FRIFoldPlan.execute (QM31FRIFold.swift:960-1117)."""
     ev, inv, ch = _q(evaluations), _q(inverse_points), _q(challenge)
@@ -424,14 +452,16 @@ class BatchProver(_Plan):
 
     _destroy = "azk_batch_destroy"
 
-    def __init__(self, ctx: Context, log_sizes, rounds, log_blowup: int, queries: int, schedule=None):
+    def __init__(self, ctx: Context, log_sizes, rounds, log_blowup: int, queries: int, schedule=None, leaf_bytes: int = 16):
         super().__init__(ctx)
         self.log_sizes = [int(v) for v in log_sizes]
         self.rounds = [int(v) for v in rounds]
         self.queries = queries
+        self.leaf_bytes = leaf_bytes
         ls = np.ascontiguousarray(self.log_sizes, dtype=np.uint32)
         rs = np.ascontiguousarray(self.rounds, dtype=np.uint32)
-        self._check(lib().azk_batch_create(ctx.handle, len(ls), _ptr(ls), _ptr(rs), log_blowup, queries, _sched(schedule), ctypes.byref(self._h)))
+        self._check(lib().azk_batch_create_leaves(ctx.handle, len(ls), _ptr(ls), _ptr(rs), log_blowup, queries, leaf_bytes, _sched(schedule),
+                                                  ctypes.byref(self._h)))
         sizes = np.empty(len(ls), np.uint64)
         total = ctypes.c_uint64()
         self._check(lib().azk_batch_proof_sizes(self._h, _ptr(sizes), ctypes.byref(total)))

@@ -389,6 +389,7 @@ def main():
     ap.add_argument("--final-log", type=int, default=6)
     ap.add_argument("--treelet-log", type=int, default=0, help="fixed treelet depth (0: the library's tuned per-layer table)")
     ap.add_argument("--compare-schedules", type=int, default=1)
+    ap.add_argument("--leaf64", type=int, default=1)
     ap.add_argument("--group-log", type=int, default=12)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=1)
@@ -542,6 +543,22 @@ def main():
             plain_times.append(st.gpu_s)
         del bp
     t_plain = max_over_ranks(dist, statistics.median(plain_times), local) if plain_times else float("nan")
+
+    # ---- the same superstep with 64-byte Merkle leaves (4 QM31 per leaf): the
+    # survey's second C4 row; bit-exact against the oracle's 64-byte-leaf chain, no
+    # verifier proof format ----
+    leaf64 = None
+    if args.leaf64:
+        b64 = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=sched, leaf_bytes=64)
+        b64.upload(host_rows, offsets, counts)
+        for _ in range(args.warmup):
+            b64.prove(pubs)
+        lt = [b64.prove(pubs).gpu_s for _ in range(max(2, args.steps // 2))]
+        t64 = max_over_ranks(dist, statistics.median(lt), local)
+        w64 = b64.work()
+        leaf64 = {"value": world * elems / t64, "unit": UNIT, "ms_per_step": 1000 * t64, "tree_permutations": w64["tree_permutations"],
+                  "output": "commitments, challenges, final layers (no proof encoding: the reference's verifier opens 16-byte leaves)"}
+        del b64
     print(f"[bench] plain: {[round(1000 * g, 2) for g in plain_times]} ms, e2e {[round(1000 * g, 2) for g in e2e_times]} ms, profile {prof}",
           file=sys.stderr, flush=True)
     plain_value = world * elems / t_plain if plain_times else None
@@ -576,6 +593,7 @@ def main():
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": 1000 * t_plain if plain_values_ok(plain_value) else None,
                       "batched_over_plain": value / plain_value if plain_values_ok(plain_value) else None,
                       "schedule": "tuned single-instance per-layer table" if (tuned_tables() and not args.treelet_log) else "same as batched"},
+            "leaf64": leaf64,
             "untuned": {"value": untuned_value, "unit": UNIT, "schedule": "treelet depth 12 on every layer",
                         "tuned_over_untuned": value / untuned_value if untuned_value else None},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e_report,

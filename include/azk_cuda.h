@@ -228,6 +228,15 @@ void azk_pcs_prover_destroy(azk_pcs_prover* p);
  * proof emission), optionally captured in a CUDA graph. */
 azk_status azk_batch_create(azk_ctx* ctx, uint32_t count, const uint32_t* log_sizes, const uint32_t* rounds, uint32_t log_blowup,
                             uint32_t queries, const azk_schedule* schedule, azk_batch** out);
+/* Same with the Merkle leaf size of every committed layer: 16 bytes (one QM31
+ * value per leaf, the reference's layout, CircleFRIFoldPlan.swift:1055-1062) or 64
+ * bytes (four consecutive values per leaf; same transcript frames and folds, every
+ * committed layer needs >= 4 values).  A 64-byte-leaf batch yields commitments,
+ * challenges and final layers through azk_batch_trace; it has no proof encoding
+ * (the reference's verifier opens 16-byte leaves), so azk_batch_download_proofs
+ * fails and azk_batch_proof_sizes reports 0. */
+azk_status azk_batch_create_leaves(azk_ctx* ctx, uint32_t count, const uint32_t* log_sizes, const uint32_t* rounds, uint32_t log_blowup,
+                                   uint32_t queries, uint32_t leaf_bytes, const azk_schedule* schedule, azk_batch** out);
 /* Device pointer of instance i's coefficient input (N_i QM31); the caller may
  * fill it in place (resident input).  Fetching the pointer drops what the last
  * azk_batch_upload learned about that input (its nonzero prefix, whether it is a
@@ -254,6 +263,23 @@ azk_status azk_batch_profile(azk_batch* b, double* seconds4);
  * single-pass FFT bytes, final-fold bytes, and kernel launches per superstep. */
 azk_status azk_batch_work(azk_batch* b, uint64_t* tree_permutations, uint64_t* fft_bytes, uint64_t* fold_bytes, uint32_t* launches);
 void azk_batch_destroy(azk_batch* b);
+
+/* ---- witness columns -> Circle FFT-basis coefficients
+ * (CircleWitnessToFFTBasisPlanV1, CircleWitnessFFTBasis.swift:226-590) ----
+ * For a domain of 2^log_size points (log_size 1...22): x and y monomial
+ * coefficient columns (QM31, at most 2^(log_size-1) each, not both empty) become
+ * the interleaved FFT-basis buffer [x0, y0, x1, y1, ...] of 2^log_size QM31 that
+ * azk_pcs_prover_prove_coefficients / azk_codeword_plan_execute take.  Work grows
+ * with the square of the longer column (the reference's dense matrix), without a
+ * matrix in memory.  Non-canonical coefficients fail with
+ * AZK_ERR_INVALID_INPUT_LAYOUT; so does a resident output that overlaps a column. */
+typedef struct azk_witness_plan azk_witness_plan;
+azk_status azk_witness_plan_create(azk_ctx* ctx, uint32_t log_size, azk_witness_plan** out);
+azk_status azk_witness_plan_execute(azk_witness_plan* plan, const uint32_t* x_coefficients, uint64_t x_count, const uint32_t* y_coefficients,
+                                    uint64_t y_count, uint32_t* fft_basis_out, azk_stats* stats);
+azk_status azk_witness_plan_execute_resident(azk_witness_plan* plan, const void* dev_x, uint64_t x_offset, uint64_t x_count, const void* dev_y,
+                                             uint64_t y_offset, uint64_t y_count, void* dev_out, uint64_t out_offset, azk_stats* stats);
+void azk_witness_plan_destroy(azk_witness_plan* plan);
 
 /* ---- M31 multilinear sum-check (M31MultilinearSumcheckProofBuilderV1.prove,
  * SumcheckOracle.swift:797-868) ----

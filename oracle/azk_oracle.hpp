@@ -1002,6 +1002,34 @@ inline Proof build_proof(const std::vector<QM31>& evaluations, const Domain& d, 
 }
 
 // ---------------------------------------------------------------------------
+// Commit-and-fold chain with 64-byte Merkle leaves (4 consecutive QM31, little-
+// endian, per leaf): the transcript frames and folds of build_proof (header,
+// domain, security, public input, per round commitment + challenge), with each
+// layer's root taken over n/4 leaves of 64 bytes (MerkleOracle.swift:4-51 on the
+// packed layer).  The reference's verifier reads 16-byte leaves, so this chain has
+// commitments, challenges and a final layer but no proof encoding.
+// ---------------------------------------------------------------------------
+inline ProverTrace commit_fold_chain_leaf64(const std::vector<QM31>& evaluations, const Domain& d, const Security& s, const Digest& pub, u32 rounds) {
+  require(d.storageOrder == 1 && d.canonical() && evaluations.size() == d.size() && rounds > 0 && rounds + 1 <= d.logSize);
+  validate_security(s);
+  for (auto& e : evaluations) require(q_canonical(e));
+  auto inv = inverse_domain_layers(d, rounds);
+  ProverTrace tr;
+  Transcript t = transcript_prefix(d, s, pub);
+  std::vector<QM31> cur = evaluations;
+  for (u32 r = 0; r < rounds; r++) {
+    Bytes b = pack_qm31(cur);
+    MerkleTree tree = merkle_raw(b.data(), b.size(), cur.size() / 4, 64, 64);
+    tr.commitments.push_back(tree.root());
+    QM31 c = transcript_round(t, r, tr.commitments.back());
+    tr.challenges.push_back(c);
+    cur = fold(cur, lift(inv[r]), c);
+  }
+  tr.finalLayer = cur;
+  return tr;
+}
+
+// ---------------------------------------------------------------------------
 // Verifier (CirclePCSFRIProofVerifierV1.verify, CircleProofFormat.swift:1397-1488)
 // ---------------------------------------------------------------------------
 inline bool verify_value_opening(const ValueOpening& o, const Digest& root, u64 idx, size_t sibCount) {

@@ -277,6 +277,18 @@ int azko_prove(u32 logSize, const u32* evaluations, u32 logBlowup, u32 queries, 
   AZKO_CATCH
 }
 
+int azko_commit_fold_chain_leaf64(u32 logSize, const u32* evaluations, u32 logBlowup, u32 queries, const u8* pub, u32 rounds, u8* commitOut,
+                                  u32* chOut, u32* finalOut) {
+  AZKO_TRY
+  Domain d = canonical_domain(logSize);
+  Security s{logBlowup, queries, 1, 0};
+  ProverTrace tr = commit_fold_chain_leaf64(q_vec(evaluations, d.size()), d, s, dg(pub), rounds);
+  for (u32 r = 0; r < rounds; r++) std::memcpy(commitOut + 32 * r, tr.commitments[r].b, 32);
+  q_out(tr.challenges, chOut);
+  q_out(tr.finalLayer, finalOut);
+  AZKO_CATCH
+}
+
 // 1 accepted, 0 rejected, negative if the bytes do not decode.
 int azko_verify(const u8* proof, u64 n, const u8* pub) {
   try {

@@ -315,6 +315,18 @@ def prove(log_size: int, evaluations, log_blowup: int, queries: int, public_dige
     return ProofResult(out[: plen.value].tobytes(), [cm[32 * r:32 * r + 32].tobytes() for r in range(rounds)], ch, fin, [int(v) for v in qp])
 
 
+def commit_fold_chain_leaf64(log_size: int, evaluations, log_blowup: int, queries: int, public_digest: bytes, rounds: int):
+    """Commitments, challenges and final layer of the chain with 64-byte (4 x QM31) Merkle leaves."""
+    ev = _q(evaluations)
+    pub = _bytes(public_digest)
+    cm = np.zeros(32 * rounds, np.uint8)
+    ch = np.zeros((rounds, 4), np.uint32)
+    fl = np.zeros(((1 << log_size) >> rounds, 4), np.uint32)
+    _check(lib().azko_commit_fold_chain_leaf64(c_u32(log_size), _p32(ev), c_u32(log_blowup), c_u32(queries), _p8(pub), c_u32(rounds), _p8(cm),
+                                               _p32(ch), _p32(fl)))
+    return [cm[32 * k:32 * k + 32].tobytes() for k in range(rounds)], ch, fl
+
+
 def verify(proof: bytes, public_digest: bytes) -> bool:
     pb, pub = _bytes(proof), _bytes(public_digest)
     rc = lib().azko_verify(_p8(pb), c_u64(len(pb)), _p8(pub))

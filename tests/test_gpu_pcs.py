@@ -215,3 +215,35 @@ def test_batch_mixes_m31_and_qm31_instances(ctx, oracle):
     b.prove(pubs)
     want = oracle.prove(logs[0], oracle.fft_evaluate(logs[0], full), 2, 8, pubs[:32], rounds[0]).proof
     assert b.proofs()[0] == want
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_batch_64_byte_leaves_match_oracle(ctx, oracle, plain):
+    """64-byte Merkle leaves (4 QM31 per leaf): commitments, challenges and final layers
+    of every instance equal the oracle's chain; no proof bytes exist for this layout."""
+    logs = [14, 9, 12, 7, 16, 11]
+    rounds = [lg - 6 if lg > 7 else 1 for lg in logs]
+    flat, offs, cnts = _batch_inputs(logs, 64)
+    flat[offs[1]:offs[1] + cnts[1], 1:] = 0  # one lifted-M31 instance
+    b = azk.BatchProver(ctx, logs, rounds, 2, 16, leaf_bytes=64)
+    b.upload(flat, offs, cnts)
+    pubs = bytes((3 * i + 1) & 0xFF for i in range(32 * len(logs)))
+    b.prove(pubs, plain=plain)
+    for i, lg in enumerate(logs):
+        full = np.zeros((1 << lg, 4), np.uint32)
+        full[:cnts[i]] = flat[offs[i]:offs[i] + cnts[i]]
+        cm, ch, fl = oracle.commit_fold_chain_leaf64(lg, oracle.fft_evaluate(lg, full), 2, 16, pubs[32 * i:32 * i + 32], rounds[i])
+        gcm, gch, gfl, _ = b.trace(i)
+        assert gcm == cm, i
+        assert np.array_equal(gch, ch), i
+        assert np.array_equal(gfl, fl), i
+    assert b.proof_total == 0
+    with pytest.raises(azk.AZKError):
+        b.proofs()
+
+
+def test_batch_64_byte_leaves_need_four_values_per_layer(ctx):
+    with pytest.raises(azk.AZKError):
+        azk.BatchProver(ctx, [8], [8], 2, 4, leaf_bytes=64)
+    with pytest.raises(azk.AZKError):
+        azk.BatchProver(ctx, [8], [2], 2, 4, leaf_bytes=32)

@@ -298,3 +298,26 @@ def test_multilinear_sumcheck_relations(oracle):
         assert (int(z) + int(o)) % G.P == prev
         prev = ((1 - int(c)) * int(z) + int(c) * int(o)) % G.P
     assert prev == p["final"]
+
+
+def test_leaf64_chain_is_built_from_pinned_parts(oracle):
+    """The 64-byte-leaf chain (4 QM31 per Merkle leaf) uses the pinned pieces: each
+    commitment is the raw-leaf Merkle root of the packed layer over n/4 leaves of 64
+    bytes, the layers follow the Circle fold chain with the chain's challenges, and
+    with the same frames the first challenge differs from the 16-byte-leaf proof's
+    only because the committed root differs."""
+    import numpy as np
+
+    rng = np.random.default_rng(64)
+    log_size, rounds = 9, 5
+    ev = rng.integers(0, (1 << 31) - 1, size=(1 << log_size, 4), dtype=np.uint32)
+    pub = bytes(range(32))
+    cm, ch, fl = oracle.commit_fold_chain_leaf64(log_size, ev, 2, 8, pub, rounds)
+    assert len(cm) == rounds and ch.shape == (rounds, 4) and fl.shape == ((1 << log_size) >> rounds, 4)
+    for r in range(rounds):
+        layer = ev if r == 0 else oracle.circle_fold_chain(log_size, ev, ch[:r])
+        packed = np.ascontiguousarray(layer, dtype="<u4").tobytes()
+        assert cm[r] == oracle.merkle_root(packed, len(layer) // 4, 64, 64)
+    assert np.array_equal(fl, oracle.circle_fold_chain(log_size, ev, ch))
+    p16 = oracle.prove(log_size, ev, 2, 8, pub, rounds)
+    assert p16.commitments[0] != cm[0] and not np.array_equal(p16.challenges[0], ch[0])
