@@ -366,21 +366,45 @@ cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_
 
 // Fold with a QM31 inverse-domain layer given as full QM31 values (the QM31 fold
 // plan API takes arbitrary QM31 inverse points, QM31FRIFold.swift:960-1338).
-__global__ void fold_qm31_inv_kernel(const uint4* __restrict__ prev, const uint4* __restrict__ inv, const uint32_t* __restrict__ chp, uint4* __restrict__ out,
-                                     uint64_t n_out) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_out) return;
-  qm31 ch = {__ldcg(chp), __ldcg(chp + 1), __ldcg(chp + 2), __ldcg(chp + 3)};
-  uint4 p = prev[2 * i], q = prev[2 * i + 1], t = inv[i];
-  qm31 pos = {p.x, p.y, p.z, p.w}, neg = {q.x, q.y, q.z, q.w};
-  qm31 odd = q_mul(q_sub(pos, neg), qm31{t.x, t.y, t.z, t.w});
-  qm31 r = q_half(q_add(q_add(pos, neg), q_mul(ch, odd)));
-  out[i] = make_uint4(r.a, r.b, r.c, r.d);
+// The challenge is read once per block into shared memory; a grid-stride loop
+// with two outputs per step keeps two sets of loads in flight per thread.
+__global__ void __launch_bounds__(256) fold_qm31_inv_kernel(const uint4* __restrict__ prev, const uint4* __restrict__ inv,
+                                                            const uint32_t* __restrict__ chp, uint4* __restrict__ out, uint64_t n_out) {
+  __shared__ uint32_t s_ch[4];
+  if (threadIdx.x < 4) s_ch[threadIdx.x] = __ldcg(chp + threadIdx.x);
+  __syncthreads();
+  const qm31 ch = {s_ch[0], s_ch[1], s_ch[2], s_ch[3]};
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out; i += 2 * stride) {
+    const uint64_t i2 = i + stride;
+    const bool two = i2 < n_out;
+    const uint4 p = __ldg(prev + 2 * i), q = __ldg(prev + 2 * i + 1), t = __ldg(inv + i);
+    uint4 p2 = p, q2 = q, t2 = t;
+    if (two) {
+      p2 = __ldg(prev + 2 * i2);
+      q2 = __ldg(prev + 2 * i2 + 1);
+      t2 = __ldg(inv + i2);
+    }
+    {
+      qm31 pos = {p.x, p.y, p.z, p.w}, neg = {q.x, q.y, q.z, q.w};
+      qm31 odd = q_mul(q_sub(pos, neg), qm31{t.x, t.y, t.z, t.w});
+      qm31 r = q_half(q_add(q_add(pos, neg), q_mul(ch, odd)));
+      out[i] = make_uint4(r.a, r.b, r.c, r.d);
+    }
+    if (two) {
+      qm31 pos = {p2.x, p2.y, p2.z, p2.w}, neg = {q2.x, q2.y, q2.z, q2.w};
+      qm31 odd = q_mul(q_sub(pos, neg), qm31{t2.x, t2.y, t2.z, t2.w});
+      qm31 r = q_half(q_add(q_add(pos, neg), q_mul(ch, odd)));
+      out[i2] = make_uint4(r.a, r.b, r.c, r.d);
+    }
+  }
 }
 
 cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s) {
   if (n_out == 0) return cudaSuccess;
-  fold_qm31_inv_kernel<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(prev, inv, ch, out, n_out);
+  uint64_t blocks = (n_out + 511) / 512;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  fold_qm31_inv_kernel<<<(unsigned)blocks, 256, 0, s>>>(prev, inv, ch, out, n_out);
   return cudaGetLastError();
 }
 

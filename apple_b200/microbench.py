@@ -112,6 +112,18 @@ def run(which, log_count, reps=5):
         hbm, kind = _hbm_peak()
         emit({"what": "qm31 fold (QM31 inverse points)", "count": n, "seconds": t, "hbm_gbs": 32 * n / t / 1e9, "frac_hbm": 32 * n / t / 1e9 / hbm,
               "peak_source": kind})
+        # Circle fold of one layer with M31 inverse twiddles: 16n read + 2n twiddle
+        # read + 8n write bytes (n inputs), as in the superstep's final folds
+        ts = []
+        chs = np.array([[11, 13, 17, 19]], np.uint32)
+        for _ in range(reps + 1):
+            st = azk.Stats()
+            azk._capi.check(azk.lib().azk_circle_fold_chain(ctx.handle, log_count, ev.ctypes.data, chs.ctypes.data, 1, res.ctypes.data,
+                                                            ctypes.byref(st)), ctx.handle)
+            ts.append(st.gpu_s)
+        t = statistics.median(ts[1:])
+        emit({"what": "circle fold, one layer (M31 inverse twiddles)", "count": n, "seconds": t, "hbm_gbs": 26 * n / t / 1e9,
+              "frac_hbm": 26 * n / t / 1e9 / hbm, "peak_source": kind})
     if "fft" in which:
         # Circle FFT stage of a batch of 16 log-22 instances (blowup 4): lifted M31
         # coefficients (one-limb path) and full QM31 coefficients
