@@ -14,21 +14,32 @@ namespace azk {
 static constexpr uint32_t kP = 2147483647u;
 static constexpr uint32_t kInv2 = 1073741824u;
 
+// s < 2p -> s mod p.  s - p is below s exactly when s >= p (otherwise it wraps
+// above it), so the reduction is an unsigned minimum: one subtract, one min.
+__host__ __device__ __forceinline__ uint32_t m31_reduce_once(uint32_t s) {
+  const uint32_t t = s - kP;
+  return t < s ? t : s;
+}
 __host__ __device__ __forceinline__ uint32_t m31_fold64(uint64_t v) {
   // v < 2^62: two Mersenne folds then one conditional subtraction
   uint64_t r = (v & kP) + (v >> 31);
   uint32_t s = (uint32_t)((r & kP) + (r >> 31));
   return s >= kP ? s - kP : s;
 }
-__host__ __device__ __forceinline__ uint32_t m31_add(uint32_t a, uint32_t b) {
-  uint32_t s = a + b;
-  return s >= kP ? s - kP : s;
-}
-__host__ __device__ __forceinline__ uint32_t m31_sub(uint32_t a, uint32_t b) { return a >= b ? a - b : a + kP - b; }
+// Inputs are at most p (canonical values, or p itself as a redundant zero).
+__host__ __device__ __forceinline__ uint32_t m31_add(uint32_t a, uint32_t b) { return m31_reduce_once(a + b); }
+// a + (p - b) lies in [0, 2p): one reduction, no branch on a >= b.
+__host__ __device__ __forceinline__ uint32_t m31_sub(uint32_t a, uint32_t b) { return m31_reduce_once(a + (kP - b)); }
 __host__ __device__ __forceinline__ uint32_t m31_neg(uint32_t a) { return a == 0 ? 0 : kP - a; }
-__host__ __device__ __forceinline__ uint32_t m31_mul(uint32_t a, uint32_t b) { return m31_fold64((uint64_t)a * (uint64_t)b); }
-// x * 2^-1 mod p: halve an even value, or (x + p) / 2 for an odd one.
-__host__ __device__ __forceinline__ uint32_t m31_half(uint32_t a) { return (a & 1u) ? (uint32_t)(((uint64_t)a + kP) >> 1) : (a >> 1); }
+// a, b <= p: the product is below 2^62 - 2^32 + 2, so one Mersenne fold of it in
+// 32-bit arithmetic, (v mod 2^31) + (v >> 31), is below 2p and one reduction
+// finishes it.
+__host__ __device__ __forceinline__ uint32_t m31_mul(uint32_t a, uint32_t b) {
+  const uint64_t v = (uint64_t)a * (uint64_t)b;
+  return m31_reduce_once(((uint32_t)v & kP) + (uint32_t)(v >> 31));
+}
+// x * 2^-1 mod p: halve an even value, or (x + p) / 2 = (x >> 1) + 2^30 for an odd one.
+__host__ __device__ __forceinline__ uint32_t m31_half(uint32_t a) { return (a >> 1) + ((a & 1u) << 30); }
 __host__ __device__ __forceinline__ uint32_t m31_pow(uint32_t b, uint32_t e) {
   uint32_t r = 1;
   while (e) {

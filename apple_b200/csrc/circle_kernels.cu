@@ -149,18 +149,23 @@ __global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __res
   uint32_t* sd = sc + TP;
   uint32_t* stw = sd + TP;
   fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
-    const uint64_t gi = fft_global_index(g, w.y, L);
-    uint4 v;
-    if (ft.first)
-      v = gi < ft.count ? __ldg(job.in + gi) : make_uint4(0u, 0u, 0u, 0u);
-    else
-      v = job.out[gi];
-    const uint32_t a = fpad(L);
-    sa[a] = v.x;
-    sb[a] = v.y;
-    sc[a] = v.z;
-    sd[a] = v.w;
+  // tile index L = threadIdx.x + k * THREADS: the global index advances by a constant
+  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
+  const uint64_t gi0 = fft_global_index(g, w.y, threadIdx.x);
+  {
+    uint64_t gi = gi0;
+    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
+      uint4 v;
+      if (ft.first)
+        v = gi < ft.count ? __ldg(job.in + gi) : make_uint4(0u, 0u, 0u, 0u);
+      else
+        v = job.out[gi];
+      const uint32_t a = fpad(L);
+      sa[a] = v.x;
+      sb[a] = v.y;
+      sc[a] = v.z;
+      sd[a] = v.w;
+    }
   }
   __syncthreads();
   int j = (int)g.m - 1;
@@ -169,12 +174,13 @@ __global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __res
     const uint32_t* tw_j = stw + fft_stw_offset(g.m, (uint32_t)j);
     const uint32_t* tw_j1 = stw + fft_stw_offset(g.m, (uint32_t)j - 1);
     const uint32_t lowmask = (1u << (p - 1)) - 1;
+    const uint32_t o1 = fpad(1u << (p - 1)), o2 = fpad(1u << p), o3 = fpad(3u << (p - 1));
     for (uint32_t k = threadIdx.x; k < T / 4; k += THREADS) {
       const uint32_t e0 = ((k & ~lowmask) << 2) | (k & lowmask);
       const uint32_t row = e0 >> g.c;
       const uint32_t t1 = tw_j[row >> (j + 1)];
       const uint32_t t2a = tw_j1[row >> j], t2b = tw_j1[(row >> j) | 1u];
-      const uint32_t a0 = fpad(e0), a1 = fpad(e0 | (1u << (p - 1))), a2 = fpad(e0 | (1u << p)), a3 = fpad(e0 | (3u << (p - 1)));
+      const uint32_t a0 = fpad(e0), a1 = a0 + o1, a2 = a0 + o2, a3 = a0 + o3;
       qm31 v0 = {sa[a0], sb[a0], sc[a0], sd[a0]}, v1 = {sa[a1], sb[a1], sc[a1], sd[a1]};
       qm31 v2 = {sa[a2], sb[a2], sc[a2], sd[a2]}, v3 = {sa[a3], sb[a3], sc[a3], sd[a3]};
       bfly_q(v0, v2, t1);
@@ -201,9 +207,12 @@ __global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __res
     }
     __syncthreads();
   }
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
-    const uint32_t a = fpad(L);
-    job.out[fft_global_index(g, w.y, L)] = make_uint4(sa[a], sb[a], sc[a], sd[a]);
+  {
+    uint64_t gi = gi0;
+    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
+      const uint32_t a = fpad(L);
+      job.out[gi] = make_uint4(sa[a], sb[a], sc[a], sd[a]);
+    }
   }
 }
 
@@ -224,14 +233,20 @@ __global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __r
   uint32_t* stw = sv + T + (T >> 5);
   fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
   const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
-    const uint64_t gi = fft_global_index(g, w.y, L);
-    uint32_t v;
-    if (ft.first)
-      v = gi < ft.count ? __ldg(in_a + 4 * gi) : 0u;
-    else
-      v = job.narrow[gi];
-    sv[fpad(L)] = v;
+  // tile index L = threadIdx.x + k * THREADS: the rows advance by THREADS >> c, so
+  // the global index advances by a constant
+  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
+  const uint64_t gi0 = fft_global_index(g, w.y, threadIdx.x);
+  {
+    uint64_t gi = gi0;
+    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
+      uint32_t v;
+      if (ft.first)
+        v = gi < ft.count ? __ldg(in_a + 4 * gi) : 0u;
+      else
+        v = job.narrow[gi];
+      sv[fpad(L)] = v;
+    }
   }
   __syncthreads();
   int j = (int)g.m - 1;
@@ -241,13 +256,19 @@ __global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __r
     const uint32_t* tw1 = stw + fft_stw_offset(g.m, (uint32_t)j - 1);
     const uint32_t* tw2 = stw + fft_stw_offset(g.m, (uint32_t)j - 2);
     const uint32_t lowmask = (1u << (p - 2)) - 1;
+    // the group's 8 indices are e0 with bits p, p-1, p-2 set per b; e0 has those
+    // bits clear, so fpad(e0 | o) = fpad(e0) + fpad(o)
+    uint32_t ob[8];
+#pragma unroll
+    for (uint32_t b = 0; b < 8; b++) ob[b] = fpad(((b >> 2) << p) | (((b >> 1) & 1u) << (p - 1)) | ((b & 1u) << (p - 2)));
     for (uint32_t k = threadIdx.x; k < T / 8; k += THREADS) {
       const uint32_t e0 = ((k & ~lowmask) << 3) | (k & lowmask);
       const uint32_t row = e0 >> g.c;
+      const uint32_t a0 = fpad(e0);
       uint32_t a[8], v[8];
 #pragma unroll
       for (uint32_t b = 0; b < 8; b++) {
-        a[b] = fpad(e0 | ((b >> 2) << p) | (((b >> 1) & 1u) << (p - 1)) | ((b & 1u) << (p - 2)));
+        a[b] = a0 + ob[b];
         v[b] = sv[a[b]];
       }
       const uint32_t t0 = tw0[row >> (j + 1)];
@@ -305,13 +326,15 @@ __global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __r
     }
     __syncthreads();
   }
-  for (uint32_t L = threadIdx.x; L < T; L += THREADS) {
-    const uint64_t gi = fft_global_index(g, w.y, L);
-    const uint32_t v = sv[fpad(L)];
-    if (ft.last)
-      job.out[gi] = make_uint4(v, 0u, 0u, 0u);
-    else
-      job.narrow[gi] = v;
+  {
+    uint64_t gi = gi0;
+    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
+      const uint32_t v = sv[fpad(L)];
+      if (ft.last)
+        job.out[gi] = make_uint4(v, 0u, 0u, 0u);
+      else
+        job.narrow[gi] = v;
+    }
   }
 }
 
