@@ -163,6 +163,14 @@ def profile_traffic():
         return {}
 
 
+def dist_backend() -> str:
+    """NCCL on GPU boxes; gloo where no CUDA device exists (the CPU tests of the
+    multi-rank path), or whatever AZK_DIST_BACKEND names."""
+    import torch
+
+    return os.environ.get("AZK_DIST_BACKEND") or ("nccl" if torch.cuda.is_available() else "gloo")
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -174,8 +182,10 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = dist_backend()
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local, dist
 
 
@@ -189,7 +199,8 @@ def max_over_ranks(dist, value: float, local: int) -> float:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
