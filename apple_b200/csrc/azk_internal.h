@@ -203,7 +203,10 @@ cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
 // of count_x / count_y monomial coefficients into 2n interleaved QM31.
 cudaError_t launch_witness_tables(uint64_t n, uint32_t* fact, uint32_t* seg, uint32_t* ifact, uint32_t* scale, cudaStream_t s);
 cudaError_t launch_witness_transform(const uint4* x, uint64_t count_x, const uint4* y, uint64_t count_y, uint64_t n, const uint32_t* ifact,
-                                     const uint32_t* scale, uint4* ax, uint4* ay, uint4* cx, uint4* cy, uint4* out, cudaStream_t s);
+                                     const uint32_t* scale, uint4* ax, uint4* ay, uint4* px, uint4* py, uint4* cx, uint4* cy, uint4* out,
+                                     cudaStream_t s);
+// QM31 values of each partial-sum buffer (px, py) the transform needs at capacity n.
+uint64_t witness_partial_values(uint64_t n);
 
 // `narrow`: the work items' inputs are lifted M31 polynomials (one-limb kernel).
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s);
@@ -211,6 +214,13 @@ cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t 
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
 // info = {1, 0, count} first).
 cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad, InputInfo* d_info, cudaStream_t s);
+// The same over many coefficient buffers in one launch.
+struct ScanJob {
+  const uint4* in;
+  uint64_t count;
+  InputInfo* info;
+};
+cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_count, uint32_t* d_bad, cudaStream_t s);
 cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s);
 cudaError_t launch_pcs_prefix(PcsInstance* d_inst, uint32_t ninst, cudaStream_t s);

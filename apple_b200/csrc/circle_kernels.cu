@@ -789,6 +789,31 @@ cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad
   return cudaGetLastError();
 }
 
+// One launch over many buffers: blockIdx.y picks the buffer (plus `base`), the
+// blocks along x stride through its coefficients.
+__global__ void scan_inputs_kernel(const ScanJob* __restrict__ jobs, uint32_t base, uint32_t* bad) {
+  const ScanJob j = jobs[base + blockIdx.y];
+  bool b = false, upper = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < j.count; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 v = j.in[i];
+    b |= v.x >= kP || v.y >= kP || v.z >= kP || v.w >= kP;
+    upper |= (v.y | v.z | v.w) != 0;
+  }
+  if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+  if (j.info && __any_sync(0xffffffffu, upper) && (threadIdx.x & 31) == 0) atomicAnd(&j.info->m31, 0u);
+}
+
+cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_count, uint32_t* d_bad, cudaStream_t s) {
+  if (!njobs || !max_count) return cudaSuccess;
+  uint64_t bx = (max_count + 255) / 256;
+  if (bx > 64) bx = 64;
+  for (uint32_t base = 0; base < njobs; base += 65535) {
+    const uint32_t ny = njobs - base < 65535 ? njobs - base : 65535;
+    scan_inputs_kernel<<<dim3((unsigned)bx, ny), 256, 0, s>>>(d_jobs, base, d_bad);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_check_canonical(const uint32_t* d_words, uint64_t nwords, uint32_t* d_flag, cudaStream_t s) {
   if (!nwords) return cudaSuccess;
   uint64_t blocks = (nwords + 255) / 256;

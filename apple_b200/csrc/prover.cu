@@ -59,6 +59,7 @@ struct Engine {
   uint32_t leaf_values = 1;  // all instances of an engine share the leaf size
   FftPlan fft;
   std::vector<FftJob> fft_transforms;
+  DevBuf d_scan;  // upload scan jobs, one per instance
   std::vector<uint8_t> fft_narrow;  // per instance: input known to be a lifted M31 polynomial
   // rounds: tree step k (kind QM31 at k == 0, fold+hash after), final folds at step k
   std::vector<TreeJob> tree_jobs;
@@ -135,7 +136,15 @@ struct Engine {
     for (size_t i = 0; i < cfg.size(); i++) h[i] = InputInfo{1u, 0u, counts[i]};
     AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s));
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
-    for (size_t i = 0; i < cfg.size(); i++) AZK_CU(launch_scan_input(arena.at<uint4>(off_input[i]), counts[i], d_flag(), d_info() + i, s));
+    std::vector<ScanJob> jobs(cfg.size());
+    uint64_t max_count = 0;
+    for (size_t i = 0; i < cfg.size(); i++) {
+      jobs[i] = ScanJob{arena.at<uint4>(off_input[i]), counts[i], d_info() + i};
+      max_count = std::max(max_count, counts[i]);
+    }
+    if (!d_scan.p) d_scan.alloc(sizeof(ScanJob) * cfg.size(), "PCS.ScanJobs");
+    AZK_CU(cudaMemcpyAsync(d_scan.p, jobs.data(), sizeof(ScanJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    AZK_CU(launch_scan_inputs(d_scan.as<ScanJob>(), (uint32_t)jobs.size(), max_count, d_flag(), s));
     uint32_t f = 0;
     AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
     AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s));

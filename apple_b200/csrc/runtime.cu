@@ -795,7 +795,7 @@ struct azk_witness_plan {
   cudaStream_t s = nullptr;
   uint32_t logn;
   uint64_t n;  // coefficient capacity = half the domain
-  DevBuf fact, seg, ifact, scale, ax, ay, cx, cy, xin, yin, out, flag;
+  DevBuf fact, seg, ifact, scale, ax, ay, px, py, cx, cy, xin, yin, out, flag;
   ~azk_witness_plan() {
     if (s) cudaStreamDestroy(s);
   }
@@ -812,7 +812,7 @@ static void witness_run(azk_witness_plan* p, const uint4* x, uint64_t nx, const 
   layout(bad == 0, "witness coefficients contain a non-canonical field element");
   GpuTimer g(p->s);
   AZK_CU(launch_witness_transform(x, nx, y, ny, p->n, p->ifact.as<uint32_t>(), p->scale.as<uint32_t>(), p->ax.as<uint4>(), p->ay.as<uint4>(),
-                                  p->cx.as<uint4>(), p->cy.as<uint4>(), out, p->s));
+                                  p->px.as<uint4>(), p->py.as<uint4>(), p->cx.as<uint4>(), p->cy.as<uint4>(), out, p->s));
   g.stop();
   fill_stats(st, t, 0, g.seconds());
 }
@@ -834,6 +834,8 @@ azk_status azk_witness_plan_create(azk_ctx* ctx, uint32_t log_size, azk_witness_
     p->ifact.alloc(4 * n, "Witness.InverseFactorials");
     p->scale.alloc(4 * n, "Witness.Scale");
     for (DevBuf* b : {&p->ax, &p->ay, &p->cx, &p->cy, &p->xin, &p->yin}) b->alloc(16 * n, "Witness.Scratch");
+    p->px.alloc(16 * witness_partial_values(n), "Witness.PartialSums");
+    p->py.alloc(16 * witness_partial_values(n), "Witness.PartialSums");
     p->out.alloc(32 * n, "Witness.Output");
     p->flag.alloc(16, "Witness.Flag");
     AZK_CU(launch_witness_tables(n, p->fact.as<uint32_t>(), p->seg.as<uint32_t>(), p->ifact.as<uint32_t>(), p->scale.as<uint32_t>(), p->s));

@@ -91,13 +91,15 @@ __global__ void witness_scale_kernel(const uint4* __restrict__ col, uint64_t cou
 
 // Chebyshev coefficients of both columns: one output index m per thread, the
 // sum over j in chunks whose table entries and scaled coefficients are staged in
-// shared memory.
+// shared memory.  blockIdx.y takes a slice of the j range (so short outputs still
+// fill the GPU) and writes its partial sums; chebyshev_sum_kernel adds the slices.
 static constexpr uint32_t kChebM = 256;  // outputs per block
 static constexpr uint32_t kChebJ = 256;  // terms per chunk
+static constexpr uint32_t kWitnessBlockTarget = 296;  // two blocks per SM
 
 __global__ void __launch_bounds__(kChebM) chebyshev_kernel(const uint4* __restrict__ ax, const uint4* __restrict__ ay, uint64_t count,
-                                                          const uint32_t* __restrict__ ifact, uint4* __restrict__ cx, uint4* __restrict__ cy,
-                                                          uint64_t capacity) {
+                                                          const uint32_t* __restrict__ ifact, uint4* __restrict__ px, uint4* __restrict__ py,
+                                                          uint64_t capacity, uint64_t chunks_per_slice) {
   __shared__ uint32_t s_ij[kChebJ];            // ifact[j0 + t]
   __shared__ uint32_t s_imj[kChebM + kChebJ];  // ifact[m0 + j0 + t]
   __shared__ uint4 s_ax[kChebM + 2 * kChebJ];  // a[m0 + 2 j0 + t]
@@ -107,7 +109,10 @@ __global__ void __launch_bounds__(kChebM) chebyshev_kernel(const uint4* __restri
   qm31 sx = {0, 0, 0, 0}, sy = {0, 0, 0, 0};
   // terms need m + 2j < count: j < (count - m0 + 1) / 2 for the block's first m
   const uint64_t jend = count > m0 ? (count - m0 + 1) / 2 : 0;
-  for (uint64_t j0 = 0; j0 < jend; j0 += kChebJ) {
+  const uint64_t jlo = (uint64_t)blockIdx.y * chunks_per_slice * kChebJ;
+  const uint64_t jhi_slice = jlo + chunks_per_slice * kChebJ;
+  const uint64_t jhi = jhi_slice < jend ? jhi_slice : jend;
+  for (uint64_t j0 = jlo; j0 < jhi; j0 += kChebJ) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < kChebJ; t += kChebM) s_ij[t] = j0 + t < capacity ? ifact[j0 + t] : 0u;
     for (uint32_t t = threadIdx.x; t < kChebM + kChebJ; t += kChebM) {
@@ -132,6 +137,22 @@ __global__ void __launch_bounds__(kChebM) chebyshev_kernel(const uint4* __restri
     }
   }
   if (m >= capacity) return;
+  const uint64_t o = (uint64_t)blockIdx.y * capacity + m;
+  px[o] = make_uint4(sx.a, sx.b, sx.c, sx.d);
+  py[o] = make_uint4(sy.a, sy.b, sy.c, sy.d);
+}
+
+// c_m = sum of the slices' partial sums, halved for m = 0.
+__global__ void chebyshev_sum_kernel(const uint4* __restrict__ px, const uint4* __restrict__ py, uint32_t slices, uint4* __restrict__ cx,
+                                     uint4* __restrict__ cy, uint64_t capacity) {
+  const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= capacity) return;
+  qm31 sx = {0, 0, 0, 0}, sy = {0, 0, 0, 0};
+  for (uint32_t y = 0; y < slices; y++) {
+    const uint4 vx = px[(uint64_t)y * capacity + m], vy = py[(uint64_t)y * capacity + m];
+    sx = q_add(sx, qm31{vx.x, vx.y, vx.z, vx.w});
+    sy = q_add(sy, qm31{vy.x, vy.y, vy.z, vy.w});
+  }
   if (m == 0) {
     sx = q_mul_m31(sx, kInv2);
     sy = q_mul_m31(sy, kInv2);
@@ -199,14 +220,35 @@ cudaError_t launch_witness_tables(uint64_t n, uint32_t* fact, uint32_t* seg, uin
   return cudaGetLastError();
 }
 
+// Slices of the j range so that the Chebyshev launch has about two blocks per SM
+// (at least one chunk of kChebJ terms per slice).
+static uint32_t chebyshev_slices(uint64_t n, uint64_t count) {
+  const uint64_t mblocks = (n + kChebM - 1) / kChebM;
+  const uint64_t chunks = ((count + 1) / 2 + kChebJ - 1) / kChebJ;
+  uint64_t y = (kWitnessBlockTarget + mblocks - 1) / mblocks;
+  if (y > chunks) y = chunks;
+  return (uint32_t)(y ? y : 1);
+}
+
+uint64_t witness_partial_values(uint64_t n) {
+  // slices * n <= (kWitnessBlockTarget / mblocks + 1) * n <= kWitnessBlockTarget * kChebM + n
+  return (uint64_t)kWitnessBlockTarget * kChebM + n;
+}
+
 // x, y: count_x / count_y monomial coefficients (QM31); capacity n = half the
-// domain; out: 2n QM31.  ax, ay, cx, cy: n QM31 each of scratch.
+// domain; out: 2n QM31.  ax, ay, cx, cy: n QM31 each of scratch; px, py:
+// witness_partial_values(n) QM31 each.
 cudaError_t launch_witness_transform(const uint4* x, uint64_t count_x, const uint4* y, uint64_t count_y, uint64_t n, const uint32_t* ifact,
-                                     const uint32_t* scale, uint4* ax, uint4* ay, uint4* cx, uint4* cy, uint4* out, cudaStream_t s) {
+                                     const uint32_t* scale, uint4* ax, uint4* ay, uint4* px, uint4* py, uint4* cx, uint4* cy, uint4* out,
+                                     cudaStream_t s) {
   const uint64_t count = count_x > count_y ? count_x : count_y;
   witness_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, count_x, scale, ax, n);
   witness_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(y, count_y, scale, ay, n);
-  chebyshev_kernel<<<(unsigned)((n + kChebM - 1) / kChebM), kChebM, 0, s>>>(ax, ay, count, ifact, cx, cy, n);
+  const uint32_t slices = chebyshev_slices(n, count);
+  const uint64_t chunks = ((count + 1) / 2 + kChebJ - 1) / kChebJ;
+  const uint64_t per_slice = (chunks + slices - 1) / slices;
+  chebyshev_kernel<<<dim3((unsigned)((n + kChebM - 1) / kChebM), slices), kChebM, 0, s>>>(ax, ay, count, ifact, px, py, n, per_slice ? per_slice : 1);
+  chebyshev_sum_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(px, py, slices, cx, cy, n);
   for (uint64_t sz = n; sz > kLineTile; sz >>= 1) {
     const uint64_t pairs = (n / sz) * ((sz >> 1) - 1);
     line_level_kernel<<<(unsigned)((pairs + 255) / 256), 256, 0, s>>>(cx, n, sz);
