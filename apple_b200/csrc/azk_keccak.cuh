@@ -93,7 +93,58 @@ __host__ __device__ __forceinline__ void rho_pi_all(const uint64_t (&a)[25], con
   (rho_pi_lane<Is>(a, d, b), ...);
 }
 
+#if defined(__CUDA_ARCH__)
+// Three-input logic on the 32-bit halves as single LOP3 instructions (truth
+// tables over inputs a = 0xF0, b = 0xCC, c = 0xAA): 0x96 = a ^ b ^ c,
+// 0xD2 = a ^ (~b & c).  Written out so that theta's column terms are folded into
+// each lane's XOR (one LOP3 per half) instead of being combined first and XORed
+// in afterwards (two), which is the 180-operation round the roofline counts.
+__device__ __forceinline__ uint32_t lop3_xor3(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+__device__ __forceinline__ uint32_t lop3_chi(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0xD2;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+__device__ __forceinline__ uint64_t xor3_64(uint64_t a, uint64_t b, uint64_t c) {
+  return ((uint64_t)lop3_xor3((uint32_t)(a >> 32), (uint32_t)(b >> 32), (uint32_t)(c >> 32)) << 32) |
+         lop3_xor3((uint32_t)a, (uint32_t)b, (uint32_t)c);
+}
+__device__ __forceinline__ uint64_t chi_64(uint64_t a, uint64_t b, uint64_t c) {
+  return ((uint64_t)lop3_chi((uint32_t)(a >> 32), (uint32_t)(b >> 32), (uint32_t)(c >> 32)) << 32) |
+         lop3_chi((uint32_t)a, (uint32_t)b, (uint32_t)c);
+}
+
+// rho-pi of lane I after theta: a[I] ^ C[x-1] ^ rotl1(C[x+1]) in one three-input XOR
+template <int I>
+__device__ __forceinline__ void rho_pi_lane3(const uint64_t (&a)[25], const uint64_t (&c)[5], const uint64_t (&r1)[5], uint64_t (&b)[25]) {
+  constexpr int x = I % 5;
+  b[RhoPi<I>::dst] = rotl<RhoPi<I>::rho>(xor3_64(a[I], c[(x + 4) % 5], r1[(x + 1) % 5]));
+}
+template <int... Is>
+__device__ __forceinline__ void rho_pi_all3(const uint64_t (&a)[25], const uint64_t (&c)[5], const uint64_t (&r1)[5], uint64_t (&b)[25], LaneSeq<Is...>) {
+  (rho_pi_lane3<Is>(a, c, r1, b), ...);
+}
+#endif
+
 __host__ __device__ __forceinline__ void keccak_round(uint64_t (&a)[25], uint64_t rc) {
+#if defined(__CUDA_ARCH__)
+  uint64_t c[5], r1[5], b[25];
+#pragma unroll
+  for (int x = 0; x < 5; x++) c[x] = xor3_64(xor3_64(a[x], a[x + 5], a[x + 10]), a[x + 15], a[x + 20]);
+#pragma unroll
+  for (int x = 0; x < 5; x++) r1[x] = rotl<1>(c[x]);
+  rho_pi_all3(a, c, r1, b, LaneSeq<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24>{});
+#pragma unroll
+  for (int y = 0; y < 25; y += 5) {
+#pragma unroll
+    for (int x = 0; x < 5; x++) a[y + x] = chi_64(b[y + x], b[y + (x + 1) % 5], b[y + (x + 2) % 5]);
+  }
+  a[0] ^= rc;
+#else
   uint64_t c[5], d[5], b[25];
 #pragma unroll
   for (int x = 0; x < 5; x++) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
@@ -106,6 +157,7 @@ __host__ __device__ __forceinline__ void keccak_round(uint64_t (&a)[25], uint64_
     for (int x = 0; x < 5; x++) a[y + x] = b[y + x] ^ (~b[y + (x + 1) % 5] & b[y + (x + 2) % 5]);
   }
   a[0] ^= rc;
+#endif
 }
 
 // Full 24-round permutation.  UNROLL rounds per loop iteration (a tuning knob:
