@@ -7,7 +7,17 @@ no CPU fallback.
 """
 from __future__ import annotations
 
-from ._capi import (  # noqa: F401
+import os as _os
+
+# Every plan, batch and server worker runs on its own CUDA stream.  With the
+# driver's default of 8 hardware work queues, streams share queues and work on one
+# waits behind another's whole CUDA graph (a prover's upload stalls until another
+# prover's superstep ends).  The queue count is read when CUDA initialises in the
+# process, so it is set here, at import, before torch or anything else starts
+# CUDA; a value the caller set is kept.
+_os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+from ._capi import (  # noqa: E402,F401
     AZK_STATUS_NAMES,
     AZKError,
     Schedule,
@@ -15,7 +25,7 @@ from ._capi import (  # noqa: F401
     lib,
     library_path,
 )
-from .plans import (  # noqa: F401
+from .plans import (  # noqa: E402,F401
     BatchProver,
     CircleCodewordPlan,
     CirclePCSFRIProver,

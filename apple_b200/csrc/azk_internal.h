@@ -214,13 +214,15 @@ cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t 
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
 // info = {1, 0, count} first).
 cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad, InputInfo* d_info, cudaStream_t s);
-// The same over many coefficient buffers in one launch.
+// The same over many coefficient buffers in one launch, which also writes zeros
+// over each buffer's tail [count, n) (the coefficients past the uploaded prefix).
 struct ScanJob {
-  const uint4* in;
+  uint4* in;
   uint64_t count;
+  uint64_t n;
   InputInfo* info;
 };
-cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_count, uint32_t* d_bad, cudaStream_t s);
+cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_n, uint32_t* d_bad, cudaStream_t s);
 cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s);
 cudaError_t launch_pcs_prefix(PcsInstance* d_inst, uint32_t ninst, cudaStream_t s);

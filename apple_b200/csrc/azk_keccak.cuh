@@ -93,7 +93,6 @@ __host__ __device__ __forceinline__ void rho_pi_all(const uint64_t (&a)[25], con
   (rho_pi_lane<Is>(a, d, b), ...);
 }
 
-#if defined(__CUDA_ARCH__)
 // Three-input logic on the 32-bit halves as single LOP3 instructions (truth
 // tables over inputs a = 0xF0, b = 0xCC, c = 0xAA): 0x96 = a ^ b ^ c,
 // 0xD2 = a ^ (~b & c).  Written out so that theta's column terms are folded into
@@ -128,7 +127,6 @@ template <int... Is>
 __device__ __forceinline__ void rho_pi_all3(const uint64_t (&a)[25], const uint64_t (&c)[5], const uint64_t (&r1)[5], uint64_t (&b)[25], LaneSeq<Is...>) {
   (rho_pi_lane3<Is>(a, c, r1, b), ...);
 }
-#endif
 
 __host__ __device__ __forceinline__ void keccak_round(uint64_t (&a)[25], uint64_t rc) {
 #if defined(__CUDA_ARCH__)

@@ -790,22 +790,28 @@ cudaError_t launch_scan_input(const uint4* d_in, uint64_t count, uint32_t* d_bad
 }
 
 // One launch over many buffers: blockIdx.y picks the buffer (plus `base`), the
-// blocks along x stride through its coefficients.
+// blocks along x stride through its coefficients, checking [0, count) and
+// writing zeros over [count, n).  One launch instead of a memset per buffer
+// matters when another prover's superstep holds the GPU: every separate small
+// launch waits for free SM slots between that superstep's large launches.
 __global__ void scan_inputs_kernel(const ScanJob* __restrict__ jobs, uint32_t base, uint32_t* bad) {
   const ScanJob j = jobs[base + blockIdx.y];
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool b = false, upper = false;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < j.count; i += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t i = i0; i < j.count; i += stride) {
     uint4 v = j.in[i];
     b |= v.x >= kP || v.y >= kP || v.z >= kP || v.w >= kP;
     upper |= (v.y | v.z | v.w) != 0;
   }
+  for (uint64_t i = j.count + i0; i < j.n; i += stride) j.in[i] = make_uint4(0u, 0u, 0u, 0u);
   if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
   if (j.info && __any_sync(0xffffffffu, upper) && (threadIdx.x & 31) == 0) atomicAnd(&j.info->m31, 0u);
 }
 
-cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_count, uint32_t* d_bad, cudaStream_t s) {
-  if (!njobs || !max_count) return cudaSuccess;
-  uint64_t bx = (max_count + 255) / 256;
+cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_n, uint32_t* d_bad, cudaStream_t s) {
+  if (!njobs || !max_n) return cudaSuccess;
+  uint64_t bx = (max_n + 255) / 256;
   if (bx > 64) bx = 64;
   for (uint32_t base = 0; base < njobs; base += 65535) {
     const uint32_t ny = njobs - base < 65535 ? njobs - base : 65535;

@@ -8,6 +8,7 @@
 // still active in that round, so small instances share the GPU with large ones
 // and the whole superstep is a fixed launch sequence captured in a CUDA graph.
 // Plain form: the same kernels, launched instance after instance.
+#include <memory>
 #include <algorithm>
 #include <condition_variable>
 #include <deque>
@@ -43,6 +44,10 @@ struct InstanceCfg {
 struct Engine {
   azk_ctx* ctx = nullptr;
   cudaStream_t s = nullptr;
+  // Uploads (input copies and the scan launch) run on a high-priority stream: their
+  // one launch takes the first free SM slots instead of queueing behind another
+  // prover's superstep, so one prover uploads while another proves.
+  cudaStream_t s_up = nullptr;
   Sched sched;
   std::vector<InstanceCfg> cfg;
   uint32_t rmax = 0, qmax = 0;
@@ -92,6 +97,7 @@ struct Engine {
     for (auto e : ev_a) cudaEventDestroy(e);
     for (auto e : ev_b) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
+    if (s_up) cudaStreamDestroy(s_up);
   }
 
   // Event pair for the next profiled region (created up front, outside capture).
@@ -131,24 +137,28 @@ struct Engine {
   // Canonicality gate over the staged coefficients of every instance (counts[i]
   // leading QM31 values; the rest are zero) and the FFT's input description:
   // which instances are lifted M31 polynomials, how many coefficients are nonzero.
+  // Gate and describe the uploaded coefficients (the caller queued their copies
+  // on s_up): canonicality, the lifted-M31 flag and zeros over each tail
+  // [counts[i], N) in one launch on s_up, then one small readback.
   void scan_inputs(const std::vector<uint64_t>& counts) {
     std::vector<InputInfo> h(cfg.size());
     for (size_t i = 0; i < cfg.size(); i++) h[i] = InputInfo{1u, 0u, counts[i]};
-    AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s));
-    AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
+    AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s_up));
+    AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s_up));
     std::vector<ScanJob> jobs(cfg.size());
-    uint64_t max_count = 0;
+    uint64_t max_n = 0;
     for (size_t i = 0; i < cfg.size(); i++) {
-      jobs[i] = ScanJob{arena.at<uint4>(off_input[i]), counts[i], d_info() + i};
-      max_count = std::max(max_count, counts[i]);
+      const uint64_t N = 1ull << cfg[i].logn;
+      jobs[i] = ScanJob{arena.at<uint4>(off_input[i]), counts[i], N, d_info() + i};
+      max_n = std::max(max_n, N);
     }
     if (!d_scan.p) d_scan.alloc(sizeof(ScanJob) * cfg.size(), "PCS.ScanJobs");
-    AZK_CU(cudaMemcpyAsync(d_scan.p, jobs.data(), sizeof(ScanJob) * jobs.size(), cudaMemcpyHostToDevice, s));
-    AZK_CU(launch_scan_inputs(d_scan.as<ScanJob>(), (uint32_t)jobs.size(), max_count, d_flag(), s));
+    AZK_CU(cudaMemcpyAsync(d_scan.p, jobs.data(), sizeof(ScanJob) * jobs.size(), cudaMemcpyHostToDevice, s_up));
+    AZK_CU(launch_scan_inputs(d_scan.as<ScanJob>(), (uint32_t)jobs.size(), max_n, d_flag(), s_up));
     uint32_t f = 0;
-    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
-    AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s));
-    sync_stream(s);
+    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s_up));
+    AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s_up));
+    sync_stream(s_up);
     layout(f == 0, "input contains a non-canonical field element");
     std::vector<uint8_t> narrow(cfg.size());
     for (size_t i = 0; i < cfg.size(); i++) narrow[i] = h[i].m31 ? 1 : 0;
@@ -180,6 +190,9 @@ struct Engine {
     cfg = cf;
     AZK_CU(cudaSetDevice(ctx->device));
     AZK_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int prio_lo = 0, prio_hi = 0;
+    AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    AZK_CU(cudaStreamCreateWithPriority(&s_up, cudaStreamNonBlocking, prio_hi));
     size_t n = cfg.size();
     leaf_values = cfg.empty() ? 1 : cfg[0].leaf_values;
     for (auto& i : cfg) {
@@ -622,8 +635,7 @@ azk_status azk_pcs_prover_prove_coefficients(azk_pcs_prover* p, const uint32_t* 
     pcs_ensure_claimed(p, {});
     Engine& e = p->eng;
     uint4* in = e.arena.at<uint4>(e.off_input[0]);
-    AZK_CU(cudaMemcpyAsync(in, coeffs, 16 * count, cudaMemcpyHostToDevice, e.s));
-    if (count < N) AZK_CU(cudaMemsetAsync(in + count, 0, 16 * (N - count), e.s));
+    AZK_CU(cudaMemcpyAsync(in, coeffs, 16 * count, cudaMemcpyHostToDevice, e.s_up));
     e.scan_inputs({count});
     pcs_prove_common(p, true, pub, proof_out, false, proof_len, st, t);
   });
@@ -640,11 +652,13 @@ azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* din, uin
     Engine& e = p->eng;
     const uint8_t* src = static_cast<const uint8_t*>(din) + in_off;
     void* dst = is_coeffs ? (void*)e.arena.at<uint4>(e.off_input[0]) : (void*)e.h_inst[0].layers;
-    AZK_CU(cudaMemcpyAsync(dst, src, 16 * N, cudaMemcpyDeviceToDevice, e.s));
-    if (is_coeffs)
+    if (is_coeffs) {
+      AZK_CU(cudaMemcpyAsync(dst, src, 16 * N, cudaMemcpyDeviceToDevice, e.s_up));
       e.scan_inputs({N});
-    else
+    } else {
+      AZK_CU(cudaMemcpyAsync(dst, src, 16 * N, cudaMemcpyDeviceToDevice, e.s));
       e.check_input_canonical(dst, 4 * N);
+    }
     pcs_prove_common(p, is_coeffs != 0, pub, static_cast<uint8_t*>(dproof), true, proof_len, st, t);
   });
 }
@@ -730,8 +744,7 @@ azk_status azk_batch_upload(azk_batch* b, const uint32_t* host, const uint64_t* 
       uint64_t N = 1ull << e.cfg[i].logn;
       layout(counts[i] >= 1 && counts[i] <= N);
       uint4* in = e.arena.at<uint4>(e.off_input[i]);
-      AZK_CU(cudaMemcpyAsync(in, host + 4 * offsets[i], 16 * counts[i], cudaMemcpyHostToDevice, e.s));
-      if (counts[i] < N) AZK_CU(cudaMemsetAsync(in + counts[i], 0, 16 * (N - counts[i]), e.s));
+      AZK_CU(cudaMemcpyAsync(in, host + 4 * offsets[i], 16 * counts[i], cudaMemcpyHostToDevice, e.s_up));
     }
     // every staged word must be canonical (QM31CanonicalityCheck.swift:11-117)
     e.scan_inputs(std::vector<uint64_t>(counts, counts + e.cfg.size()));
@@ -931,13 +944,11 @@ void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st) {
     r.eng->init(sv->ctx, {InstanceCfg{j.logn, j.rounds, j.queries, j.log_blowup, 0, {}}}, sc);
   }
   Engine* e = r.eng.get();
-  uint64_t N = 1ull << j.logn;
   const uint64_t in_bytes = 16 * j.count, proof = e->proof_len[0];
   uint8_t* pin = st.ensure(std::max<uint64_t>(in_bytes, proof) + 64);
   std::memcpy(pin, j.input.data(), in_bytes);
   uint4* in = e->arena.at<uint4>(e->off_input[0]);
-  AZK_CU(cudaMemcpyAsync(in, pin, in_bytes, cudaMemcpyHostToDevice, e->s));
-  if (j.count < N) AZK_CU(cudaMemsetAsync(in + j.count, 0, 16 * (N - j.count), e->s));
+  AZK_CU(cudaMemcpyAsync(in, pin, in_bytes, cudaMemcpyHostToDevice, e->s_up));
   e->scan_inputs({j.count});
   e->set_publics(j.pub);
   Timer t;
@@ -953,7 +964,7 @@ void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st) {
 // `evals` and `pin` (>= 4n + sizeof(SumcheckOut) + 12 log n bytes) may be the same
 // page-locked buffer: the evaluations are consumed by the upload before the
 // results land.
-std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s, uint8_t* pin) {
+std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s, uint8_t* pin, double* gpu_s = nullptr) {
   const uint64_t n = 1ull << logn;
   if (!b.ev.p) {
     b.ev.alloc(4 * n, "Sumcheck.Evals");
@@ -970,10 +981,14 @@ std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint3
   ptrs.challenges = ptrs.r1 + logn;
   *h = ptrs;
   AZK_CU(cudaMemcpyAsync(b.out.p, h, sizeof(SumcheckOut), cudaMemcpyHostToDevice, s));
+  std::unique_ptr<GpuTimer> gt;
+  if (gpu_s) gt.reset(new GpuTimer(s));  // the two kernels, digest and rounds
   AZK_CU(launch_sumcheck(b.ev.as<uint32_t>(), logn, b.scratch.as<uint32_t>(), b.out.as<SumcheckOut>(), s));
+  if (gt) gt->stop();
   AZK_CU(cudaMemcpyAsync(h, b.out.p, sizeof(SumcheckOut), cudaMemcpyDeviceToHost, s));
   AZK_CU(cudaMemcpyAsync(rounds_h, b.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, s));
   sync_stream(s);
+  if (gt) *gpu_s = gt->seconds();
   const SumcheckOut r = *h;
   std::vector<uint32_t> rounds(rounds_h, rounds_h + 3 * logn);
   std::vector<uint32_t> words = {r.claimed_sum, r.final_eval};
@@ -1125,14 +1140,15 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evals, uint64_t coun
     Staging staging;
     uint8_t* pin = staging.ensure(sumcheck_pinned_bytes(logn));
     std::memcpy(pin, evals, 4ull << logn);
-    std::vector<uint32_t> w = sumcheck_run(b, reinterpret_cast<const uint32_t*>(pin), logn, ctx->stream, pin);
+    double gpu_s = 0.0;
+    std::vector<uint32_t> w = sumcheck_run(b, reinterpret_cast<const uint32_t*>(pin), logn, ctx->stream, pin, &gpu_s);
     *claimed_sum = w[0];
     *final_eval = w[1];
     std::memcpy(digest, w.data() + 2, 32);
     std::memcpy(sums0, w.data() + 10, 4ull * logn);
     std::memcpy(sums1, w.data() + 10 + logn, 4ull * logn);
     std::memcpy(challenges, w.data() + 10 + 2 * logn, 4ull * logn);
-    fill_stats(st, t, 0, 0.0);
+    fill_stats(st, t, 0, gpu_s);
   });
 }
 

@@ -11,6 +11,7 @@ L2).  Keccak rates are compared with the device's measured LOP3+SHF issue rate
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import statistics
 
@@ -95,7 +96,6 @@ def run(which, log_count, reps=5):
     if "fold" in which:
         # QM31 fold of 2^log values with QM31 inverse points: 16n read + 8n inverse
         # read + 8n write bytes (n inputs), one launch
-        import ctypes
 
         ev = np.zeros((n, 4), np.uint32)
         ev[:] = rng.integers(0, 2**31 - 1, size=ev.shape, dtype=np.uint32)
@@ -148,6 +148,23 @@ def run(which, log_count, reps=5):
             emit({"what": f"circle fft 16 x log 22, {label} coefficients", "seconds": t, "elems_per_s": N / t, "hbm_gbs": alg / t / 1e9,
                   "frac_hbm": alg / t / 1e9 / hbm, "algorithmic": "16N read + 16N write + 4N twiddles", "peak_source": kind})
             del b
+    if "sumcheck" in which:
+        # M31 multilinear sum-check over 2^20 evaluations: the statement digest (one
+        # sequential SHA3 sponge over the 4 MiB table, 30,841 permutations) and the
+        # 20 rounds, device time of the two kernels
+        ev = rng.integers(0, 2**31 - 1, size=1 << 20, dtype=np.uint32)
+        ts = []
+        for _ in range(reps + 1):
+            st = azk.Stats()
+            r0, r1, ch = (np.zeros(20, np.uint32) for _ in range(3))
+            cs, fe, dg = ctypes.c_uint32(), ctypes.c_uint32(), np.zeros(32, np.uint8)
+            azk._capi.check(azk.lib().azk_sumcheck_prove(ctx.handle, ev.ctypes.data, len(ev), r0.ctypes.data, r1.ctypes.data, ch.ctypes.data,
+                                                         ctypes.byref(cs), ctypes.byref(fe), dg.ctypes.data, ctypes.byref(st)), ctx.handle)
+            ts.append(st.gpu_s)
+        t = statistics.median(ts[1:])
+        perms = (50 + 4 * len(ev)) // 136 + 1
+        emit({"what": "m31 multilinear sum-check 2^20 (digest + 20 rounds)", "seconds": t, "digest_permutations": perms,
+              "us_per_permutation": t / perms * 1e6})
     ctx.close()
     return out
 
@@ -165,7 +182,7 @@ def _hbm_peak():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--which", default="perm,sha3,merkle,prove,fold,fft")
+    ap.add_argument("--which", default="perm,sha3,merkle,prove,fold,fft,sumcheck")
     ap.add_argument("--log", type=int, default=24)
     ap.add_argument("--reps", type=int, default=5)
     a = ap.parse_args()
