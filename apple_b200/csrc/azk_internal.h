@@ -209,7 +209,8 @@ cudaError_t launch_witness_transform(const uint4* x, uint64_t count_x, const uin
 uint64_t witness_partial_values(uint64_t n);
 
 // `narrow`: the work items' inputs are lifted M31 polynomials (one-limb kernel).
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s);
+// `last`: the items are the low-stage (last) passes of their transforms.
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, bool last, cudaStream_t s);
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
 // info = {1, 0, count} first).

@@ -93,6 +93,7 @@ struct FftTile {
   uint32_t T;
   uint64_t count;
   bool first, last;
+  bool top_zero;  // first pass over a nonzero prefix of at most N/4 (see fft_m31_tile_stages)
 };
 
 __device__ __forceinline__ FftTile fft_tile(const FftJob& job) {
@@ -103,6 +104,7 @@ __device__ __forceinline__ FftTile fft_tile(const FftJob& job) {
   t.count = (job.info != nullptr && job.info->count != 0) ? job.info->count : N;
   t.first = job.pass == 0;
   t.last = job.pass == fft_high_chunks(job.logn);
+  t.top_zero = t.first && job.logn >= 2 && t.count <= (N >> 2);
   return t;
 }
 
@@ -221,35 +223,54 @@ __global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __res
 // a limbs of the nonzero prefix, passes exchange one word per element through
 // `narrow`, and the last pass writes the QM31 codeword (a, 0, 0, 0).  Three stages
 // per shared-memory round trip (radix 8 in registers).
+// The stages of one one-limb tile (2^m rows x 2^c columns, values in `sv` with one
+// pad word per 32, stage twiddles in `stw`), three per shared-memory round trip.
+// Starts after and ends with a __syncthreads.  `top_zero`: the tile holds the
+// transform's two top stages and every value whose row has either of the two top
+// bits set is zero (a first pass whose nonzero prefix is at most N/4, as at blowup
+// 4).  Those two stages then only copy (l + 0 t, l - 0 t), so the first round trip
+// reads 2 of its 8 values and runs 4 of its 12 butterflies.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
-  extern __shared__ uint32_t nsm[];
-  const uint2 w = work[blockIdx.x];
-  const FftJob& job = jobs[w.x];
-  const FftTile ft = fft_tile(job);
-  const FftPassGeom& g = ft.g;
-  const uint32_t T = ft.T;
-  uint32_t* sv = nsm;
-  uint32_t* stw = sv + T + (T >> 5);
-  fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
-  const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
-  // tile index L = threadIdx.x + k * THREADS: the rows advance by THREADS >> c, so
-  // the global index advances by a constant
-  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
-  const uint64_t gi0 = fft_global_index(g, w.y, threadIdx.x);
-  {
-    uint64_t gi = gi0;
-    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
-      uint32_t v;
-      if (ft.first)
-        v = gi < ft.count ? __ldg(in_a + 4 * gi) : 0u;
-      else
-        v = job.narrow[gi];
-      sv[fpad(L)] = v;
-    }
-  }
-  __syncthreads();
+__device__ __forceinline__ void fft_m31_tile_stages(uint32_t* sv, const uint32_t* stw, const FftPassGeom& g, uint32_t T, bool top_zero) {
   int j = (int)g.m - 1;
+  if (top_zero && j >= 2) {
+    const uint32_t p = (uint32_t)j + g.c;
+    const uint32_t* tw2 = stw + fft_stw_offset(g.m, (uint32_t)j - 2);
+    const uint32_t lowmask = (1u << (p - 2)) - 1;
+    uint32_t ob[8];
+#pragma unroll
+    for (uint32_t b = 0; b < 8; b++) ob[b] = fpad(((b >> 2) << p) | (((b >> 1) & 1u) << (p - 1)) | ((b & 1u) << (p - 2)));
+    for (uint32_t k = threadIdx.x; k < T / 8; k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << 3) | (k & lowmask);
+      const uint32_t row = e0 >> g.c;
+      const uint32_t a0 = fpad(e0);
+      const uint32_t x0 = sv[a0], x1 = sv[a0 + ob[1]];
+      const uint32_t r2 = row >> (j - 1);
+#pragma unroll
+      for (uint32_t q = 0; q < 4; q++) {
+        // after the two copying stages the pair (2q, 2q + 1) holds (x0, x1)
+        uint32_t l = x0, r = x1;
+        bfly_m31(l, r, tw2[r2 | q]);
+        sv[a0 + ob[2 * q]] = l;
+        sv[a0 + ob[2 * q + 1]] = r;
+      }
+    }
+    __syncthreads();
+    j -= 3;
+  } else if (top_zero && j >= 0) {
+    // one or two stages, both copying: every value of a group takes its live one
+    const uint32_t p = (uint32_t)j + g.c;
+    const uint32_t span = 1u << (p - (uint32_t)j);  // the live row's stride: the group is {e0 + span * b}
+    const uint32_t bits = (uint32_t)j + 1;
+    const uint32_t lowmask = span - 1;
+    for (uint32_t k = threadIdx.x; k < (T >> bits); k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << bits) | (k & lowmask);
+      const uint32_t x = sv[fpad(e0)];
+      for (uint32_t b = 1; b < (1u << bits); b++) sv[fpad(e0 + span * b)] = x;
+    }
+    __syncthreads();
+    return;
+  }
   for (; j >= 2; j -= 3) {
     const uint32_t p = (uint32_t)j + g.c;  // stages j, j-1, j-2 pair bits p, p-1, p-2
     const uint32_t* tw0 = stw + fft_stw_offset(g.m, (uint32_t)j);
@@ -326,6 +347,37 @@ __global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __r
     }
     __syncthreads();
   }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) fft_pass_m31_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  extern __shared__ uint32_t nsm[];
+  const uint2 w = work[blockIdx.x];
+  const FftJob& job = jobs[w.x];
+  const FftTile ft = fft_tile(job);
+  const FftPassGeom& g = ft.g;
+  const uint32_t T = ft.T;
+  uint32_t* sv = nsm;
+  uint32_t* stw = sv + T + (T >> 5);
+  fft_stage_twiddles<THREADS>(job, ft, w.y, stw);
+  const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
+  // tile index L = threadIdx.x + k * THREADS: the rows advance by THREADS >> c, so
+  // the global index advances by a constant
+  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
+  const uint64_t gi0 = fft_global_index(g, w.y, threadIdx.x);
+  {
+    uint64_t gi = gi0;
+    for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
+      uint32_t v;
+      if (ft.first)
+        v = gi < ft.count ? __ldg(in_a + 4 * gi) : 0u;
+      else
+        v = job.narrow[gi];
+      sv[fpad(L)] = v;
+    }
+  }
+  __syncthreads();
+  fft_m31_tile_stages<THREADS>(sv, stw, g, T, ft.top_zero);
   {
     uint64_t gi = gi0;
     for (uint32_t L = threadIdx.x; L < T; L += THREADS, gi += gstep) {
@@ -346,18 +398,111 @@ static constexpr size_t kFftSmemM31 = (size_t)4 * (kFftTilePadded + kFftTileMax)
 static constexpr int kFftThreadsQ = 512;
 static constexpr int kFftThreadsM31 = 256;
 
+// Low-stage (last) passes of one-limb transforms, persistent: each CTA walks the
+// work list with a stride of the grid and prefetches its next tile's values and
+// stage twiddles into a second pair of shared buffers with cp.async while it
+// computes the current tile, so the loads run under the butterflies instead of
+// stalling every warp before them (16 x log 22: 2.36 -> 2.82 TB/s for the whole
+// transform).  The high-stage passes are bound by instruction issue instead; there
+// the double buffers' smaller occupancy (3 instead of 5 CTAs per SM) measured
+// slower (2.56 TB/s), so they keep fft_pass_m31_kernel.
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const void* src, uint32_t src_bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int THREADS>
+__device__ __forceinline__ void fft_m31_prefetch(const FftJob* __restrict__ jobs, uint2 w, uint32_t* sv, uint32_t* stw) {
+  const FftJob& job = jobs[w.x];
+  const FftTile ft = fft_tile(job);
+  const FftPassGeom& g = ft.g;
+  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
+  uint64_t gi = fft_global_index(g, w.y, threadIdx.x);
+  if (ft.first) {
+    // the a limbs of the nonzero prefix, zeros past it
+    const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
+    for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) {
+      const bool live = gi < ft.count;
+      cp_async4(sv + fpad(L), in_a + 4 * (live ? gi : 0), live ? 4u : 0u);
+    }
+  } else {
+    for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) cp_async4(sv + fpad(L), job.narrow + gi, 4u);
+  }
+  // stage j's 2^(m-1-j) twiddles of this tile sit at stw + 2^m - 2^(m-j): entry q
+  // belongs to the stage j with 2^(m-1-j) <= 2^m - 1 - q < 2^(m-j)
+  const uint32_t M = 1u << g.m;
+  const uint32_t midbits = g.s_lo > g.c ? g.s_lo - g.c : 0;
+  const uint64_t hi = (uint64_t)w.y >> midbits;
+  for (uint32_t q = threadIdx.x; q + 1 < M; q += THREADS) {
+    const uint32_t j = g.m - 1 - (31 - __clz(M - 1 - q));
+    const uint32_t r = q - (M - (M >> j));
+    cp_async4(stw + q, job.tw + tw_offset(job.logn, g.s_lo + j) + (hi << (g.m - 1 - j)) + r, 4u);
+  }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) fft_m31_persistent_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work, uint32_t nwork) {
+  extern __shared__ uint32_t lsm[];
+  constexpr uint32_t kBuf = kFftTilePadded + kFftTileMax;  // values (padded) + twiddles
+  uint32_t item = blockIdx.x;
+  if (item >= nwork) return;
+  fft_m31_prefetch<THREADS>(jobs, work[item], lsm, lsm + kFftTilePadded);
+  cp_async_commit();
+  for (uint32_t b = 0; item < nwork; item += gridDim.x, b ^= 1u) {
+    const uint32_t next = item + gridDim.x;
+    uint32_t* nbuf = lsm + (b ^ 1u) * kBuf;
+    if (next < nwork) fft_m31_prefetch<THREADS>(jobs, work[next], nbuf, nbuf + kFftTilePadded);
+    cp_async_commit();
+    cp_async_wait_one();  // this thread's copies of the current tile have landed
+    __syncthreads();      // ... and every other thread's
+    const uint2 w = work[item];
+    const FftJob& job = jobs[w.x];
+    const FftTile ft = fft_tile(job);
+    uint32_t* sv = lsm + b * kBuf;
+    fft_m31_tile_stages<THREADS>(sv, sv + kFftTilePadded, ft.g, ft.T, ft.top_zero);
+    const uint64_t gstep = (uint64_t)(THREADS >> ft.g.c) << ft.g.s_lo;
+    uint64_t gi = fft_global_index(ft.g, w.y, threadIdx.x);
+    if (ft.last) {
+      for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) job.out[gi] = make_uint4(sv[fpad(L)], 0u, 0u, 0u);
+    } else {
+      for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) job.narrow[gi] = sv[fpad(L)];
+    }
+    __syncthreads();  // the next iteration prefetches into this buffer
+  }
+}
+
+static constexpr size_t kFftSmemPersistent = 2 * kFftSmemM31;  // two buffers of values + twiddles
+static uint32_t g_fft_m31_grid = 0;                            // resident CTAs of the persistent kernel
+
 cudaError_t prepare_fft_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fft_pass_q_kernel<kFftThreadsQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemQ);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(fft_pass_m31_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemM31);
+  e = cudaFuncSetAttribute(fft_pass_m31_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemM31);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fft_m31_persistent_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemPersistent);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_m31_persistent_kernel<kFftThreadsM31>, kFftThreadsM31, kFftSmemPersistent)) !=
+      cudaSuccess)
+    return e;
+  g_fft_m31_grid = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
+  return cudaSuccess;
 }
 
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, cudaStream_t s) {
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, bool last, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
-  if (narrow)
+  if (narrow && last) {
+    const uint32_t grid = g_fft_m31_grid && g_fft_m31_grid < nwork ? g_fft_m31_grid : nwork;
+    fft_m31_persistent_kernel<kFftThreadsM31><<<grid, kFftThreadsM31, kFftSmemPersistent, s>>>(d_jobs, d_work, nwork);
+  } else if (narrow) {
     fft_pass_m31_kernel<kFftThreadsM31><<<nwork, kFftThreadsM31, kFftSmemM31, s>>>(d_jobs, d_work);
-  else
+  } else {
     fft_pass_q_kernel<kFftThreadsQ><<<nwork, kFftThreadsQ, kFftSmemQ, s>>>(d_jobs, d_work);
+  }
   return cudaGetLastError();
 }
 

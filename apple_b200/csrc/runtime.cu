@@ -103,13 +103,16 @@ void FftPlan::upload(cudaStream_t s) {
   if (!jobs.empty()) AZK_CU(cudaMemcpyAsync(d_jobs.p, jobs.data(), jobs.size() * sizeof(FftJob), cudaMemcpyHostToDevice, s));
   if (!work.empty()) AZK_CU(cudaMemcpyAsync(d_work.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
 }
+// Steps are aligned at the end: the last step holds every transform's low-stage pass.
 void FftPlan::launch_step(size_t step, cudaStream_t s) const {
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + step_off[step], (uint32_t)step_cnt[step], false, s));
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + nstep_off[step], (uint32_t)nstep_cnt[step], true, s));
+  const bool last = step + 1 == step_cnt.size();
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + step_off[step], (uint32_t)step_cnt[step], false, last, s));
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + nstep_off[step], (uint32_t)nstep_cnt[step], true, last, s));
 }
 void FftPlan::launch_step_for(size_t step, size_t t, cudaStream_t s) const {
   auto r = inst_range[step][t];
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, narrow[t] != 0, s));
+  const bool last = step + 1 == step_cnt.size();
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, narrow[t] != 0, last, s));
 }
 
 // ---------------------------------------------------------------------------

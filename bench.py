@@ -327,14 +327,16 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
     sat_jobs_s = len(mix) / t_sat
     sat_elems_s = sat_elems / t_sat
 
-    def poisson(lam, seconds, seed, window_only=False):
+    def poisson(lam, seconds, seed, steady_after=0.0):
         """Submit Poisson arrivals at `lam` jobs/s for `seconds`; returns the job ids,
-        submission lags and the completions counted while submitting."""
+        submission lags and the completion rate counted from `steady_after` seconds
+        into the run to its end."""
         n = max(50, int(lam * seconds))
         jobs = serving_mix(n, seed)
         gaps = -np.log1p(-((splitmix64(seed ^ 0x9A, n) >> np.uint64(11)).astype(np.float64) / float(1 << 53))) / lam
         arrivals = np.cumsum(gaps)
         ids, lags = [], []
+        mark = None
         c0 = server.stats()["completed"]
         t0 = time.perf_counter()
         for i, (job, at) in enumerate(zip(jobs, arrivals)):
@@ -344,16 +346,19 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
                     break
                 if at - now > 2e-3:
                     time.sleep(at - now - 1e-3)
+            if mark is None and now >= steady_after:
+                mark = (server.stats()["completed"], time.perf_counter())
             ids.append(submit(job, i))
             lags.append(time.perf_counter() - t0 - at)
-        window = time.perf_counter() - t0
-        done_in_window = server.stats()["completed"] - c0
-        return jobs, ids, lags, done_in_window / window, t0
+        c1, t1 = server.stats()["completed"], time.perf_counter()
+        if mark is None:
+            mark = (c0, t0)
+        return jobs, ids, lags, (c1 - mark[0]) / (t1 - mark[1]), t0
 
     # sustained rate: arrivals above what the backlog suggests, completions counted
-    # while the queue stays full (a backlog of simultaneous jobs reads higher than
-    # what the mix sustains under continuous arrivals)
-    _, over_ids, _, sustained, _ = poisson(1.5 * sat_jobs_s, 2.0, SEED ^ 0x0F)
+    # once the queue has been full for a second (a backlog of simultaneous jobs
+    # reads higher than what the mix sustains under continuous arrivals)
+    _, over_ids, _, sustained, _ = poisson(1.5 * sat_jobs_s, 3.0, SEED ^ 0x0F, steady_after=1.0)
     collect(over_ids)
 
     # Poisson arrivals
@@ -377,7 +382,7 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
         "saturated": {"jobs_per_s": sat_jobs_s, "elems_per_s": sat_elems_s, "jobs": args.serve_backlog, "seconds": t_sat},
         "arrival_rate_jobs_per_s": lam,
         "sustained_jobs_per_s": sustained,
-        "arrival_rule": f"{args.serve_load} x sustained jobs/s (completions under arrivals at 1.5 x the backlog rate)" if args.serve_rate <= 0
+        "arrival_rule": f"{args.serve_load} x sustained jobs/s (completions in seconds 1-3 of arrivals at 1.5 x the backlog rate)" if args.serve_rate <= 0
         else "fixed",
         "batched_superstep_jobs_per_s": batched_jobs_per_s,
         "throughput_elems_per_s": (s1["pcs_elements"] - s0["pcs_elements"]) / t_run, "jobs_per_s": len(mix) / t_run,
