@@ -48,6 +48,7 @@ struct Engine {
   // one launch takes the first free SM slots instead of queueing behind another
   // prover's superstep, so one prover uploads while another proves.
   cudaStream_t s_up = nullptr;
+  bool owns_streams = true;
   Sched sched;
   std::vector<InstanceCfg> cfg;
   uint32_t rmax = 0, qmax = 0;
@@ -96,8 +97,8 @@ struct Engine {
     if (graph) cudaGraphExecDestroy(graph);
     for (auto e : ev_a) cudaEventDestroy(e);
     for (auto e : ev_b) cudaEventDestroy(e);
-    if (s) cudaStreamDestroy(s);
-    if (s_up) cudaStreamDestroy(s_up);
+    if (owns_streams && s) cudaStreamDestroy(s);
+    if (owns_streams && s_up) cudaStreamDestroy(s_up);
   }
 
   // Event pair for the next profiled region (created up front, outside capture).
@@ -184,15 +185,24 @@ struct Engine {
     graph = nullptr;
   }
 
-  void init(azk_ctx* c, const std::vector<InstanceCfg>& cf, const Sched& sc) {
+  // `run_stream` / `upload_stream`: streams owned by the caller (a server worker,
+  // whose engines never run at the same time), else the engine creates its own.
+  void init(azk_ctx* c, const std::vector<InstanceCfg>& cf, const Sched& sc, cudaStream_t run_stream = nullptr,
+            cudaStream_t upload_stream = nullptr) {
     ctx = c;
     sched = sc;
     cfg = cf;
     AZK_CU(cudaSetDevice(ctx->device));
-    AZK_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    int prio_lo = 0, prio_hi = 0;
-    AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    AZK_CU(cudaStreamCreateWithPriority(&s_up, cudaStreamNonBlocking, prio_hi));
+    if (run_stream && upload_stream) {
+      s = run_stream;
+      s_up = upload_stream;
+      owns_streams = false;
+    } else {
+      AZK_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      int prio_lo = 0, prio_hi = 0;
+      AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+      AZK_CU(cudaStreamCreateWithPriority(&s_up, cudaStreamNonBlocking, prio_hi));
+    }
     size_t n = cfg.size();
     leaf_values = cfg.empty() ? 1 : cfg[0].leaf_values;
     for (auto& i : cfg) {
@@ -856,6 +866,7 @@ struct ServeJob {
   uint32_t logn = 0, rounds = 0, queries = 0, log_blowup = 0;
   std::vector<uint32_t> input;  // pcs: coefficient words; sumcheck: evaluations
   uint64_t count = 0;           // pcs: coefficient count
+  bool zeros = false;           // warm-up job: `count` zero coefficients, no `input`
   uint8_t pub[32] = {0};
   uint64_t bytes = 0;  // device memory of its shape
   std::chrono::steady_clock::time_point submitted, started, finished;
@@ -906,6 +917,11 @@ struct azk_server {
   uint64_t tick = 0;
   bool stop = false;
   std::vector<std::map<ShapeKey, Resident>> cache;  // per worker
+  // per worker: jobs of zeros it runs once before serving (azk_server_warm), so its
+  // engines, sum-check buffers and pinned staging exist before the first real job
+  std::vector<std::deque<std::shared_ptr<ServeJob>>> warm;
+  uint64_t warm_pending = 0;
+  std::vector<cudaStream_t> streams;  // one per worker
   std::vector<std::thread> workers;
   uint64_t completed = 0, elems = 0;
   std::chrono::steady_clock::time_point first_submit, last_finish;
@@ -936,17 +952,20 @@ struct Staging {
   }
 };
 
-void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st) {
+void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st, cudaStream_t s) {
   if (!r.eng) {
     r.eng = std::make_unique<Engine>();
     Sched sc = sv->sched;
     sc.graph = false;
-    r.eng->init(sv->ctx, {InstanceCfg{j.logn, j.rounds, j.queries, j.log_blowup, 0, {}}}, sc);
+    r.eng->init(sv->ctx, {InstanceCfg{j.logn, j.rounds, j.queries, j.log_blowup, 0, {}}}, sc, s, s);
   }
   Engine* e = r.eng.get();
   const uint64_t in_bytes = 16 * j.count, proof = e->proof_len[0];
   uint8_t* pin = st.ensure(std::max<uint64_t>(in_bytes, proof) + 64);
-  std::memcpy(pin, j.input.data(), in_bytes);
+  if (j.zeros)
+    std::memset(pin, 0, in_bytes);
+  else
+    std::memcpy(pin, j.input.data(), in_bytes);
   uint4* in = e->arena.at<uint4>(e->off_input[0]);
   AZK_CU(cudaMemcpyAsync(in, pin, in_bytes, cudaMemcpyHostToDevice, e->s_up));
   e->scan_inputs({j.count});
@@ -1016,6 +1035,27 @@ void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j, Staging& st) {
 // recently used shapes when that makes room.  Nothing is taken while the job
 // cannot fit; a job larger than the budget never enters the queue.
 std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
+  // this worker's warm-up jobs first; one that cannot fit the budget is dropped
+  while (!sv->warm[w].empty()) {
+    auto j = sv->warm[w].front();
+    auto& cache = sv->cache[w];
+    ShapeKey key = shape_of(*j);
+    if (!cache.count(key)) {
+      if (sv->held + j->bytes > sv->budget) {
+        sv->warm[w].pop_front();
+        sv->warm_pending--;
+        sv->done_cv.notify_all();
+        continue;
+      }
+      Resident& r = cache[key];
+      r.bytes = j->bytes;
+      sv->held += j->bytes;
+    }
+    cache[key].last_use = ++sv->tick;
+    sv->warm[w].pop_front();
+    j->state = 1;
+    return j;
+  }
   if (sv->queue.empty()) return nullptr;
   auto& cache = sv->cache[w];
   const auto& j = sv->queue.front();
@@ -1044,12 +1084,10 @@ std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
 
 void worker_loop(azk_server* sv, int w) {
   cudaSetDevice(sv->ctx->device);
-  // sum-check jobs are one long chain of dependent permutations: their stream gets
-  // the device's highest priority, so their blocks are placed first
-  int prio_lo = 0, prio_hi = 0;
-  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
-  cudaStream_t s = nullptr;
-  cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio_hi);
+  // everything this worker runs (uploads, proof kernels, sum-checks) goes on its one
+  // stream: its jobs run one at a time, and one stream per worker keeps each worker
+  // on its own hardware work queue (see azk_server_create)
+  cudaStream_t s = sv->streams[w];
   Staging staging;
   for (;;) {
     std::shared_ptr<ServeJob> job;
@@ -1057,7 +1095,7 @@ void worker_loop(azk_server* sv, int w) {
     {
       std::unique_lock<std::mutex> lk(sv->mu);
       for (;;) {
-        if (sv->stop && sv->queue.empty()) break;
+        if (sv->stop && sv->queue.empty() && sv->warm[w].empty()) break;
         job = try_take(sv, w);
         if (job) break;
         sv->cv.wait(lk);
@@ -1065,21 +1103,39 @@ void worker_loop(azk_server* sv, int w) {
       if (!job) break;
       res = &sv->cache[w][shape_of(*job)];
     }
+    // the outcome is published under the lock together with the finish time, so a
+    // poll never sees a finished job without its latency
+    int outcome = 2;
+    std::string error;
     try {
       if (job->kind == 0)
-        run_pcs(sv, *res, *job, staging);
+        run_pcs(sv, *res, *job, staging, s);
       else
         run_sumcheck(*res, s, *job, staging);
-      job->state = 2;
     } catch (const Error& e) {
-      job->error = e.msg;
-      job->state = 3;
+      error = e.msg;
+      outcome = 3;
     } catch (const std::exception& e) {
-      job->error = e.what();
-      job->state = 3;
+      error = e.what();
+      outcome = 3;
     }
     {
       std::lock_guard<std::mutex> lk(sv->mu);
+      job->error = error;
+      job->state = outcome;
+      if (job->id == 0) {  // a warm-up job: not a result anyone polls
+        if (job->state == 3) {
+          auto it = sv->cache[w].find(shape_of(*job));
+          if (it != sv->cache[w].end()) {
+            sv->held -= it->second.bytes;
+            sv->cache[w].erase(it);
+          }
+        }
+        sv->warm_pending--;
+        sv->cv.notify_all();
+        sv->done_cv.notify_all();
+        continue;
+      }
       job->finished = std::chrono::steady_clock::now();
       job->input.clear();
       job->input.shrink_to_fit();
@@ -1103,7 +1159,6 @@ void worker_loop(azk_server* sv, int w) {
     for (auto& kv : sv->cache[w]) sv->held -= kv.second.bytes;
     sv->cache[w].clear();
   }
-  if (s) cudaStreamDestroy(s);
 }
 
 uint64_t submit(azk_server* sv, std::shared_ptr<ServeJob> j) {
@@ -1164,6 +1219,18 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     sv->budget = hbm_budget_bytes;
     sv->slots = slots;
     sv->cache.resize(slots);
+    sv->warm.resize(slots);
+    // The workers' streams are created here, one after another, so that with up to
+    // CUDA_DEVICE_MAX_CONNECTIONS (32) workers each lands on its own hardware work
+    // queue.  Streams that share a queue wait on each other's dependent launches:
+    // a sum-check's 64 ms digest followed by its rounds kernel then stalls every
+    // stream behind it (measured with two streams per cached engine, ~800 streams:
+    // completions stopped for up to a second at a time).  Highest priority: a
+    // sum-check digest or a job's input scan takes the first free SM slot.
+    int prio_lo = 0, prio_hi = 0;
+    AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    sv->streams.assign(slots, nullptr);
+    for (uint32_t w = 0; w < slots; w++) AZK_CU(cudaStreamCreateWithPriority(&sv->streams[w], cudaStreamNonBlocking, prio_hi));
     for (uint32_t w = 0; w < slots; w++) sv->workers.emplace_back(worker_loop, sv.get(), (int)w);
     *out = sv.release();
   });
@@ -1187,6 +1254,45 @@ azk_status azk_server_submit_pcs(azk_server* sv, uint32_t logn, uint32_t log_blo
     std::memcpy(j->pub, pub, 32);
     j->bytes = pcs_shape_bytes(logn, rounds, queries);
     *job_id = submit(sv, j);
+  });
+}
+
+azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint32_t* pcs_rounds, uint32_t n_pcs, uint32_t log_blowup,
+                           uint32_t queries, const uint32_t* sumcheck_logn, uint32_t n_sumcheck) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv && (n_pcs == 0 || (pcs_logn && pcs_rounds)) && (n_sumcheck == 0 || sumcheck_logn));
+    for (uint32_t i = 0; i < n_pcs; i++) validate_params(pcs_logn[i], log_blowup, queries, 0, pcs_rounds[i]);
+    for (uint32_t i = 0; i < n_sumcheck; i++) layout(sumcheck_logn[i] >= 1 && sumcheck_logn[i] <= 28);
+    std::unique_lock<std::mutex> lk(sv->mu);
+    for (uint32_t w = 0; w < sv->slots; w++) {
+      for (uint32_t i = 0; i < n_pcs; i++) {
+        auto j = std::make_shared<ServeJob>();  // id 0: a warm-up job
+        j->kind = 0;
+        j->logn = pcs_logn[i];
+        j->rounds = pcs_rounds[i];
+        j->queries = queries;
+        j->log_blowup = log_blowup;
+        // all 2^logn coefficients (zeros): the worker's pinned staging grows to the
+        // largest input of the shape now, not in the middle of serving, where
+        // freeing the smaller buffer would wait for the whole device
+        j->zeros = true;
+        j->count = 1ull << j->logn;
+        j->bytes = pcs_shape_bytes(j->logn, j->rounds, j->queries);
+        sv->warm[w].push_back(j);
+        sv->warm_pending++;
+      }
+      for (uint32_t i = 0; i < n_sumcheck; i++) {
+        auto j = std::make_shared<ServeJob>();
+        j->kind = 1;
+        j->logn = sumcheck_logn[i];
+        j->input.assign(1ull << j->logn, 0u);
+        j->bytes = sumcheck_shape_bytes(j->logn);
+        sv->warm[w].push_back(j);
+        sv->warm_pending++;
+      }
+    }
+    sv->cv.notify_all();
+    sv->done_cv.wait(lk, [&] { return sv->warm_pending == 0; });
   });
 }
 
@@ -1264,6 +1370,8 @@ void azk_server_destroy(azk_server* sv) {
   }
   sv->cv.notify_all();
   for (auto& t : sv->workers) t.join();
+  for (auto st : sv->streams)
+    if (st) cudaStreamDestroy(st);
   delete sv;
 }
 

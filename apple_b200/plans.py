@@ -564,6 +564,17 @@ class ProofServer:
         self._kind[jid.value] = 0
         return jid.value
 
+    def warm(self, pcs_shapes=(), log_blowup: int = 2, queries: int = 64, sumcheck_logs=()):
+        """Run, on every worker, one job of zeros of each shape before serving:
+        `pcs_shapes` = [(log_size, rounds), ...], `sumcheck_logs` = [log2(count), ...].
+        Afterwards no real job pays for creating its worker's device memory or
+        pinned staging.  Shapes over the HBM budget are skipped."""
+        logs = np.array([int(a) for a, _ in pcs_shapes], np.uint32)
+        rounds = np.array([int(b) for _, b in pcs_shapes], np.uint32)
+        sc = np.array([int(x) for x in sumcheck_logs], np.uint32)
+        self._check(lib().azk_server_warm(self._h, _ptr(logs) if len(logs) else None, _ptr(rounds) if len(rounds) else None, len(logs),
+                                          log_blowup, queries, _ptr(sc) if len(sc) else None, len(sc)))
+
     def submit_sumcheck(self, evaluations) -> int:
         ev = np.ascontiguousarray(evaluations, dtype=np.uint32).reshape(-1)
         jid = ctypes.c_uint64()

@@ -281,9 +281,9 @@ def serving_mix(n_jobs, seed, lo=12, hi=22, sumcheck_every=5):
 def run_serving(azk, ctx, args, batched_jobs_per_s):
     """Continuous-batching server on the serving mix.  A backlog and an overloaded
     Poisson run give the server's throughput on this mix; Poisson arrivals at
-    `--serve-load` of the sustained rate give p50/p99 latency (completion - arrival).  The batched superstep's jobs/s (the
-    512-instance leg, larger jobs on average) is reported beside it.  Every job's
-    bytes are those of the same job alone (tests/test_gpu_server.py)."""
+    `--serve-load` x the batched superstep's jobs/s (the 512-instance leg) give
+    p50/p99 latency (completion - arrival).  Every job's bytes are those of the same
+    job alone (tests/test_gpu_server.py)."""
     final_log, queries, blowup = args.final_log, 64, 2
     rng_rows = {k: None for k in range(12, 23)}
     for k in rng_rows:
@@ -305,14 +305,11 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
         server.wait_all()
         return [server.poll(j) for j in ids]
 
-    # warm every worker's resident shapes: one burst of `slots` jobs per shape
+    # every worker builds its device memory and pinned staging for every shape of
+    # the mix before the timed runs, then a short stretch of the mix itself
     t0 = time.perf_counter()
-    warm = []
-    for k in range(12, 23):
-        warm += [submit(("pcs", k), i) for i in range(args.serve_slots)]
-        collect(warm)
-        warm = []
-    collect([submit(("sc", 20), i) for i in range(args.serve_slots)])
+    server.warm(pcs_shapes=[(k, k - final_log) for k in range(12, 23)], log_blowup=blowup, queries=queries, sumcheck_logs=[20])
+    collect([submit(j, i) for i, j in enumerate(serving_mix(4 * args.serve_slots, SEED ^ 0x3B))])
     t_warm = time.perf_counter() - t0
 
     # saturated backlog: the server's throughput on this mix
@@ -361,8 +358,9 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
     _, over_ids, _, sustained, _ = poisson(1.5 * sat_jobs_s, 3.0, SEED ^ 0x0F, steady_after=1.0)
     collect(over_ids)
 
-    # Poisson arrivals
-    lam = args.serve_rate if args.serve_rate > 0 else args.serve_load * sustained
+    # Poisson arrivals at `serve_load` x the batched superstep's jobs/s (the mix's
+    # sustained rate is reported beside it, so the load it puts on the server shows)
+    lam = args.serve_rate if args.serve_rate > 0 else args.serve_load * batched_jobs_per_s
     s0 = server.stats()
     mix, ids, lags, _, t0 = poisson(lam, args.serve_seconds, SEED ^ 0xA7)
     res = collect(ids)
@@ -382,8 +380,9 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
         "saturated": {"jobs_per_s": sat_jobs_s, "elems_per_s": sat_elems_s, "jobs": args.serve_backlog, "seconds": t_sat},
         "arrival_rate_jobs_per_s": lam,
         "sustained_jobs_per_s": sustained,
-        "arrival_rule": f"{args.serve_load} x sustained jobs/s (completions in seconds 1-3 of arrivals at 1.5 x the backlog rate)" if args.serve_rate <= 0
-        else "fixed",
+        "arrival_rule": f"{args.serve_load} x the batched superstep's jobs/s" if args.serve_rate <= 0 else "fixed",
+        "sustained_rule": "completions in seconds 1-3 of arrivals at 1.5 x the backlog rate",
+        "load_vs_sustained": lam / sustained if sustained > 0 else None,
         "batched_superstep_jobs_per_s": batched_jobs_per_s,
         "throughput_elems_per_s": (s1["pcs_elements"] - s0["pcs_elements"]) / t_run, "jobs_per_s": len(mix) / t_run,
         "latency_all": pct(lat), "latency_pcs": pct(lat[kinds == "pcs"]), "latency_sumcheck": pct(lat[kinds == "sc"]),

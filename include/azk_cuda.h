@@ -299,6 +299,15 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evaluations, uint64_
  * entry points (each job's kernels are the same; only their overlap differs). */
 typedef struct azk_server azk_server;
 azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t slots, const azk_schedule* schedule, azk_server** out);
+/* Before serving: every worker runs, once, a job of zeros of each listed shape (PCS
+ * proofs of 2^pcs_logn[i] coefficients folded for pcs_rounds[i] rounds; sum-checks
+ * over 2^sumcheck_logn[i] evaluations), so its device memory for those shapes, its
+ * pinned staging and every lazily built table exist before the first real job:
+ * creating them in the middle of serving costs allocations and frees that wait for
+ * the whole device.  Shapes that do not fit the HBM budget are skipped.  Returns
+ * when all workers are done; warm-up jobs produce no results. */
+azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint32_t* pcs_rounds, uint32_t n_pcs, uint32_t log_blowup,
+                           uint32_t queries, const uint32_t* sumcheck_logn, uint32_t n_sumcheck);
 /* Circle PCS proof from `count` leading FFT-basis coefficients (rest zero). */
 azk_status azk_server_submit_pcs(azk_server* sv, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t rounds, const uint32_t* coefficients,
                                  uint64_t count, const uint8_t public_digest[32], uint64_t* job_id);

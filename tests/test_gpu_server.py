@@ -105,3 +105,27 @@ def test_bad_jobs_are_refused_at_submission(ctx):
     with pytest.raises(azk.AZKError):
         server.submit_pcs(10, 2, 8, 4, np.full((4, 4), P, np.uint32), bytes(32))
     server.close()
+
+
+def test_warm_then_jobs_match_alone(ctx):
+    """Warm-up runs a job of zeros per shape on every worker and leaves no result
+    behind; jobs of those shapes afterwards give the bytes the same job gives alone,
+    and a shape over the budget is skipped rather than refused."""
+    rng = np.random.default_rng(0x3A)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=256 << 20, slots=3)
+    server.warm(pcs_shapes=[(12, 8), (14, 8), (24, 8)], log_blowup=2, queries=32, sumcheck_logs=[12])
+    st = server.stats()
+    assert st["completed"] == 0
+    assert 0 < st["held_bytes"] <= 256 << 20
+    jobs = [_pcs_job(rng, 12), _pcs_job(rng, 14), _pcs_job(rng, 12)]
+    ev = rng.integers(0, P, 1 << 12, dtype=np.uint32)
+    ids = [server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]) for j in jobs]
+    sid = server.submit_sumcheck(ev)
+    res = _wait(server, ids + [sid])
+    assert server.stats()["completed"] == 4
+    server.close()
+    for j, i in zip(jobs, ids):
+        assert res[i][0] == azk.CirclePCSFRIProver(ctx, j["log_size"], 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])
+    alone = azk.sumcheck_prove(ctx, ev)
+    assert res[sid][0]["initial_digest"] == alone["initial_digest"]
+    assert np.array_equal(res[sid][0]["challenges"], alone["challenges"])
