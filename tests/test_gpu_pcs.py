@@ -191,6 +191,34 @@ def test_lifted_m31_coefficients_match_oracle(ctx, oracle, log_size, count_log, 
     assert proof == oracle.prove(log_size, oracle.fft_evaluate(log_size, full), 2, 8, pub, rounds).proof
 
 
+@pytest.mark.parametrize("log_size", [4, 5, 12, 13, 14, 15, 18, 22])
+def test_lifted_m31_prefix_counts_match_oracle(ctx, oracle, log_size):
+    """Lifted-M31 inputs whose nonzero prefix is at most N/4 skip the two copy-only top
+    stages of the first FFT pass; longer prefixes run every stage.  Prefixes of 1,
+    N/4 - 1, N/4, N/4 + 1, N/2 and N coefficients, at sizes whose first pass covers 1,
+    2 and 3+ stages (and single-pass sizes), give the oracle's proofs."""
+    N = 1 << log_size
+    if log_size == 22:
+        counts = [N // 4, N // 4 + 1]
+    else:
+        counts = sorted({1, max(1, N // 4 - 1), max(1, N // 4), N // 4 + 1, N // 2, N})
+    rounds = max(1, log_size - 4)
+    rng = np.random.default_rng(0xC0 + log_size)
+    offs = np.cumsum([0] + counts[:-1]).tolist()
+    flat = np.zeros((sum(counts), 4), np.uint32)
+    flat[:, 0] = rng.integers(0, G.P, size=len(flat), dtype=np.uint32)
+    b = azk.BatchProver(ctx, [log_size] * len(counts), [rounds] * len(counts), 2, 8)
+    b.upload(flat, offs, counts)
+    pubs = rng.integers(0, 256, size=32 * len(counts), dtype=np.uint8).tobytes()
+    b.prove(pubs)
+    proofs = b.proofs()
+    for i, c in enumerate(counts):
+        full = np.zeros((N, 4), np.uint32)
+        full[:c] = flat[offs[i]:offs[i] + c]
+        want = oracle.prove(log_size, oracle.fft_evaluate(log_size, full), 2, 8, pubs[32 * i:32 * i + 32], rounds).proof
+        assert proofs[i] == want, (log_size, c)
+
+
 def test_batch_mixes_m31_and_qm31_instances(ctx, oracle):
     logs = [14, 13, 9, 15]
     rounds = [lg - 6 for lg in logs]
