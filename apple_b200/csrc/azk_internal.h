@@ -96,11 +96,14 @@ struct FftJob {
 };
 
 // Circle FFT pass geometry: the stages above bit 12 run first in chunks of at
-// most 10 (strided tiles of 2^m rows x 4 columns), then one pass runs stages
-// min(logn,12)-1 ... 0 on contiguous 4096-element tiles.
+// most 10 (strided tiles of 2^m rows x 2^c columns, c = 12 - m up to 8, so that a
+// tile holds 4096 values whatever m is and a block's threads all have work), then
+// one pass runs stages min(logn,12)-1 ... 0 on contiguous 4096-element tiles.
+// The tile loops step one row per THREADS >> c threads, so 2^c stays <= 256, the
+// smaller of the two kernels' block sizes.
 static constexpr uint32_t kFftLowBits = 12;
 static constexpr uint32_t kFftChunk = 10;
-static constexpr uint32_t kFftCols = 2;
+static constexpr uint32_t kFftMaxColsLog = 8;
 struct FftPassGeom {
   uint32_t s_lo, m, c;
 };
@@ -112,7 +115,9 @@ __host__ __device__ inline FftPassGeom fft_pass_geom(uint32_t logn, uint32_t pas
   if (pass < hc) {
     uint32_t top = logn - 1 - pass * kFftChunk;
     uint32_t lo = top + 1 >= kFftLowBits + kFftChunk ? top + 1 - kFftChunk : kFftLowBits;
-    return {lo, top - lo + 1, kFftCols};
+    const uint32_t m = top - lo + 1;
+    const uint32_t c = kFftLowBits - m < kFftMaxColsLog ? kFftLowBits - m : kFftMaxColsLog;
+    return {lo, m, c};
   }
   uint32_t m = logn < kFftLowBits ? logn : kFftLowBits;
   return {0, m, 0};
