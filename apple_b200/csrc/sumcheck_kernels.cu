@@ -63,8 +63,9 @@ __device__ void sc_frame(FrameBuf& f, uint8_t type) {
 //      alternate between two arrays, so the one __syncwarp after the stores also
 //      orders the previous round's loads of the other array before its next stores;
 //   2. pi and chi in one gather: lane (x, y) shuffles e from the pi sources of
-//      (x, y), (x + 1, y) and (x + 2, y); iota through a mask that is zero
-//      except on lane 0.
+//      (x, y), (x + 1, y) and (x + 2, y); iota enters as chi(b0 ^ rc, b1, b2)
+//      (= chi(b0, b1, b2) ^ rc) through a mask that is zero except on lane 0, so
+//      its XOR overlaps the wait for the later shuffles.
 // ---------------------------------------------------------------------------
 __constant__ static const uint8_t kRhoOffsets[25] = {0,  1,  62, 28, 27, 36, 44, 6,  55, 20, 3,  10, 43,
                                                      25, 39, 41, 45, 15, 21, 8,  18, 2,  61, 56, 14};
@@ -116,10 +117,10 @@ struct WarpKeccak {
         const uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
         const uint32_t l2 = swap ? hi : lo, h2 = swap ? lo : hi;
         const uint64_t e = ((uint64_t)__funnelshift_l(l2, h2, rot) << 32) | __funnelshift_l(h2, l2, rot);
-        const uint64_t b0 = __shfl_sync(0xffffffffu, e, s0);
+        const uint64_t b0 = __shfl_sync(0xffffffffu, e, s0) ^ (kKeccakRC[r + k] & rc_mask);
         const uint64_t b1 = __shfl_sync(0xffffffffu, e, s1);
         const uint64_t b2 = __shfl_sync(0xffffffffu, e, s2);
-        a = chi_64(b0, b1, b2) ^ (kKeccakRC[r + k] & rc_mask);
+        a = chi_64(b0, b1, b2);
       }
     }
   }
