@@ -649,10 +649,12 @@ def main():
                 "algorithmic": f"{work['tree_permutations']} permutations per superstep over {tree_launches} launches",
             },
             "roofline_hbm": {
-                "bound": "hbm", "kernel": "fft_pass_kernel", "achieved": fft_gbs, "peak": hbm_gbs, "unit": "GB/s",
+                "bound": "hbm", "kernel": "Circle FFT stage (fft_pass_m31_kernel + fft_m31_persistent_kernel)", "achieved": fft_gbs, "peak": hbm_gbs,
+                "unit": "GB/s",
                 "frac": fft_gbs / hbm_gbs if hbm_gbs else None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_kind})",
                 "algorithmic": "16N read + 16N write + 4(N-1) twiddle bytes per codeword",
-                "traffic": traffic.get("fft_bytes_per_launch"),
+                "traffic": traffic.get("fft_bytes_per_stage"),
+                "traffic_scope": "DRAM bytes of the whole FFT stage of one superstep (both pass launches), like achieved",
             },
             "stage_seconds": prof,
             "gpu_launches": work["launches"] * args.steps,
