@@ -233,7 +233,42 @@ __global__ void __launch_bounds__(THREADS) fft_pass_q_kernel(const FftJob* __res
 template <int THREADS>
 __device__ __forceinline__ void fft_m31_tile_stages(uint32_t* sv, const uint32_t* stw, const FftPassGeom& g, uint32_t T, bool top_zero) {
   int j = (int)g.m - 1;
-  if (top_zero && j >= 2) {
+  if (top_zero && g.m % 3 == 1 && j >= 3) {
+    // m = 4, 7, 10: the two copying stages and the next two (radix 4 on the 4 live
+    // values of a 16-value group, once per copy) in one round trip, so the rest is
+    // whole radix-8 trips instead of ending on a one-stage trip
+    const uint32_t p = (uint32_t)j + g.c;
+    const uint32_t* tw2 = stw + fft_stw_offset(g.m, (uint32_t)j - 2);
+    const uint32_t* tw3 = stw + fft_stw_offset(g.m, (uint32_t)j - 3);
+    const uint32_t lowmask = (1u << (p - 3)) - 1;
+    uint32_t ob[16];
+#pragma unroll
+    for (uint32_t b = 0; b < 16; b++)
+      ob[b] = fpad(((b >> 3) << p) | (((b >> 2) & 1u) << (p - 1)) | (((b >> 1) & 1u) << (p - 2)) | ((b & 1u) << (p - 3)));
+    for (uint32_t k = threadIdx.x; k < T / 16; k += THREADS) {
+      const uint32_t e0 = ((k & ~lowmask) << 4) | (k & lowmask);
+      const uint32_t row = e0 >> g.c;
+      const uint32_t a0 = fpad(e0);
+      const uint32_t x0 = sv[a0], x1 = sv[a0 + ob[1]], x2 = sv[a0 + ob[2]], x3 = sv[a0 + ob[3]];
+      const uint32_t r2 = row >> (j - 1), r3 = row >> (j - 2);
+#pragma unroll
+      for (uint32_t q = 0; q < 4; q++) {
+        // copy q of the live values (its two top row bits = q)
+        const uint32_t t2 = tw2[r2 | q];
+        uint32_t y0 = x0, y1 = x1, y2 = x2, y3 = x3;
+        bfly_m31(y0, y2, t2);
+        bfly_m31(y1, y3, t2);
+        bfly_m31(y0, y1, tw3[r3 | (q << 1)]);
+        bfly_m31(y2, y3, tw3[r3 | (q << 1) | 1u]);
+        sv[a0 + ob[4 * q]] = y0;
+        sv[a0 + ob[4 * q + 1]] = y1;
+        sv[a0 + ob[4 * q + 2]] = y2;
+        sv[a0 + ob[4 * q + 3]] = y3;
+      }
+    }
+    __syncthreads();
+    j -= 4;
+  } else if (top_zero && j >= 2) {
     const uint32_t p = (uint32_t)j + g.c;
     const uint32_t* tw2 = stw + fft_stw_offset(g.m, (uint32_t)j - 2);
     const uint32_t lowmask = (1u << (p - 2)) - 1;

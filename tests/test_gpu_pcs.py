@@ -191,7 +191,7 @@ def test_lifted_m31_coefficients_match_oracle(ctx, oracle, log_size, count_log, 
     assert proof == oracle.prove(log_size, oracle.fft_evaluate(log_size, full), 2, 8, pub, rounds).proof
 
 
-@pytest.mark.parametrize("log_size", [4, 5, 12, 13, 14, 15, 18, 22])
+@pytest.mark.parametrize("log_size", [4, 5, 12, 13, 14, 15, 16, 18, 19, 22])
 def test_lifted_m31_prefix_counts_match_oracle(ctx, oracle, log_size):
     """Lifted-M31 inputs whose nonzero prefix is at most N/4 skip the two copy-only top
     stages of the first FFT pass; longer prefixes run every stage.  Prefixes of 1,
