@@ -509,7 +509,10 @@ __global__ void __launch_bounds__(THREADS) fft_m31_persistent_kernel(const FftJo
 }
 
 static constexpr size_t kFftSmemPersistent = 2 * kFftSmemM31;  // two buffers of values + twiddles
-static uint32_t g_fft_m31_grid = 0;                            // resident CTAs of the persistent kernel
+// Resident CTAs of the persistent kernel, per device (contexts on different devices
+// size their grids from their own SM counts).
+static constexpr int kFftMaxDevices = 64;
+static uint32_t g_fft_m31_grid[kFftMaxDevices] = {0};
 
 cudaError_t prepare_fft_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fft_pass_q_kernel<kFftThreadsQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemQ);
@@ -524,14 +527,17 @@ cudaError_t prepare_fft_kernels() {
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_m31_persistent_kernel<kFftThreadsM31>, kFftThreadsM31, kFftSmemPersistent)) !=
       cudaSuccess)
     return e;
-  g_fft_m31_grid = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
+  if (dev >= 0 && dev < kFftMaxDevices) g_fft_m31_grid[dev] = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
   return cudaSuccess;
 }
 
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, bool last, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
   if (narrow && last) {
-    const uint32_t grid = g_fft_m31_grid && g_fft_m31_grid < nwork ? g_fft_m31_grid : nwork;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kFftMaxDevices) dev = 0;
+    const uint32_t resident = g_fft_m31_grid[dev];
+    const uint32_t grid = resident && resident < nwork ? resident : nwork;
     fft_m31_persistent_kernel<kFftThreadsM31><<<grid, kFftThreadsM31, kFftSmemPersistent, s>>>(d_jobs, d_work, nwork);
   } else if (narrow) {
     fft_pass_m31_kernel<kFftThreadsM31><<<nwork, kFftThreadsM31, kFftSmemM31, s>>>(d_jobs, d_work);

@@ -36,7 +36,9 @@ static constexpr uint64_t kNoAllocScratchBytes = kNoAllocNodeOffset + 32ull * kN
 static __device__ __align__(256) uint8_t g_merkle_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device addresses of the array, resolved once per device with that device current
-// (the array's host-side name is not a device address).
+// (the array's host-side name is not a device address).  The cached address lives
+// as long as the device's context: a cudaDeviceReset in the same process unloads
+// the library's device image, so this entry point is not supported after one.
 static std::mutex g_noalloc_mu;
 static uint8_t* g_noalloc_ptr[64] = {nullptr};
 

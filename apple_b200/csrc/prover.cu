@@ -917,6 +917,7 @@ struct azk_server {
   uint64_t tick = 0;
   bool stop = false;
   std::vector<std::map<ShapeKey, Resident>> cache;  // per worker
+  std::vector<uint8_t> busy;                         // per worker: running a job (its cache must stay)
   // per worker: jobs of zeros it runs once before serving (azk_server_warm), so its
   // engines, sum-check buffers and pinned staging exist before the first real job
   std::vector<std::deque<std::shared_ptr<ServeJob>>> warm;
@@ -1030,11 +1031,29 @@ void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j, Staging& st) {
   std::memcpy(j.result.data(), words.data(), j.result.size());
 }
 
+// Evict the least recently used cached shape of worker `w` into `dropped` (its
+// device memory is freed by the caller after the server lock is released: a free
+// waits for the whole device).  Returns false when the worker caches nothing.
+bool evict_lru(azk_server* sv, int w, std::vector<Resident>& dropped) {
+  auto& cache = sv->cache[w];
+  if (cache.empty()) return false;
+  auto lru = cache.begin();
+  for (auto it = cache.begin(); it != cache.end(); ++it)
+    if (it->second.last_use < lru->second.last_use) lru = it;
+  sv->held -= lru->second.bytes;
+  dropped.push_back(std::move(lru->second));
+  cache.erase(lru);
+  return true;
+}
+
 // Called with the server lock held.  Takes the front job if its shape is cached
-// by this worker or its bytes fit the budget, evicting this worker's least
-// recently used shapes when that makes room.  Nothing is taken while the job
-// cannot fit; a job larger than the budget never enters the queue.
-std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
+// by this worker or its bytes fit the budget.  To make room it evicts this
+// worker's least recently used shapes first, then those of idle workers (a worker
+// that is not running a job has nothing in flight on its stream, so its cached
+// memory can go); busy workers keep theirs.  Nothing is taken while the job cannot
+// fit; a job larger than the budget never enters the queue.  Evicted memory is
+// handed back in `dropped` for the caller to free outside the lock.
+std::shared_ptr<ServeJob> try_take(azk_server* sv, int w, std::vector<Resident>& dropped) {
   // this worker's warm-up jobs first; one that cannot fit the budget is dropped
   while (!sv->warm[w].empty()) {
     auto j = sv->warm[w].front();
@@ -1053,6 +1072,7 @@ std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
     }
     cache[key].last_use = ++sv->tick;
     sv->warm[w].pop_front();
+    sv->busy[w] = 1;
     j->state = 1;
     return j;
   }
@@ -1061,12 +1081,12 @@ std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
   const auto& j = sv->queue.front();
   ShapeKey key = shape_of(*j);
   if (!cache.count(key)) {
-    while (sv->held + j->bytes > sv->budget && !cache.empty()) {
-      auto lru = cache.begin();
-      for (auto it = cache.begin(); it != cache.end(); ++it)
-        if (it->second.last_use < lru->second.last_use) lru = it;
-      sv->held -= lru->second.bytes;
-      cache.erase(lru);  // frees the device memory of that shape
+    while (sv->held + j->bytes > sv->budget && evict_lru(sv, w, dropped)) {
+    }
+    for (uint32_t v = 0; v < sv->slots && sv->held + j->bytes > sv->budget; v++) {
+      if ((int)v == w || sv->busy[v]) continue;
+      while (sv->held + j->bytes > sv->budget && evict_lru(sv, (int)v, dropped)) {
+      }
     }
     if (sv->held + j->bytes > sv->budget) return nullptr;
     Resident& r = cache[key];
@@ -1077,6 +1097,7 @@ std::shared_ptr<ServeJob> try_take(azk_server* sv, int w) {
   auto job = j;
   sv->queue.pop_front();
   sv->running++;
+  sv->busy[w] = 1;
   job->state = 1;
   job->started = std::chrono::steady_clock::now();
   return job;
@@ -1092,17 +1113,25 @@ void worker_loop(azk_server* sv, int w) {
   for (;;) {
     std::shared_ptr<ServeJob> job;
     Resident* res = nullptr;
+    std::vector<Resident> dropped;  // evicted shapes, freed below without the lock
     {
       std::unique_lock<std::mutex> lk(sv->mu);
       for (;;) {
         if (sv->stop && sv->queue.empty() && sv->warm[w].empty()) break;
-        job = try_take(sv, w);
+        job = try_take(sv, w, dropped);
         if (job) break;
+        if (!dropped.empty()) {  // free what was evicted, then look again
+          lk.unlock();
+          dropped.clear();
+          lk.lock();
+          continue;
+        }
         sv->cv.wait(lk);
       }
       if (!job) break;
       res = &sv->cache[w][shape_of(*job)];
     }
+    dropped.clear();
     // the outcome is published under the lock together with the finish time, so a
     // poll never sees a finished job without its latency
     int outcome = 2;
@@ -1119,23 +1148,26 @@ void worker_loop(azk_server* sv, int w) {
       error = e.what();
       outcome = 3;
     }
+    std::vector<Resident> failed;  // a failed job's shape, freed without the lock
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       job->error = error;
       job->state = outcome;
+      sv->busy[w] = 0;
       if (job->id == 0) {  // a warm-up job: not a result anyone polls
         if (job->state == 3) {
           auto it = sv->cache[w].find(shape_of(*job));
           if (it != sv->cache[w].end()) {
             sv->held -= it->second.bytes;
+            failed.push_back(std::move(it->second));
             sv->cache[w].erase(it);
           }
         }
         sv->warm_pending--;
         sv->cv.notify_all();
         sv->done_cv.notify_all();
-        continue;
       }
+      if (job->id == 0) continue;
       job->finished = std::chrono::steady_clock::now();
       job->input.clear();
       job->input.shrink_to_fit();
@@ -1143,6 +1175,7 @@ void worker_loop(azk_server* sv, int w) {
         auto it = sv->cache[w].find(shape_of(*job));
         if (it != sv->cache[w].end()) {
           sv->held -= it->second.bytes;
+          failed.push_back(std::move(it->second));
           sv->cache[w].erase(it);
         }
       }

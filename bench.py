@@ -209,25 +209,79 @@ def max_over_ranks(dist, value: float, local: int) -> float:
     return float(t.item())
 
 
-def cpu_sample(logs, rounds, counts, offsets, rows, pubs, budget_elems):
-    """Prove a prefix of the workload's instances with the CPU oracle (all host threads)."""
+def stratified_sample(logs, max_log=64):
+    """One instance of each log size present up to `max_log` (the first of each,
+    smallest size first).  The workload draws log sizes uniformly, so the full
+    sample has the workload's size mix."""
+    first = {}
+    for i, lg in enumerate(logs):
+        if lg <= max_log:
+            first.setdefault(lg, i)
+    return [first[lg] for lg in sorted(first)]
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_sample(logs, rounds, counts, offsets, rows, pubs, sample):
+    """Prove the instances `sample` with the CPU oracle (all host threads): FFT of the
+    coefficients, then the proof.  Returns (elements, seconds, proofs)."""
     from oracle import pyoracle as O
 
     t0 = time.perf_counter()
     elems = 0
-    done = 0
-    for i, lg in enumerate(logs):
-        if elems >= budget_elems and done:
-            break
+    proofs = {}
+    for i in sample:
+        lg = logs[i]
         n = 1 << lg
         c = np.zeros((n, 4), np.uint32)
         c[: counts[i]] = rows[offsets[i]:offsets[i] + counts[i]]
         ev = O.fft_evaluate(lg, c)
-        O.prove(lg, ev, 2, 64, pubs[32 * i:32 * i + 32], rounds[i])
+        proofs[i] = O.prove(lg, ev, 2, 64, pubs[32 * i:32 * i + 32], rounds[i]).proof
         elems += n
-        done += 1
     dt = time.perf_counter() - t0
-    return elems, dt, done
+    return elems, dt, proofs
+
+
+def cpu_literal_sample(logs, rounds, counts, offsets, rows, pubs, max_log=14):
+    """The reference's literal single-thread builder (a full layer re-hash per opening,
+    CircleProofFormat.swift:1287-1356) on the sampled instances of log size <=
+    `max_log`, one host thread.  Returns (elements, seconds, proofs)."""
+    from oracle import pyoracle as O
+
+    sample = [i for i in stratified_sample(logs) if logs[i] <= max_log]
+    t0 = time.perf_counter()
+    elems = 0
+    proofs = {}
+    for i in sample:
+        lg = logs[i]
+        n = 1 << lg
+        c = np.zeros((n, 4), np.uint32)
+        c[: counts[i]] = rows[offsets[i]:offsets[i] + counts[i]]
+        proofs[i] = O.prove_literal(lg, c, 2, 64, pubs[32 * i:32 * i + 32], rounds[i])
+        elems += n
+    return elems, time.perf_counter() - t0, proofs
+
+
+def verify_all(proofs, pubs):
+    """The oracle's verifier over every proof, on all host threads."""
+    import concurrent.futures as cf
+
+    from oracle import pyoracle as O
+
+    def one(i):
+        return O.verify(proofs[i], pubs[32 * i:32 * i + 32])
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        return list(ex.map(one, range(len(proofs))))
 
 
 def run_reference(args, logs, rounds, counts, offsets, rows, pubs, world, rank, dist):
@@ -237,24 +291,23 @@ def run_reference(args, logs, rounds, counts, offsets, rows, pubs, world, rank, 
 
     O.lib()
     threads = O.num_threads()
-    budget = args.cpu_budget_elems
+    sample = stratified_sample(logs, args.cpu_max_log)
+    small = [i for i in sample if logs[i] <= 12]
     for _ in range(args.warmup):
-        cpu_sample(logs[:2], rounds[:2], counts[:2], offsets[:2], rows, pubs, 1)
-    vals = []
-    total_t, total_e, inst = 0.0, 0, 0
+        cpu_sample(logs, rounds, counts, offsets, rows, pubs, small[:2])
+    total_t, total_e = 0.0, 0
     for _ in range(args.steps):
-        e, dt, k = cpu_sample(logs, rounds, counts, offsets, rows, pubs, budget)
-        vals.append(e / dt)
+        e, dt, _ = cpu_sample(logs, rounds, counts, offsets, rows, pubs, sample)
         total_t += dt
         total_e += e
-        inst = k
     value = total_e / total_t
-    sample = f"first {inst} instances of the workload (sum 2^logN = {total_e // args.steps}), FFT + prove with the C++ oracle per step"
+    desc = (f"one instance of each log size {logs[sample[0]]}..{logs[sample[-1]]} of the workload (its size mix; sum 2^logN = "
+            f"{total_e // args.steps}), FFT + prove with the C++ oracle on {threads} threads per step")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * total_t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64",
         "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "The reference (Swift + Metal) cannot run on Linux/B200; this arm times the repository's C++ restatement of its CPU oracles.",
     }
@@ -428,8 +481,10 @@ def main():
     ap.add_argument("--leaf64", type=int, default=1)
     ap.add_argument("--group-log", type=int, default=12)
     ap.add_argument("--threads", type=int, default=256)
-    ap.add_argument("--plain-steps", type=int, default=1)
-    ap.add_argument("--cpu-budget-elems", type=int, default=1 << 21)
+    ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--plain-warmup", type=int, default=1)
+    ap.add_argument("--cpu-max-log", type=int, default=64, help="largest log size in the CPU oracle's sample")
+    ap.add_argument("--literal-max-log", type=int, default=14, help="largest log size the literal single-thread CPU form proves")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--e2e-pipeline", type=int, default=1)
@@ -489,6 +544,8 @@ def main():
     t_dev = max_over_ranks(dist, sum(gpu_times), local)
     value = world * elems * args.steps / t_dev
     print(f"[bench] batched steps: {[round(1000 * g, 2) for g in gpu_times]} ms", file=sys.stderr, flush=True)
+    # the proofs of the last timed superstep, checked against the oracle below
+    gpu_proofs = batch.proofs() if rank == 0 and not args.no_cpu else None
 
     # ---- per-stage profile (events inside the captured graph) ----
     batch.set_profiling(True)
@@ -571,6 +628,7 @@ def main():
         untuned_value = world * elems / max_over_ranks(dist, statistics.median(ut), local)
         del bu
     plain_times = []
+    plain_mismatch = False
     if args.plain_steps:
         tables = tuned_tables()
         psched = dict(layer_treelet=tables["pcs_single"], group_log=args.group_log, threads=args.threads, use_graph=0) if tables and not args.treelet_log \
@@ -580,9 +638,13 @@ def main():
             batch = None
         bp = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=psched)
         bp.upload(host_rows, offsets, counts)
+        for _ in range(args.plain_warmup):
+            bp.prove(pubs, plain=True)
         for _ in range(args.plain_steps):
             st = bp.prove(pubs, plain=True)
             plain_times.append(st.gpu_s)
+        if gpu_proofs is not None and bp.proofs() != gpu_proofs:
+            plain_mismatch = True
         del bp
     t_plain = max_over_ranks(dist, statistics.median(plain_times), local) if plain_times else float("nan")
 
@@ -611,7 +673,12 @@ def main():
     tree_rate = work["tree_permutations"] / prof["tree_s"] if prof["tree_s"] > 0 else 0.0
     tree_launches = max(1, max(rounds))
     hbm_gbs, hbm_kind = measured_peaks()
-    fft_gbs = work["fft_bytes"] / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
+    # FFT bytes: the input's nonzero prefix (16 B per coefficient read; the zero tail
+    # is known from the upload and never read) + the 16 B per element codeword
+    # written + 4 B per stage twiddle; the dense figure charges all 16N input bytes
+    fft_bytes_prefix = int(sum(16 * c + 16 * (1 << lg) + 4 * ((1 << lg) - 1) for c, lg in zip(counts, logs)))
+    fft_gbs = fft_bytes_prefix / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
+    fft_gbs_dense = work["fft_bytes"] / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
     traffic = profile_traffic()
 
     serving = None
@@ -620,19 +687,47 @@ def main():
         print(f"[bench] serving {serving}", file=sys.stderr, flush=True)
 
     line = None
+    parity_ok = True
     if rank == 0:
         cpu = None
+        parity = None
         if not args.no_cpu and world == 1:
             from oracle import pyoracle as O
 
-            e, dt, k = cpu_sample(logs, rounds, counts, offsets, rows, pubs, args.cpu_budget_elems)
-            cpu = {"value": e / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                   "sample": f"first {k} instances of the workload (sum 2^logN = {e}), FFT + prove with the C++ oracle ({dt:.1f} s)"}
+            sample = stratified_sample(logs, args.cpu_max_log)
+            e, dt, want = cpu_sample(logs, rounds, counts, offsets, rows, pubs, sample)
+            equal = [i for i in sample if gpu_proofs[i] == want[i]]
+            t0 = time.perf_counter()
+            accepted = verify_all(gpu_proofs, pubs)
+            t_verify = time.perf_counter() - t0
+            parity = {"instances_checked": len(sample), "equal": len(equal) == len(sample), "log_sizes": [logs[i] for i in sample],
+                      "verified": int(sum(accepted)), "verified_of": len(gpu_proofs), "verified_all": all(accepted),
+                      "plain_equal": not plain_mismatch, "verify_s": t_verify,
+                      "check": "proof bytes of the stratified sample equal the oracle's; every proof of the superstep is accepted by "
+                               "the oracle's verifier; the plain form's proofs equal the batched form's"}
+            parity_ok = parity["equal"] and parity["verified_all"] and not plain_mismatch
+            cpu = {"value": e / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port", "cpu_model": cpu_model(),
+                   "sample": f"one instance of each log size {logs[sample[0]]}..{logs[sample[-1]]} of the workload (its size mix; "
+                             f"sum 2^logN = {e}), FFT + prove with the C++ oracle on {O.num_threads()} threads ({dt:.1f} s)"}
+            if args.literal_max_log:
+                le, ldt, lproofs = cpu_literal_sample(logs, rounds, counts, offsets, rows, pubs, args.literal_max_log)
+                if lproofs:
+                    cpu["literal_single_thread"] = {
+                        "value": le / ldt, "unit": UNIT, "cores": 1, "seconds": ldt, "log_sizes": [logs[i] for i in lproofs],
+                        "equal": all(lproofs[i] == gpu_proofs[i] for i in lproofs),
+                        "form": "the reference's literal builder: one thread, radix-2 FFT stage by stage, a full layer re-hash "
+                                "for every opening, the transcript replayed from the start for every challenge; sizes above "
+                                f"log {args.literal_max_log} are not run (the per-opening rebuild grows as queries x rounds x N)"}
+                    parity["equal"] = parity["equal"] and cpu["literal_single_thread"]["equal"]
+                    parity_ok = parity_ok and cpu["literal_single_thread"]["equal"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/u64 (M31/QM31 field, Keccak lanes)", "data": "synthetic (seeded SplitMix64)", "config": config_block(args, logs),
+            "parity": parity,
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": 1000 * t_plain if plain_values_ok(plain_value) else None,
+                      "samples_ms": [1000 * t for t in plain_times], "warmup": args.plain_warmup,
+                      "spread_ms": [1000 * min(plain_times), 1000 * max(plain_times)] if plain_times else None,
                       "batched_over_plain": value / plain_value if plain_values_ok(plain_value) else None,
                       "schedule": "tuned single-instance per-layer table" if (tuned_tables() and not args.treelet_log) else "same as batched"},
             "leaf64": leaf64,
@@ -652,7 +747,10 @@ def main():
                 "bound": "hbm", "kernel": "Circle FFT stage (fft_pass_m31_kernel + fft_m31_persistent_kernel)", "achieved": fft_gbs, "peak": hbm_gbs,
                 "unit": "GB/s",
                 "frac": fft_gbs / hbm_gbs if hbm_gbs else None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_kind})",
-                "algorithmic": "16N read + 16N write + 4(N-1) twiddle bytes per codeword",
+                "algorithmic": "16 B per nonzero input coefficient read + 16N codeword bytes written + 4(N-1) twiddle bytes per codeword",
+                "algorithmic_bytes": fft_bytes_prefix,
+                "dense": {"achieved": fft_gbs_dense, "frac": fft_gbs_dense / hbm_gbs if hbm_gbs else None,
+                          "algorithmic": "16N read + 16N write + 4(N-1) twiddle bytes per codeword"},
                 "traffic": traffic.get("fft_bytes_per_stage"),
                 "traffic_scope": "DRAM bytes of the whole FFT stage of one superstep (both pass launches), like achieved",
             },
@@ -667,6 +765,10 @@ def main():
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
+    if not parity_ok:
+        # the reference's bench exits 2 when a GPU result differs from its CPU oracle
+        print("[bench] PARITY FAILURE: GPU proofs differ from the CPU oracle", file=sys.stderr, flush=True)
+        sys.exit(2)
 
 
 if __name__ == "__main__":

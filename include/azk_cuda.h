@@ -130,7 +130,8 @@ azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* host_digests, u
  * rejected with AZK_ERR_INVALID_INPUT_LAYOUT.  Work is queued on `stream`
  * (NULL = default stream) and the call returns without waiting.  The first call on
  * a device resolves the array's device address, so make it before any stream
- * capture.  The array is shared by every call on a device: calls whose work
+ * capture; that address is kept for the life of the device's context, so the entry
+ * point is not supported after a cudaDeviceReset in the same process.  The array is shared by every call on a device: calls whose work
  * overlaps on the GPU race and must be serialised by the caller.  Errors are
  * reported through azk_last_error_message(NULL). */
 azk_status azk_merkle_root_noalloc(const void* dev_leaves, uint64_t leaf_count, uint64_t leaf_stride, uint64_t leaf_length, void* dev_root,

@@ -1001,6 +1001,61 @@ inline Proof build_proof(const std::vector<QM31>& evaluations, const Domain& d, 
   return p;
 }
 
+// The reference's builder as written (CircleProofFormat.swift:1173-1356): every
+// round's challenge comes from deriveChallenges over all commitments so far (the
+// transcript replayed from its prefix), and every query opening packs its layer
+// and rebuilds that layer's whole Merkle tree (MerkleOracle.openingSHA3_256), so
+// openings cost O(queries x rounds x N) permutations.  Same bytes as build_proof;
+// the CPU baseline times it (on one thread) beside the efficient form.
+inline Proof build_proof_literal(const std::vector<QM31>& evaluations, const Domain& d, const Security& s, const Digest& pub, u32 rounds) {
+  require(d.storageOrder == 1 && d.canonical() && evaluations.size() == d.size() && s.foldingStep == 1 && s.grindingBits <= 20 && rounds > 0 && rounds <= d.logSize);
+  validate_security(s);
+  for (auto& e : evaluations) require(q_canonical(e));
+  auto inv = inverse_domain_layers(d, rounds);
+  std::vector<std::vector<QM31>> layers;
+  std::vector<Digest> cm;
+  std::vector<QM31> ch;
+  std::vector<QM31> cur = evaluations;
+  for (u32 r = 0; r < rounds; r++) {  // :1209-1242
+    layers.push_back(cur);
+    Bytes lb = pack_qm31(cur);
+    cm.push_back(merkle_raw(lb.data(), lb.size(), cur.size(), 16, 16).root());
+    std::vector<QM31> prefix = derive_challenges(d, s, pub, cm);
+    require(prefix.size() == cm.size());
+    ch.push_back(prefix[r]);
+    cur = fold(cur, lift(inv[r]), prefix[r]);
+  }
+  Proof p;
+  p.domain = d;
+  p.security = s;
+  p.publicDigest = pub;
+  p.commitments = cm;
+  p.finalLayer = cur;
+  p.hasNonce = find_grinding_nonce(d, s, pub, cm, cur, &p.nonce);
+  TranscriptResult tr = transcript_derive(d, s, pub, cm, cur, p.hasNonce, p.nonce);
+  if (!(tr.challenges.size() == ch.size() && std::equal(ch.begin(), ch.end(), tr.challenges.begin())))
+    fail(Err::correctnessValidationFailed, "Circle FRI transcript challenge changed after final-layer binding.");
+  for (u32 pair : tr.queryPairs) {  // makeQuery / makeOpening (:1287-1356)
+    Query q;
+    q.initialPair = pair;
+    u64 cp = pair;
+    for (u32 li = 0; li < layers.size(); li++) {
+      require(cp < layers[li].size() / 2);
+      Bytes lb = pack_qm31(layers[li]);
+      LayerOpening lo;
+      lo.layerIndex = li;
+      lo.pairIndex = cp;
+      lo.left = {cp * 2, layers[li][cp * 2], merkle_opening_literal(lb.data(), lb.size(), layers[li].size(), 16, 16, cp * 2, nullptr)};
+      lo.right = {cp * 2 + 1, layers[li][cp * 2 + 1], merkle_opening_literal(lb.data(), lb.size(), layers[li].size(), 16, 16, cp * 2 + 1, nullptr)};
+      q.layers.push_back(std::move(lo));
+      cp >>= 1;
+    }
+    p.queries.push_back(std::move(q));
+  }
+  validate_proof_shape(p);
+  return p;
+}
+
 // ---------------------------------------------------------------------------
 // Commit-and-fold chain with 64-byte Merkle leaves (4 consecutive QM31, little-
 // endian, per leaf): the transcript frames and folds of build_proof (header,

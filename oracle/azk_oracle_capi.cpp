@@ -277,6 +277,37 @@ int azko_prove(u32 logSize, const u32* evaluations, u32 logBlowup, u32 queries, 
   AZKO_CATCH
 }
 
+// The reference's literal single-thread form from FFT-basis coefficients: the
+// stage-by-stage FFT (CircleCodeword.swift:72-98) and build_proof_literal, with the
+// oracle's thread count held at one for the call.
+int azko_prove_literal(u32 logSize, const u32* coefficients, u32 logBlowup, u32 queries, const u8* pub, u32 rounds, u8* proofOut, u64* proofLen) {
+#ifdef _OPENMP
+  const int saved = omp_get_max_threads();
+  omp_set_num_threads(1);
+#endif
+  int rc = 0;
+  try {
+    Domain d = canonical_domain(logSize);
+    Security s{logBlowup, queries, 1, 0};
+    auto v = q_vec(coefficients, d.size());
+    fft_in_place(v, d, fft_twiddles(d));
+    Bytes b = encode_proof(build_proof_literal(v, d, s, dg(pub), rounds));
+    require(b.size() <= *proofLen, Err::invalidInputLayout, "proof buffer too small");
+    std::memcpy(proofOut, b.data(), b.size());
+    *proofLen = b.size();
+  } catch (const OracleError& e) {
+    g_err = e.what();
+    rc = int(e.kind);
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    rc = 99;
+  }
+#ifdef _OPENMP
+  omp_set_num_threads(saved);
+#endif
+  return rc;
+}
+
 int azko_commit_fold_chain_leaf64(u32 logSize, const u32* evaluations, u32 logBlowup, u32 queries, const u8* pub, u32 rounds, u8* commitOut,
                                   u32* chOut, u32* finalOut) {
   AZKO_TRY

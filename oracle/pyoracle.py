@@ -315,6 +315,21 @@ def prove(log_size: int, evaluations, log_blowup: int, queries: int, public_dige
     return ProofResult(out[: plen.value].tobytes(), [cm[32 * r:32 * r + 32].tobytes() for r in range(rounds)], ch, fin, [int(v) for v in qp])
 
 
+def prove_literal(log_size: int, coefficients, log_blowup: int, queries: int, public_digest: bytes, rounds: int) -> bytes:
+    """FFT-basis coefficients -> proof bytes through the reference's literal builder on
+    one thread (stage-by-stage FFT, transcript replayed per challenge, a full Merkle
+    rebuild per opening); the same bytes as fft_evaluate + prove."""
+    c = _q(coefficients)
+    pub = _bytes(public_digest)
+    n = 1 << log_size
+    cap = 64 + 44 + 64 + 32 * rounds + 16 * n + queries * rounds * 2 * (16 + 32 * log_size + 32) + 64
+    out = np.zeros(cap, np.uint8)
+    plen = c_u64(cap)
+    _check(lib().azko_prove_literal(c_u32(log_size), _p32(c), c_u32(log_blowup), c_u32(queries), _p8(pub), c_u32(rounds), _p8(out),
+                                    ctypes.byref(plen)))
+    return out[: plen.value].tobytes()
+
+
 def commit_fold_chain_leaf64(log_size: int, evaluations, log_blowup: int, queries: int, public_digest: bytes, rounds: int):
     """Commitments, challenges and final layer of the chain with 64-byte (4 x QM31) Merkle leaves."""
     ev = _q(evaluations)

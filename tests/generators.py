@@ -128,3 +128,60 @@ def uniform_m31(seed, n) -> np.ndarray:
         v = v[v != np.uint32(P)]
         out = np.concatenate([out, v])
     return out[:n]
+
+
+# --- seeded inputs of the benchmark configurations ---------------------------
+# Seeds per configuration: C1 0xA11CE001, C2 0xA11CE002, C3 0xA11CE003,
+# C4 0xA11CE004 (bench.py), C5 0xA11CE005.  Uniform bytes are the little-endian
+# bytes of the SplitMix64 stream; uniform M31 values are the low 31 bits of a
+# draw with 0x7fffffff rejected (uniform_m31 above).
+C1_SEED, C2_SEED, C3_SEED = 0xA11CE001, 0xA11CE002, 0xA11CE003
+
+
+def splitmix64_range(seed, start, stop) -> np.ndarray:
+    """Outputs start+1 ... stop of the SplitMix64 stream (element k of the result is
+    output start + k + 1), so a long stream can be made in chunks."""
+    GOLD = np.uint64(0x9E3779B97F4A7C15)
+    k = np.arange(start + 1, stop + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + k * GOLD
+        z ^= z >> np.uint64(30)
+        z *= np.uint64(0xBF58476D1CE4E5B9)
+        z ^= z >> np.uint64(27)
+        z *= np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return z
+
+
+def config_bytes(seed, nbytes) -> np.ndarray:
+    """`nbytes` uniform bytes: the little-endian bytes of the SplitMix64 stream."""
+    words = (nbytes + 7) // 8
+    out = np.empty(words, np.uint64)
+    chunk = 1 << 24
+    for s in range(0, words, chunk):
+        e = min(words, s + chunk)
+        out[s:e] = splitmix64_range(seed, s, e)
+    return out.view(np.uint8)[:nbytes]
+
+
+def config_indices(seed, count, modulus) -> np.ndarray:
+    """`count` seeded leaf indices in [0, modulus) (a power of two)."""
+    return (splitmix64_array(seed ^ 0x1D, count) % np.uint64(modulus)).astype(np.uint64)
+
+
+def config_c1():
+    """C1: 2^16 leaves of 64 uniform bytes and 16 opening indices."""
+    n = 1 << 16
+    return config_bytes(C1_SEED, n * 64), config_indices(C1_SEED, 16, n)
+
+
+def config_c3(log_size=22, log_blowup=2):
+    """C3: FFT-basis coefficient prefix of a log-22 codeword at blowup 4 -- x-line and
+    y-line indices below 2^19 carry uniform M31 values lifted to QM31 (the first
+    2^20 interleaved positions), the rest of the 2^22 coefficients are zero -- and a
+    32-byte public-input digest."""
+    count = (1 << log_size) >> log_blowup
+    coeffs = np.zeros((count, 4), np.uint32)
+    coeffs[:, 0] = uniform_m31(C3_SEED, count)
+    pub = config_bytes(C3_SEED ^ 0x9B, 32).tobytes()
+    return coeffs, pub

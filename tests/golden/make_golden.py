@@ -1,9 +1,9 @@
 """Extract the reference's own golden vectors into tests/golden/ fixtures.
 
-Run in a container where the reference checkout is mounted (default
-/root/reference, override with AZK_REFERENCE_ROOT):
+Run where a checkout of the reference is available, naming its root either as the
+first argument or in AZK_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference root>
 
 It reads the reference's XCTest sources, its checked-in benchmark JSON reports and
 its proof corpus, and writes:
@@ -22,7 +22,7 @@ import os
 import re
 import sys
 
-ROOT = os.environ.get("AZK_REFERENCE_ROOT", "/root/reference")
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("AZK_REFERENCE_ROOT", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 TESTS = "Tests/AppleZKProverTests"
 BENCH = "BenchmarkBaselines"
@@ -164,6 +164,8 @@ def main():
 
 
 if __name__ == "__main__":
+    if not ROOT:
+        sys.exit("usage: make_golden.py <reference root> (or set AZK_REFERENCE_ROOT)")
     if not os.path.isdir(ROOT):
         sys.exit(f"reference checkout not found at {ROOT}")
     main()

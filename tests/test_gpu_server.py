@@ -129,3 +129,35 @@ def test_warm_then_jobs_match_alone(ctx):
     alone = azk.sumcheck_prove(ctx, ev)
     assert res[sid][0]["initial_digest"] == alone["initial_digest"]
     assert np.array_equal(res[sid][0]["challenges"], alone["challenges"])
+
+
+def _shape_bytes(ctx, log_size, rounds, queries):
+    """Device bytes the server holds for one PCS shape (one worker, warmed)."""
+    s = azk.ProofServer(ctx, hbm_budget_bytes=1 << 34, slots=1)
+    s.warm(pcs_shapes=[(log_size, rounds)], log_blowup=2, queries=queries)
+    held = s.stats()["held_bytes"]
+    s.close()
+    return held
+
+
+def test_idle_workers_give_back_memory_for_a_larger_job(ctx):
+    """Shapes cached by idle workers are evicted to admit a job that does not fit
+    otherwise: with a budget of one log-16 shape plus 1 MiB, workers that cached
+    log-14 and log-15 shapes while those jobs ran must give all of it back for the
+    log-16 job (a worker that could only drop its own cache would wait forever)."""
+    rng = np.random.default_rng(0xE71C)
+    a, b, c = (_shape_bytes(ctx, lg, 8, 32) for lg in (14, 15, 16))
+    assert a + b < c
+    server = azk.ProofServer(ctx, hbm_budget_bytes=c + (1 << 20), slots=3)
+    small = [_pcs_job(rng, lg) for lg in (14, 15, 14, 15, 14, 15)]
+    ids = [server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]) for j in small]
+    first = _wait(server, ids)
+    assert server.stats()["held_bytes"] > 0
+    big = _pcs_job(rng, 16)
+    bid = server.submit_pcs(16, 2, big["queries"], big["rounds"], big["coeffs"], big["pub"])
+    got = _wait(server, [bid], timeout=60.0)
+    assert server.stats()["held_bytes"] <= c + (1 << 20)
+    server.close()
+    assert got[bid][0] == azk.CirclePCSFRIProver(ctx, 16, 2, big["queries"], big["rounds"]).prove_coefficients(big["coeffs"], big["pub"])
+    for j, i in zip(small, ids):
+        assert first[i][0] == azk.CirclePCSFRIProver(ctx, j["log_size"], 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])

@@ -50,7 +50,7 @@ def test_reference_arm_prints_once_under_torchrun():
     env = dict(os.environ, AZK_DIST_BACKEND="gloo", OMP_NUM_THREADS="2")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
            "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0", "--instances", "4",
-           "--cpu-budget-elems", "1024"]  # the workload's first instance is log 10
+           "--cpu-max-log", "11"]  # the workload's first instance is log 10
     r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]

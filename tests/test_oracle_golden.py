@@ -321,3 +321,25 @@ def test_leaf64_chain_is_built_from_pinned_parts(oracle):
     assert np.array_equal(fl, oracle.circle_fold_chain(log_size, ev, ch))
     p16 = oracle.prove(log_size, ev, 2, 8, pub, rounds)
     assert p16.commitments[0] != cm[0] and not np.array_equal(p16.challenges[0], ch[0])
+
+
+@pytest.mark.parametrize("log_size,rounds", [(4, 2), (8, 2), (10, 4)])
+def test_literal_builder_equals_efficient_builder(oracle, log_size, rounds):
+    """The reference's literal builder (transcript replayed per challenge, a full Merkle
+    rebuild per opening, one thread), timed as the CPU baseline's single-thread form,
+    gives the same bytes as the efficient builder, and the pinned log-10 proof."""
+    rng = np.random.default_rng(log_size)
+    n = 1 << log_size
+    c = np.zeros((n, 4), np.uint32)
+    c[: n // 4, 0] = rng.integers(0, G.P, size=n // 4, dtype=np.uint32)
+    pub = bytes(range(32))
+    lit = oracle.prove_literal(log_size, c, 2, 9, pub, rounds)
+    assert lit == oracle.prove(log_size, oracle.fft_evaluate(log_size, c), 2, 9, pub, rounds).proof
+    assert oracle.verify(lit, pub)
+
+
+def test_literal_builder_golden_log10(oracle, golden):
+    v = golden["bench_codeword_prover_log10"]
+    x, y = G.bench_codeword_polynomial(1 << 10)
+    proof = oracle.prove_literal(10, oracle.fft_basis_coefficients(10, x, y), 2, 4, bytes(0xA0 + i for i in range(32)), 3)
+    assert oracle.sha3_256(proof).hex() == v["proof_hex"]
