@@ -28,11 +28,14 @@ from ._capi import (  # noqa: E402,F401
 from .plans import (  # noqa: E402,F401
     BatchProver,
     CircleCodewordPlan,
+    CircleFRIResidentQueryExtractor,
     CirclePCSFRIProver,
     CircleWitnessToFFTBasisPlan,
     Context,
     ProofServer,
     KeccakF1600PermutationPlan,
+    QM31FRIFoldChainPlan,
+    QM31FRIFoldPlan,
     SHA3FixedOneBlockHashPlan,
     SHA3RawLeavesMerkleCommitPlan,
     circle_domain_points,

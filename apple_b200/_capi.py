@@ -38,7 +38,16 @@ class Stats(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     _fields_ = [("treelet_log", ctypes.c_uint32), ("group_log", ctypes.c_uint32), ("threads", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
-                ("layer_treelet", ctypes.c_uint8 * 32)]
+                ("layer_treelet", ctypes.c_uint8 * 32), ("layer_threads", ctypes.c_uint16 * 32)]
+
+
+class TunerCandidate(ctypes.Structure):
+    _fields_ = [("tile_log", ctypes.c_uint32), ("group_log", ctypes.c_uint32), ("threads", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class TunerMeasurement(ctypes.Structure):
+    _fields_ = [("median_gpu_s", ctypes.c_double), ("p95_gpu_s", ctypes.c_double), ("median_submit_s", ctypes.c_double),
+                ("passed_gate", ctypes.c_uint32), ("runs", ctypes.c_uint32)]
 
 
 def library_path() -> str:
@@ -104,6 +113,27 @@ PROTOTYPES = {
     "azk_qm31_transcript_challenges": (I32, [P, U64, P, U32, P]),
     "azk_circle_merkle_fold_chain": (I32, [P, U32, P, U32, U32, U32, P, U32, P, P, P, STATS]),
     "azk_check_canonical": (I32, [P, P, U64, U32P]),
+    "azk_qm31_fold_plan_create": (I32, [P, U64, PP]),
+    "azk_qm31_fold_plan_execute": (I32, [P, P, P, P, P, STATS]),
+    "azk_qm31_fold_plan_execute_resident": (I32, [P, P, U64, P, U64, P, U64, P, STATS]),
+    "azk_qm31_fold_plan_clear": (I32, [P]),
+    "azk_qm31_fold_plan_destroy": (None, [P]),
+    "azk_fold_chain_plan_create": (I32, [P, U64, U32, PP]),
+    "azk_fold_chain_plan_info": (I32, [P, U64P, U64P, U64P]),
+    "azk_fold_chain_plan_execute": (I32, [P, P, P, P, P, STATS]),
+    "azk_fold_chain_plan_execute_resident": (I32, [P, P, U64, P, U64, P, U64, P, STATS]),
+    "azk_fold_chain_plan_execute_transcript": (I32, [P, P, P, P, P, P, STATS]),
+    "azk_fold_chain_plan_execute_transcript_resident": (I32, [P, P, U64, P, U64, P, U64, U64, P, U64, STATS]),
+    "azk_fold_chain_plan_execute_merkle": (I32, [P, P, P, P, P, P, STATS]),
+    "azk_fold_chain_plan_execute_merkle_readback": (I32, [P, P, U64, P, U64, P, P, P, STATS]),
+    "azk_fold_chain_plan_execute_merkle_resident": (I32, [P, P, U64, P, U64, P, U64, U64, P, U64, P, U64, P, U64, STATS]),
+    "azk_fold_chain_plan_challenges": (I32, [P, P]),
+    "azk_fold_chain_plan_clear": (I32, [P]),
+    "azk_fold_chain_plan_destroy": (None, [P]),
+    "azk_query_extractor_create": (I32, [P, U32, U32, PP]),
+    "azk_query_extractor_query_bytes": (U64, [U32, U32]),
+    "azk_query_extractor_extract": (I32, [P, P, U64, P, P, U64, P, U64P, STATS]),
+    "azk_query_extractor_destroy": (None, [P]),
     "azk_pcs_prover_create": (I32, [P, U32, U32, U32, U32, U32, SCHED, PP]),
     "azk_pcs_proof_size": (U64, [U32, U32, U32, U32, U32]),
     "azk_pcs_prover_prove_evaluations": (I32, [P, P, P, P, U64, P, U64P, STATS]),
@@ -137,8 +167,11 @@ PROTOTYPES = {
     "azk_server_release": (I32, [P, U64]),
     "azk_server_wait_all": (I32, [P]),
     "azk_server_stats": (I32, [P, U64P, U64P, ctypes.POINTER(ctypes.c_double), U64P]),
+    "azk_server_group_stats": (I32, [P, U64P, U64P]),
     "azk_server_destroy": (None, [P]),
     "azk_tuner_time_tree": (I32, [P, U32, U32, U32, U32, U32, U32, U32, U32, ctypes.POINTER(ctypes.c_double)]),
+    "azk_tuner_race_tree": (I32, [P, U32, U32, U32, U32, P, U32, U32, U32, U64, P, U32P]),
+    "azk_tuner_validate_tree": (I32, [P, U32, U32, U32, U32, P, U32, U64]),
     "azk_mlp_create": (I32, [P, U32, P, U64, PP]),
     "azk_mlp_param_count": (U64, [P]),
     "azk_mlp_get_params": (I32, [P, P, U64]),

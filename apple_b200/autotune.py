@@ -80,6 +80,97 @@ def collect(ctx, shapes=None, threads=THREADS, reps=3, progress=None) -> list:
 
 
 # ---------------------------------------------------------------------------
+# correctness-gated race and randomized validation (the reference's planner:
+# Planner/MetalProofPlanner.swift:224-269 races candidates behind a CPU gate,
+# :367-418 measures each one, :447-484 validates the winner on fresh inputs)
+# ---------------------------------------------------------------------------
+def race(ctx, shape, candidates, warmup=1, runs=5, seed=1):
+    """Race schedules [(tile, threads), ...] for shape (log, leaf bytes, fold, trees).
+    Each candidate commits a seeded random input whose roots the host computes;
+    one that differs is dropped untimed.  Returns (measurements, index of the
+    winner): per candidate {tile, threads, passed_gate, median_gpu_s, p95_gpu_s,
+    median_submit_s, runs}."""
+    lg, lb, fold, c = shape
+    arr = (_capi.TunerCandidate * len(candidates))(*[_capi.TunerCandidate(t, t, th, 0) for t, th in candidates])
+    out = (_capi.TunerMeasurement * len(candidates))()
+    win = ctypes.c_uint32()
+    check(lib().azk_tuner_race_tree(ctx.handle, lg, lb, 1 if fold else 0, c, arr, len(candidates), warmup, runs, seed, out, ctypes.byref(win)),
+          ctx.handle)
+    ms = [{"tile": t, "threads": th, "passed_gate": bool(m.passed_gate), "median_gpu_s": m.median_gpu_s, "p95_gpu_s": m.p95_gpu_s,
+           "median_submit_s": m.median_submit_s, "runs": m.runs} for (t, th), m in zip(candidates, out)]
+    return ms, int(win.value)
+
+
+def validate(ctx, shape, schedule, batches=3, seed=7):
+    """Commit `batches` fresh seeded inputs with `schedule` and compare each root
+    with the host's; raises AZKError(correctnessValidationFailed) on a mismatch."""
+    lg, lb, fold, c = shape
+    t, th = schedule
+    cand = _capi.TunerCandidate(t, t, th, 0)
+    check(lib().azk_tuner_validate_tree(ctx.handle, lg, lb, 1 if fold else 0, c, ctypes.byref(cand), batches, seed), ctx.handle)
+
+
+class PlanStore:
+    """Persisted race winners and live drift, the reference's plan database
+    (Planner/PlanDatabase.swift) as a JSON file: a record per shape (winner, median
+    device and submit time, p95, confidence) and an observation per shape that
+    keeps exponential moving averages of live timings; once enough samples drift
+    more than the threshold from the record, the shape is stale and is raced again
+    (recordLiveObservation, PlanDatabase.swift:192-236)."""
+
+    def __init__(self, path=None, alpha=0.2, min_samples=8, threshold=0.25):
+        self.path = path
+        self.alpha, self.min_samples, self.threshold = alpha, min_samples, threshold
+        self.records, self.observations = {}, {}
+        if path and os.path.exists(path):
+            with open(path) as f:
+                doc = json.load(f)
+            self.records = doc.get("records", {})
+            self.observations = doc.get("observations", {})
+
+    @staticmethod
+    def key(shape) -> str:
+        return "%d/%d/%d/%d" % tuple(int(v) for v in shape)
+
+    def record_race(self, shape, measurements, winner):
+        w = measurements[winner]
+        n = w["runs"]
+        self.records[self.key(shape)] = {"winner": [w["tile"], w["threads"]], "median_gpu_s": w["median_gpu_s"],
+                                         "median_submit_s": w["median_submit_s"], "p95_gpu_s": w["p95_gpu_s"],
+                                         "confidence": n / (n + 2.0), "candidates": len(measurements),
+                                         "failed_gate": sum(1 for m in measurements if not m["passed_gate"])}
+        self.observations.pop(self.key(shape), None)
+
+    def winner(self, shape):
+        r = self.records.get(self.key(shape))
+        return tuple(r["winner"]) if r else None
+
+    def record_live(self, shape, gpu_s, submit_s) -> dict:
+        """Fold one live timing into the shape's moving averages; returns
+        {"stale": bool, "samples", "relative_drift"}."""
+        rec = self.records.get(self.key(shape))
+        if rec is None:
+            raise KeyError("no race record for this shape")
+        o = self.observations.get(self.key(shape), {"samples": 0, "ema_gpu_s": None, "ema_submit_s": None})
+        ema = lambda prev, x: x if prev is None else self.alpha * x + (1 - self.alpha) * prev  # noqa: E731
+        o["samples"] += 1
+        o["ema_gpu_s"] = ema(o["ema_gpu_s"], gpu_s)
+        o["ema_submit_s"] = ema(o["ema_submit_s"], submit_s)
+        base = max(1e-12, rec["median_gpu_s"] + rec["median_submit_s"])
+        o["relative_drift"] = abs(o["ema_gpu_s"] + o["ema_submit_s"] - base) / base
+        o["stale"] = o["samples"] >= self.min_samples and o["relative_drift"] > self.threshold
+        self.observations[self.key(shape)] = o
+        return {"stale": o["stale"], "samples": o["samples"], "relative_drift": o["relative_drift"]}
+
+    def stale_shapes(self):
+        return [tuple(int(v) for v in k.split("/")) for k, o in self.observations.items() if o.get("stale")]
+
+    def save(self, path=None):
+        with open(path or self.path, "w") as f:
+            json.dump({"version": 1, "records": self.records, "observations": self.observations}, f, indent=1)
+
+
+# ---------------------------------------------------------------------------
 # features
 # ---------------------------------------------------------------------------
 SM_SLOTS = 148 * 2  # resident 256-thread CTAs of the commit kernel on a B200
@@ -237,6 +328,22 @@ class Tuner:
             timed.append((sec, (t, th)))
         return min(timed)[1]
 
+    def plan(self, shape, store: "PlanStore | None" = None, top: int = 4, runs: int = 5, batches: int = 3, seed: int = 1):
+        """A schedule for `shape` as the reference's planner makes one, with the model
+        in front: the model's `top` candidates race behind the correctness gate, the
+        winner is validated on `batches` fresh inputs, and the result is persisted in
+        `store`.  A stored winner whose live timings have not drifted is reused."""
+        if store is not None:
+            w = store.winner(shape)
+            if w is not None and tuple(shape) not in store.stale_shapes():
+                return w
+        cands = self.ranked(shape)[0][:top]
+        ms, win = race(self.ctx, shape, cands, runs=runs, seed=seed)
+        validate(self.ctx, shape, cands[win], batches=batches, seed=seed + 1)
+        if store is not None:
+            store.record_race(shape, ms, win)
+        return cands[win]
+
     def regret(self, shapes, verify: int = 0) -> dict:
         """Mean and max of (time of choice / best measured time - 1) over shapes,
         for the model and for the heuristic schedule."""
@@ -261,6 +368,18 @@ class Tuner:
             t, _ = self.choose((lg, leaf_bytes, fold, concurrent), threads=threads)
             table[lg] = int(t)
         return table
+
+    def layer_tables(self, concurrent=1, leaf_bytes=16, fold=1, logs=range(1, 27)):
+        """({layer log: treelet depth}, {layer log: threads}): the model's pick over
+        depth and threads per CTA for each layer size."""
+        tiles, threads = {}, {}
+        for lg in logs:
+            if lg < 2:
+                tiles[lg], threads[lg] = 1, 256
+                continue
+            t, th = self.choose((lg, leaf_bytes, fold, concurrent))
+            tiles[lg], threads[lg] = int(t), int(th)
+        return tiles, threads
 
     # persistence (the reference keeps a SQLite plan database; a JSON store here)
     def save(self, path):
@@ -299,10 +418,12 @@ TABLE_SHAPES = {
 
 def export(tuner: Tuner, report: dict, json_path: str, header_path: str):
     """Write the tables (and the evidence behind them) as JSON and as the C++ header
-    the library compiles in (`csrc/azk_tuned.h`)."""
-    tables = {name: tuner.layer_table(**kw) for name, kw in TABLE_SHAPES.items()}
-    doc = {"device": _device_name(tuner.ctx), "report": report, "threads": 256, "shapes": TABLE_SHAPES,
-           "tables": {k: {str(lg): t for lg, t in v.items()} for k, v in tables.items()}}
+    the library compiles in (`csrc/azk_tuned.h`): per layer size the treelet depth
+    and the threads per CTA the model picks."""
+    both = {name: tuner.layer_tables(**kw) for name, kw in TABLE_SHAPES.items()}
+    doc = {"device": _device_name(tuner.ctx), "report": report, "shapes": TABLE_SHAPES,
+           "tables": {k: {str(lg): t for lg, t in v[0].items()} for k, v in both.items()},
+           "thread_tables": {k: {str(lg): t for lg, t in v[1].items()} for k, v in both.items()}}
     with open(json_path, "w") as f:
         json.dump(doc, f, indent=1)
     with open(header_path, "w") as f:
@@ -314,7 +435,8 @@ def header_text(doc) -> str:
     lines = ["// Generated by `python -m apple_b200.autotune --export` from measured commit-kernel",
              "// timings on " + doc["device"] + f" ({doc['report'].get('records', 0)} records) and the cost model trained on them;",
              "// tests/test_tuned_tables.py keeps it equal to apple_b200/tuned_b200.json.",
-             "// Entry [k] = treelet depth for a layer of 2^k leaves (0: not used).",
+             "// Entry [k] = treelet depth (kTuned_*) and threads per CTA (kTunedThreads_*) for a layer",
+             "// of 2^k leaves (0: not used; the schedule's own value).",
              "#pragma once",
              "#include <stdint.h>",
              "",
@@ -323,6 +445,10 @@ def header_text(doc) -> str:
         tab = doc["tables"][name]
         vals = [int(tab.get(str(k), 0)) for k in range(32)]
         lines.append(f"static constexpr uint8_t kTuned_{name}[32] = {{{', '.join(str(v) for v in vals)}}};")
+    for name in TABLE_SHAPES:
+        tab = doc.get("thread_tables", {}).get(name, {})
+        vals = [int(tab.get(str(k), 0)) for k in range(32)]
+        lines.append(f"static constexpr uint16_t kTunedThreads_{name}[32] = {{{', '.join(str(v) for v in vals)}}};")
     lines += ["}  // namespace azk", ""]
     return "\n".join(lines)
 

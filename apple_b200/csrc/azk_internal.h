@@ -213,9 +213,28 @@ cudaError_t launch_witness_transform(const uint4* x, uint64_t count_x, const uin
 // QM31 values of each partial-sum buffer (px, py) the transform needs at capacity n.
 uint64_t witness_partial_values(uint64_t n);
 
-// `narrow`: the work items' inputs are lifted M31 polynomials (one-limb kernel).
-// `last`: the items are the low-stage (last) passes of their transforms.
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, bool last, cudaStream_t s);
+// FFT pass kernels.  kFftQM31: four-limb tiles (fft_pass_q_kernel); kFftM31Small:
+// one-limb transforms below 2^12 values, one pass (fft_pass_m31_kernel);
+// kFftM31Tile: one-limb passes of transforms of 2^12 or more that read the
+// coefficients or an earlier pass's exchange words (fft_m31_tile_kernel);
+// kFftM31Low: the low-stage last pass of one-limb transforms above 2^12, bulk-copied
+// tiles in a persistent kernel (fft_m31_low_tma_kernel), which raises *status when
+// a bounded wait on its copies runs out.
+enum FftKind : uint32_t { kFftQM31 = 0, kFftM31Small = 1, kFftM31Tile = 2, kFftM31Low = 3, kFftKinds = 4 };
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t kind, uint32_t* d_status, cudaStream_t s);
+cudaError_t prepare_fft_m31_kernels();
+cudaError_t launch_fft_m31_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
+cudaError_t launch_fft_m31_low(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t* d_status, cudaStream_t s);
+// Which kernel runs pass `pass` of a transform of 2^logn values, and how many
+// work items (tiles) it has.
+inline uint32_t fft_pass_kind(uint32_t logn, uint32_t pass, bool narrow) {
+  if (!narrow) return kFftQM31;
+  if (logn < kFftLowBits) return kFftM31Small;
+  return (pass == fft_high_chunks(logn) && pass > 0) ? kFftM31Low : kFftM31Tile;
+}
+inline uint64_t fft_kind_tiles(uint32_t logn, uint32_t pass, uint32_t kind) {
+  return (kind == kFftM31Tile || kind == kFftM31Low) ? (1ull << (logn - kFftLowBits)) : fft_pass_tiles(logn, pass);
+}
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets
 // info = {1, 0, count} first).
@@ -236,6 +255,8 @@ cudaError_t launch_pcs_finalize(PcsInstance* d_inst, const uint32_t* d_ids, uint
 cudaError_t launch_pcs_grind(PcsInstance* d_inst, uint32_t id, uint64_t start, uint64_t count, unsigned long long* d_found, cudaStream_t s);
 cudaError_t launch_pcs_queries(PcsInstance* d_inst, const uint32_t* d_ids, uint32_t nids, cudaStream_t s);
 cudaError_t launch_pcs_emit(PcsInstance* d_inst, const uint32_t* d_ids, uint32_t nids, uint32_t max_queries, cudaStream_t s);
+// Encoded queries (proof codec layout) of one instance's resident layers and trees.
+cudaError_t launch_query_extract(const PcsInstance* d_inst, const uint32_t* d_pairs, uint32_t count, uint8_t* d_out, cudaStream_t s);
 cudaError_t launch_qm31_transcript_prefix(Transcript* d_t, uint64_t input_count, uint32_t rounds, cudaStream_t s);
 cudaError_t launch_transcript_rounds_given(Transcript* d_t, uint32_t kind, const uint64_t* d_roots, uint32_t rounds, uint64_t input_count,
                                            uint32_t* d_ch, cudaStream_t s);

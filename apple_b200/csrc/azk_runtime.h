@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <chrono>
 #include <cstring>
 #include <map>
@@ -197,6 +198,19 @@ inline void fill_stats(azk_stats* st, const Timer& t, uint64_t submit_ns, double
   st->cpu_submit_ns = submit_ns;
 }
 
+// Resident entry points take (device pointer, byte offset) pairs.  This checks
+// that [p + off, p + off + bytes) lies inside the one device allocation containing
+// p + off (the reference's buffer-length check, e.g. QM31FRIFold.swift:1236-1244),
+// failing with AZK_ERR_INVALID_INPUT_LAYOUT otherwise or when the address is not
+// device memory.
+void require_device_range(const void* p, uint64_t off, uint64_t bytes);
+// Two byte ranges of device memory overlap (the reference's rangesOverlap on one
+// buffer, QM31FRIFold.swift:1280-1294; distinct allocations never overlap).
+inline bool ranges_overlap(const void* a, uint64_t aoff, uint64_t abytes, const void* b, uint64_t boff, uint64_t bbytes) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a) + aoff, y = reinterpret_cast<uintptr_t>(b) + boff;
+  return x < y + bbytes && y < x + abytes;
+}
+
 // Domain tables of size 2^logn, materialised once per context.
 const azk_ctx::Domain& domain_tables(azk_ctx* ctx, uint32_t logn);
 
@@ -207,10 +221,14 @@ struct Sched {
   uint32_t threads = 256;
   bool graph = true;
   uint8_t layer_tile[32] = {0};
+  uint16_t layer_threads[32] = {0};
 };
 // A schedule with no treelet depth and no layer table takes `defaults` (a tuned
-// per-layer table from azk_tuned.h) when one is given.
-Sched resolve_schedule(const azk_schedule* s, const uint8_t* defaults = nullptr);
+// per-layer table from azk_tuned.h) when one is given, and with no thread count
+// and no per-layer threads `default_threads` likewise.
+Sched resolve_schedule(const azk_schedule* s, const uint8_t* defaults = nullptr, const uint16_t* default_threads = nullptr);
+// Threads per CTA of the commit kernel for a layer of 2^logn leaves.
+inline uint32_t tree_threads(const Sched& s, uint32_t logn) { return (logn < 32 && s.layer_threads[logn]) ? s.layer_threads[logn] : s.threads; }
 // Tile depth used for a tree of 2^logn leaves under a schedule (per-layer table
 // first, then the global depth), clamped to [1, logn].
 inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
@@ -222,24 +240,31 @@ inline uint32_t tree_tile_log(const Sched& s, uint32_t logn) {
 
 // FFT work for a set of transforms: one FftJob per (transform, pass); passes of
 // all transforms are aligned so every transform's last (low-stage) pass runs at
-// the final step.  Transforms flagged `narrow` (inputs known to be lifted M31
-// polynomials) run on the one-limb kernel: in each step their work items follow
-// the QM31 items, so each kernel gets one contiguous range.
+// the final step.  Inside a step the work items are grouped by pass kernel
+// (FftKind: QM31 tiles, small one-limb transforms, one-limb tiles, bulk-copied
+// one-limb low passes), each group one contiguous range and one launch.
+// Transforms flagged `narrow` (inputs known to be lifted M31 polynomials) take the
+// one-limb kernels.
 struct FftPlan {
   std::vector<FftJob> jobs;
-  std::vector<uint2> work;                       // all steps, step-major, transform-contiguous
-  std::vector<uint64_t> step_off, step_cnt;      // per step: QM31 items
-  std::vector<uint64_t> nstep_off, nstep_cnt;    // per step: one-limb items
-  std::vector<uint8_t> narrow;                   // per transform
+  std::vector<uint2> work;  // all steps, step-major, kind-major, transform-contiguous
+  std::vector<std::array<uint64_t, kFftKinds>> part_off, part_cnt;  // per step and kind
+  std::vector<uint8_t> narrow;                                      // per transform
   std::vector<std::vector<std::pair<uint64_t, uint64_t>>> inst_range;  // [step][transform] -> (offset, count)
+  std::vector<std::vector<uint8_t>> inst_kind;                         // [step][transform] -> FftKind
   DevBuf d_jobs, d_work;
+  DevBuf d_status;  // raised by a pass kernel whose bounded wait ran out
+  size_t steps() const { return part_off.size(); }
   void build(const std::vector<FftJob>& transforms, const std::vector<uint8_t>& narrow_flags = {});
   void upload(cudaStream_t s);
   void launch_step(size_t step, cudaStream_t s) const;
   void launch_step_for(size_t step, size_t t, cudaStream_t s) const;
   void launch_all(cudaStream_t s) const {
-    for (size_t k = 0; k < step_cnt.size(); k++) launch_step(k, s);
+    for (size_t k = 0; k < steps(); k++) launch_step(k, s);
   }
+  // After the stream has finished the passes: fails with AZK_ERR_DEVICE_TIMEOUT (and
+  // clears the flag) when a pass kernel gave up waiting for its tile copies.
+  void check_status(cudaStream_t s);
 };
 
 // Monomial -> interleaved circle FFT-basis coefficients, host-side like the

@@ -433,116 +433,29 @@ static constexpr size_t kFftSmemM31 = (size_t)4 * (kFftTilePadded + kFftTileMax)
 static constexpr int kFftThreadsQ = 512;
 static constexpr int kFftThreadsM31 = 256;
 
-// Low-stage (last) passes of one-limb transforms, persistent: each CTA walks the
-// work list with a stride of the grid and prefetches its next tile's values and
-// stage twiddles into a second pair of shared buffers with cp.async while it
-// computes the current tile, so the loads run under the butterflies instead of
-// stalling every warp before them (16 x log 22: 2.36 -> 2.82 TB/s for the whole
-// transform).  The high-stage passes are bound by instruction issue instead; there
-// the double buffers' smaller occupancy (3 instead of 5 CTAs per SM) measured
-// slower (2.56 TB/s), so they keep fft_pass_m31_kernel.
-__device__ __forceinline__ void cp_async4(uint32_t* dst, const void* src, uint32_t src_bytes) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-template <int THREADS>
-__device__ __forceinline__ void fft_m31_prefetch(const FftJob* __restrict__ jobs, uint2 w, uint32_t* sv, uint32_t* stw) {
-  const FftJob& job = jobs[w.x];
-  const FftTile ft = fft_tile(job);
-  const FftPassGeom& g = ft.g;
-  const uint64_t gstep = (uint64_t)(THREADS >> g.c) << g.s_lo;
-  uint64_t gi = fft_global_index(g, w.y, threadIdx.x);
-  if (ft.first) {
-    // the a limbs of the nonzero prefix, zeros past it
-    const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
-    for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) {
-      const bool live = gi < ft.count;
-      cp_async4(sv + fpad(L), in_a + 4 * (live ? gi : 0), live ? 4u : 0u);
-    }
-  } else {
-    for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) cp_async4(sv + fpad(L), job.narrow + gi, 4u);
-  }
-  // stage j's 2^(m-1-j) twiddles of this tile sit at stw + 2^m - 2^(m-j): entry q
-  // belongs to the stage j with 2^(m-1-j) <= 2^m - 1 - q < 2^(m-j)
-  const uint32_t M = 1u << g.m;
-  const uint32_t midbits = g.s_lo > g.c ? g.s_lo - g.c : 0;
-  const uint64_t hi = (uint64_t)w.y >> midbits;
-  for (uint32_t q = threadIdx.x; q + 1 < M; q += THREADS) {
-    const uint32_t j = g.m - 1 - (31 - __clz(M - 1 - q));
-    const uint32_t r = q - (M - (M >> j));
-    cp_async4(stw + q, job.tw + tw_offset(job.logn, g.s_lo + j) + (hi << (g.m - 1 - j)) + r, 4u);
-  }
-}
-
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) fft_m31_persistent_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work, uint32_t nwork) {
-  extern __shared__ uint32_t lsm[];
-  constexpr uint32_t kBuf = kFftTilePadded + kFftTileMax;  // values (padded) + twiddles
-  uint32_t item = blockIdx.x;
-  if (item >= nwork) return;
-  fft_m31_prefetch<THREADS>(jobs, work[item], lsm, lsm + kFftTilePadded);
-  cp_async_commit();
-  for (uint32_t b = 0; item < nwork; item += gridDim.x, b ^= 1u) {
-    const uint32_t next = item + gridDim.x;
-    uint32_t* nbuf = lsm + (b ^ 1u) * kBuf;
-    if (next < nwork) fft_m31_prefetch<THREADS>(jobs, work[next], nbuf, nbuf + kFftTilePadded);
-    cp_async_commit();
-    cp_async_wait_one();  // this thread's copies of the current tile have landed
-    __syncthreads();      // ... and every other thread's
-    const uint2 w = work[item];
-    const FftJob& job = jobs[w.x];
-    const FftTile ft = fft_tile(job);
-    uint32_t* sv = lsm + b * kBuf;
-    fft_m31_tile_stages<THREADS>(sv, sv + kFftTilePadded, ft.g, ft.T, ft.top_zero);
-    const uint64_t gstep = (uint64_t)(THREADS >> ft.g.c) << ft.g.s_lo;
-    uint64_t gi = fft_global_index(ft.g, w.y, threadIdx.x);
-    if (ft.last) {
-      for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) job.out[gi] = make_uint4(sv[fpad(L)], 0u, 0u, 0u);
-    } else {
-      for (uint32_t L = threadIdx.x; L < ft.T; L += THREADS, gi += gstep) job.narrow[gi] = sv[fpad(L)];
-    }
-    __syncthreads();  // the next iteration prefetches into this buffer
-  }
-}
-
-static constexpr size_t kFftSmemPersistent = 2 * kFftSmemM31;  // two buffers of values + twiddles
-// Resident CTAs of the persistent kernel, per device (contexts on different devices
-// size their grids from their own SM counts).
-static constexpr int kFftMaxDevices = 64;
-static uint32_t g_fft_m31_grid[kFftMaxDevices] = {0};
-
 cudaError_t prepare_fft_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fft_pass_q_kernel<kFftThreadsQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemQ);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(fft_pass_m31_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemM31);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(fft_m31_persistent_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemPersistent);
-  if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0, per_sm = 0;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_m31_persistent_kernel<kFftThreadsM31>, kFftThreadsM31, kFftSmemPersistent)) !=
-      cudaSuccess)
-    return e;
-  if (dev >= 0 && dev < kFftMaxDevices) g_fft_m31_grid[dev] = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
-  return cudaSuccess;
+  return prepare_fft_m31_kernels();
 }
 
-cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, bool narrow, bool last, cudaStream_t s) {
+cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t kind, uint32_t* d_status, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
-  if (narrow && last) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kFftMaxDevices) dev = 0;
-    const uint32_t resident = g_fft_m31_grid[dev];
-    const uint32_t grid = resident && resident < nwork ? resident : nwork;
-    fft_m31_persistent_kernel<kFftThreadsM31><<<grid, kFftThreadsM31, kFftSmemPersistent, s>>>(d_jobs, d_work, nwork);
-  } else if (narrow) {
-    fft_pass_m31_kernel<kFftThreadsM31><<<nwork, kFftThreadsM31, kFftSmemM31, s>>>(d_jobs, d_work);
-  } else {
-    fft_pass_q_kernel<kFftThreadsQ><<<nwork, kFftThreadsQ, kFftSmemQ, s>>>(d_jobs, d_work);
+  switch (kind) {
+    case kFftQM31:
+      fft_pass_q_kernel<kFftThreadsQ><<<nwork, kFftThreadsQ, kFftSmemQ, s>>>(d_jobs, d_work);
+      break;
+    case kFftM31Small:
+      fft_pass_m31_kernel<kFftThreadsM31><<<nwork, kFftThreadsM31, kFftSmemM31, s>>>(d_jobs, d_work);
+      break;
+    case kFftM31Tile:
+      return launch_fft_m31_tiles(d_jobs, d_work, nwork, s);
+    case kFftM31Low:
+      return launch_fft_m31_low(d_jobs, d_work, nwork, d_status, s);
+    default:
+      return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
@@ -805,6 +718,30 @@ __device__ uint64_t pcs_write_opening(const PcsInstance& I, uint32_t k, uint64_t
   return opening_bytes(depth);
 }
 
+// One query (CircleFRIQueryV1 encoding: initial pair, layer count, then per layer
+// its index, pair index and the left and right value openings) at byte `qoff` of
+// `b`; the block's threads split the layers' openings.
+__device__ void emit_query(const PcsInstance& I, uint64_t pair, uint8_t* b, uint64_t qoff) {
+  const uint32_t R = I.rounds;
+  if (threadIdx.x == 0) {
+    pw64(b, qoff, pair);
+    pw32(b, qoff + 8, R);
+  }
+  // thread (k, side) writes layer k's left (side 0) or right opening
+  for (uint32_t t = threadIdx.x; t < 2 * R; t += blockDim.x) {
+    uint32_t k = t >> 1, side = t & 1;
+    uint64_t off = qoff + 12;
+    for (uint32_t j = 0; j < k; j++) off += 12 + 2 * opening_bytes(I.logn - j);
+    uint64_t pk = pair >> k;
+    if (side == 0) {
+      pw32(b, off, k);
+      pw64(b, off + 4, pk);
+    }
+    uint64_t oo = off + 12 + (side ? opening_bytes(I.logn - k) : 0);
+    pcs_write_opening(I, k, 2 * pk + side, b, oo);
+  }
+}
+
 __global__ void pcs_emit_kernel(const PcsInstance* __restrict__ inst, const uint32_t* __restrict__ ids, uint32_t max_queries) {
   const PcsInstance& I = inst[ids[blockIdx.x]];
   uint8_t* b = I.proof;
@@ -814,25 +751,7 @@ __global__ void pcs_emit_kernel(const PcsInstance* __restrict__ inst, const uint
   const uint64_t qbytes = proof_query_bytes(I.logn, R);
   const uint32_t q = blockIdx.y;
   if (q < I.queries) {
-    uint64_t qoff = hdr + (uint64_t)q * qbytes;
-    uint64_t pair = I.query_pairs[q];
-    if (threadIdx.x == 0) {
-      pw64(b, qoff, pair);
-      pw32(b, qoff + 8, R);
-    }
-    // thread (k, side) writes layer k's left (side 0) or right opening
-    for (uint32_t t = threadIdx.x; t < 2 * R; t += blockDim.x) {
-      uint32_t k = t >> 1, side = t & 1;
-      uint64_t off = qoff + 12;
-      for (uint32_t j = 0; j < k; j++) off += 12 + 2 * opening_bytes(I.logn - j);
-      uint64_t pk = pair >> k;
-      if (side == 0) {
-        pw32(b, off, k);
-        pw64(b, off + 4, pk);
-      }
-      uint64_t oo = off + 12 + (side ? opening_bytes(I.logn - k) : 0);
-      pcs_write_opening(I, k, 2 * pk + side, b, oo);
-    }
+    emit_query(I, I.query_pairs[q], b, hdr + (uint64_t)q * qbytes);
     return;
   }
   if (q != max_queries) return;
@@ -892,6 +811,20 @@ cudaError_t launch_pcs_emit(PcsInstance* d_inst, const uint32_t* d_ids, uint32_t
   if (!nids) return cudaSuccess;
   dim3 grid(nids, max_queries + 1);
   pcs_emit_kernel<<<grid, 64, 0, s>>>(d_inst, d_ids, max_queries);
+  return cudaGetLastError();
+}
+
+// Queries of committed resident layers (CircleFRIResidentQueryExtractorV1.extractQueries,
+// CircleFRIFoldPlan.swift:1065-1148): block q writes query q, openings read from
+// the layers and their resident trees, at byte q * (bytes per query) of `out`.
+__global__ void query_extract_kernel(const PcsInstance* __restrict__ inst, const uint32_t* __restrict__ pairs, uint8_t* __restrict__ out) {
+  const PcsInstance& I = *inst;
+  emit_query(I, pairs[blockIdx.x], out, (uint64_t)blockIdx.x * proof_query_bytes(I.logn, I.rounds));
+}
+
+cudaError_t launch_query_extract(const PcsInstance* d_inst, const uint32_t* d_pairs, uint32_t count, uint8_t* d_out, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  query_extract_kernel<<<count, 64, 0, s>>>(d_inst, d_pairs, d_out);
   return cudaGetLastError();
 }
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <condition_variable>
 #include <deque>
+#include <set>
 #include <thread>
 #include <unordered_map>
 
@@ -20,6 +21,7 @@
 #include "azk_tuned.h"
 
 namespace azk {
+// sumcheck_kernels.cu
 struct SumcheckOut {
   uint32_t claimed_sum;
   uint32_t final_eval;
@@ -28,7 +30,15 @@ struct SumcheckOut {
   uint32_t* r1;
   uint32_t* challenges;
 };
+struct SumcheckJob {
+  const uint32_t* evals;
+  uint32_t* scratch;
+  SumcheckOut* out;
+  uint32_t log_n;
+  uint32_t pad;
+};
 cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s);
+cudaError_t launch_sumcheck_batch(const SumcheckJob* d_jobs, uint32_t count, cudaStream_t s);
 }  // namespace azk
 
 using namespace azk;
@@ -73,6 +83,7 @@ struct Engine {
   std::vector<uint64_t> tstep_off, tstep_cnt;
   std::vector<std::vector<std::pair<uint64_t, uint64_t>>> tstep_inst;  // [step][inst]
   std::vector<uint32_t> tstep_tile;                                     // max tile log per step
+  std::vector<uint32_t> tstep_log;                                      // largest layer log per step
   std::vector<FoldJob> fold_jobs;
   std::vector<uint2> fold_work;
   std::vector<uint64_t> fstep_off, fstep_cnt;
@@ -141,14 +152,17 @@ struct Engine {
   // Gate and describe the uploaded coefficients (the caller queued their copies
   // on s_up): canonicality, the lifted-M31 flag and zeros over each tail
   // [counts[i], N) in one launch on s_up, then one small readback.
+  // `counts` covers the first counts.size() instances (a server group runs a prefix
+  // of its engine's instances).
   void scan_inputs(const std::vector<uint64_t>& counts) {
-    std::vector<InputInfo> h(cfg.size());
-    for (size_t i = 0; i < cfg.size(); i++) h[i] = InputInfo{1u, 0u, counts[i]};
+    const size_t m = counts.size();
+    std::vector<InputInfo> h(m);
+    for (size_t i = 0; i < m; i++) h[i] = InputInfo{1u, 0u, counts[i]};
     AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s_up));
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s_up));
-    std::vector<ScanJob> jobs(cfg.size());
+    std::vector<ScanJob> jobs(m);
     uint64_t max_n = 0;
-    for (size_t i = 0; i < cfg.size(); i++) {
+    for (size_t i = 0; i < m; i++) {
       const uint64_t N = 1ull << cfg[i].logn;
       jobs[i] = ScanJob{arena.at<uint4>(off_input[i]), counts[i], N, d_info() + i};
       max_n = std::max(max_n, N);
@@ -161,8 +175,8 @@ struct Engine {
     AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s_up));
     sync_stream(s_up);
     layout(f == 0, "input contains a non-canonical field element");
-    std::vector<uint8_t> narrow(cfg.size());
-    for (size_t i = 0; i < cfg.size(); i++) narrow[i] = h[i].m31 ? 1 : 0;
+    std::vector<uint8_t> narrow(m);
+    for (size_t i = 0; i < m; i++) narrow[i] = h[i].m31 ? 1 : 0;
     set_fft_narrow(narrow);
   }
   // Inputs written by the caller through a device pointer: nothing known.
@@ -172,13 +186,14 @@ struct Engine {
     narrow[i] = 0;
     set_fft_narrow(narrow);
   }
-  // Which instances run the one-limb FFT kernel; a change rebuilds the FFT work
-  // lists and drops the captured graph (it is captured again on the next run).
+  // Which instances run the one-limb FFT kernel; `narrow` covers the transforms of
+  // the first narrow.size() instances (the FFT runs over those).  A change rebuilds
+  // the FFT work lists and drops the captured graph (captured again on the next run).
   void set_fft_narrow(const std::vector<uint8_t>& narrow) {
     if (narrow == fft_narrow) return;
     sync_stream(s);
     fft_narrow = narrow;
-    fft.build(fft_transforms, fft_narrow);
+    fft.build(std::vector<FftJob>(fft_transforms.begin(), fft_transforms.begin() + narrow.size()), fft_narrow);
     fft.upload(s);
     sync_stream(s);
     if (graph) cudaGraphExecDestroy(graph);
@@ -294,6 +309,7 @@ struct Engine {
     tstep_off.assign(rmax, 0);
     tstep_cnt.assign(rmax, 0);
     tstep_tile.assign(rmax, 1);
+    tstep_log.assign(rmax, 0);
     tstep_inst.assign(rmax, std::vector<std::pair<uint64_t, uint64_t>>(n, {0, 0}));
     fstep_off.assign(rmax + 1, 0);
     fstep_cnt.assign(rmax + 1, 0);
@@ -338,6 +354,7 @@ struct Engine {
         tstep_inst[k][i] = {tree_work.size(), tiles};
         for (uint64_t t = 0; t < tiles; t++) tree_work.push_back(make_uint2(jid, (uint32_t)t));
         tstep_tile[k] = std::max(tstep_tile[k], tl);
+        tstep_log[k] = std::max(tstep_log[k], lg);
       }
       tstep_cnt[k] = tree_work.size() - tstep_off[k];
     }
@@ -377,53 +394,75 @@ struct Engine {
       fold_bytes += 26 * (N >> (c2.rounds - 1));
     }
     launches = 0;
-    for (auto c3 : fft.step_cnt) launches += c3 ? 1 : 0;
+    for (auto& st : fft.part_cnt)
+      for (auto c3 : st) launches += c3 ? 1 : 0;
     for (auto c3 : tstep_cnt) launches += c3 ? 1 : 0;
     for (auto c3 : fstep_cnt) launches += c3 ? 1 : 0;
     launches += 4;  // prefix, finalize, queries, emit
-    ensure_events(fft.step_cnt.size() + 2 * rmax + 8);
+    ensure_events(fft.steps() + 2 * rmax + 8);
   }
 
   uint32_t tree_kind(uint32_t k) const {
     if (leaf_values == 4) return k == 0 ? kLeafQM31x4 : kLeafFoldx4;
     return k == 0 ? kLeafQM31 : kLeafFold;
   }
-  void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt) {
+  // `lg`: the largest layer (log leaves) the launch commits; its threads per CTA
+  void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt, uint32_t lg) {
     if (!cnt) return;
-    AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], tree_kind(k), sched.threads, s));
+    AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], tree_kind(k),
+                            tree_threads(sched, lg), s));
   }
+  uint32_t layer_log(uint32_t i, uint32_t k) const { return cfg[i].logn - k - (leaf_values == 4 ? 2 : 0); }
   void launch_fold_range(uint64_t off, uint64_t cnt) {
     if (!cnt) return;
     AZK_CU(launch_fold_jobs(d_fold_jobs.as<FoldJob>(), d_fold_work.as<uint2>() + off, (uint32_t)cnt, s));
   }
 
+  // Instances a batched run covers: all of them, or the first n_act of an engine
+  // whose instances all have one shape (a server group; its work lists are then
+  // instance-major, so the first n_act instances' items are a prefix of every step).
+  uint32_t n_act = 0;
+  uint32_t active() const { return n_act ? n_act : (uint32_t)cfg.size(); }
+  uint64_t tree_step_count(uint32_t k) const {
+    if (!n_act) return tstep_cnt[k];
+    uint64_t c = 0;
+    for (uint32_t i = 0; i < n_act; i++) c += tstep_inst[k][i].second;
+    return c;
+  }
+  uint64_t fold_step_count(uint32_t k) const {
+    if (!n_act) return fstep_cnt[k];
+    uint64_t c = 0;
+    for (uint32_t i = 0; i < n_act; i++) c += fstep_inst[k][i].second;
+    return c;
+  }
   // Everything up to (not including) grinding.  from_coeffs: run the FFT first.
   void enqueue_rounds_batched(bool from_coeffs) {
     ev_used = 0;
+    const uint32_t na = active();
     if (from_coeffs) {
-      for (size_t st = 0; st < fft.step_cnt.size(); st++) {
+      for (size_t st = 0; st < fft.steps(); st++) {
         prof_begin(0);
         fft.launch_step(st, s);
         prof_end();
       }
     }
     prof_begin(3);
-    AZK_CU(launch_pcs_prefix(d_inst(), (uint32_t)cfg.size(), s));
+    AZK_CU(launch_pcs_prefix(d_inst(), na, s));
     prof_end();
     for (uint32_t k = 0; k <= rmax; k++) {
       if (k < rmax) {
         prof_begin(1);
-        launch_tree_range(k, tstep_off[k], tstep_cnt[k]);
+        launch_tree_range(k, tstep_off[k], tree_step_count(k), n_act ? layer_log(0, k) : tstep_log[k]);
         prof_end();
       }
-      if (k >= 1 && fstep_cnt[k]) {
+      if (k >= 1 && fold_step_count(k)) {
         prof_begin(2);
-        launch_fold_range(fstep_off[k], fstep_cnt[k]);
+        launch_fold_range(fstep_off[k], fold_step_count(k));
         prof_end();
       }
     }
     prof_begin(3);
-    AZK_CU(launch_pcs_finalize(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
+    AZK_CU(launch_pcs_finalize(d_inst(), d_ids.as<uint32_t>(), na, s));
     prof_end();
   }
   // Proof bytes exist only for 16-byte leaves (the reference's verifier opens one
@@ -432,18 +471,18 @@ struct Engine {
   void enqueue_tail_batched() {
     if (!has_proofs()) return;
     prof_begin(3);
-    AZK_CU(launch_pcs_queries(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), s));
-    AZK_CU(launch_pcs_emit(d_inst(), d_ids.as<uint32_t>(), (uint32_t)cfg.size(), qmax, s));
+    AZK_CU(launch_pcs_queries(d_inst(), d_ids.as<uint32_t>(), active(), s));
+    AZK_CU(launch_pcs_emit(d_inst(), d_ids.as<uint32_t>(), active(), qmax, s));
     prof_end();
   }
   void enqueue_instance(uint32_t i, bool from_coeffs) {
     if (from_coeffs)
-      for (size_t st = 0; st < fft.step_cnt.size(); st++)
+      for (size_t st = 0; st < fft.steps(); st++)
         if (fft.inst_range[st][i].second) fft.launch_step_for(st, i, s);
     AZK_CU(launch_pcs_prefix(d_inst() + i, 1, s));
     const uint32_t* id = d_ids.as<uint32_t>() + i;
     for (uint32_t k = 0; k <= cfg[i].rounds; k++) {
-      if (k < cfg[i].rounds) launch_tree_range(k, tstep_inst[k][i].first, tstep_inst[k][i].second);
+      if (k < cfg[i].rounds) launch_tree_range(k, tstep_inst[k][i].first, tstep_inst[k][i].second, layer_log(i, k));
       if (k == cfg[i].rounds) launch_fold_range(fstep_inst[k][i].first, fstep_inst[k][i].second);
     }
     AZK_CU(launch_pcs_finalize(d_inst(), id, 1, s));
@@ -477,8 +516,9 @@ struct Engine {
   }
 
   void set_publics(const uint8_t* pubs) {
-    for (size_t i = 0; i < cfg.size(); i++) std::memcpy(h_inst[i].pub, pubs + 32 * i, 32);
-    AZK_CU(cudaMemcpy2DAsync(reinterpret_cast<uint8_t*>(d_inst()) + offsetof(PcsInstance, pub), sizeof(PcsInstance), pubs, 32, 32, cfg.size(),
+    const size_t na = active();
+    for (size_t i = 0; i < na; i++) std::memcpy(h_inst[i].pub, pubs + 32 * i, 32);
+    AZK_CU(cudaMemcpy2DAsync(reinterpret_cast<uint8_t*>(d_inst()) + offsetof(PcsInstance, pub), sizeof(PcsInstance), pubs, 32, 32, na,
                              cudaMemcpyHostToDevice, s));
   }
 
@@ -488,8 +528,8 @@ struct Engine {
     GpuTimer g(s);
     if (plain) {
       ev_used = 0;
-      for (uint32_t i = 0; i < cfg.size(); i++) enqueue_instance(i, from_coeffs);
-    } else if (!any_grinding && sched.graph && !prof) {
+      for (uint32_t i = 0; i < active(); i++) enqueue_instance(i, from_coeffs);
+    } else if (!any_grinding && sched.graph && !prof && !n_act) {
       // (profiled runs take the eager path below: the same launch sequence, with
       // event pairs around each stage)
       if (!graph || graph_from_coeffs != from_coeffs) {
@@ -507,7 +547,7 @@ struct Engine {
       AZK_CU(cudaGraphLaunch(graph, s));
     } else {
       enqueue_rounds_batched(from_coeffs);
-      for (uint32_t i = 0; i < cfg.size(); i++) grind_instance(i);
+      for (uint32_t i = 0; i < active(); i++) grind_instance(i);
       enqueue_tail_batched();
     }
     if (submit_ns) *submit_ns = t.ns();
@@ -580,7 +620,7 @@ azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t logn, uint32_t log_blowu
     p->queries = queries;
     p->log_blowup = log_blowup;
     p->grinding = grinding;
-    Sched sc = resolve_schedule(schedule, kTuned_pcs_single);
+    Sched sc = resolve_schedule(schedule, kTuned_pcs_single, kTunedThreads_pcs_single);
     sc.graph = false;
     p->eng.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
     *out = p.release();
@@ -604,6 +644,7 @@ static void pcs_prove_common(azk_pcs_prover* p, bool coeffs, const uint8_t pub[3
   e.set_publics(pub);
   uint64_t sub = 0;
   double gs = e.run(coeffs, true, &sub, t);
+  if (coeffs) e.fft.check_status(e.s);
   uint64_t len = e.proof_len[0];
   layout(*proof_len >= len, "proof buffer too small");
   *proof_len = len;
@@ -691,7 +732,7 @@ azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint3
     uint64_t N = 1ull << logn;
     Timer t;
     Engine e;
-    Sched sc = resolve_schedule(nullptr, kTuned_pcs_single);
+    Sched sc = resolve_schedule(nullptr, kTuned_pcs_single, kTunedThreads_pcs_single);
     sc.graph = false;
     e.init(ctx, {InstanceCfg{logn, rounds, queries, log_blowup, grinding, {}}}, sc);
     AZK_CU(cudaMemcpyAsync(e.h_inst[0].layers, ev, 16 * N, cudaMemcpyHostToDevice, e.s));
@@ -700,7 +741,7 @@ azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t logn, const uint3
     GpuTimer g(e.s);
     AZK_CU(launch_pcs_prefix(e.d_inst(), 1, e.s));
     for (uint32_t k = 0; k <= rounds; k++) {
-      if (k < rounds) e.launch_tree_range(k, e.tstep_inst[k][0].first, e.tstep_inst[k][0].second);
+      if (k < rounds) e.launch_tree_range(k, e.tstep_inst[k][0].first, e.tstep_inst[k][0].second, e.layer_log(0, k));
       if (k == rounds) e.launch_fold_range(e.fstep_inst[k][0].first, e.fstep_inst[k][0].second);
     }
     g.stop();
@@ -723,7 +764,7 @@ azk_status azk_batch_create_leaves(azk_ctx* ctx, uint32_t count, const uint32_t*
     }
     auto b = std::make_unique<azk_batch>();
     b->ctx = ctx;
-    b->eng.init(ctx, cf, resolve_schedule(schedule, kTuned_pcs_batch));
+    b->eng.init(ctx, cf, resolve_schedule(schedule, kTuned_pcs_batch, kTunedThreads_pcs_batch));
     *out = b.release();
   });
 }
@@ -771,6 +812,7 @@ azk_status azk_batch_prove(azk_batch* b, const uint8_t* pubs, int plain, azk_sta
     uint64_t sub = 0;
     double gs = e.run(true, plain != 0, &sub, t);
     sync_stream(e.s);
+    e.fft.check_status(e.s);
     fill_stats(st, t, sub, gs);
   });
 }
@@ -846,17 +888,27 @@ void azk_batch_destroy(azk_batch* b) { delete b; }
 // Continuous-batching server
 //
 // Jobs (Circle PCS commit-and-fold proofs and M31 multilinear sum-checks) enter
-// one FIFO queue.  `slots` worker threads each own a CUDA stream; a worker takes
-// the next queued job as soon as its device memory fits the HBM budget, so jobs
-// that arrive while others run join the device as slots and memory free up and
-// their kernels overlap with the running ones.
+// one FIFO queue.  `slots` worker threads each own a CUDA stream.  A worker takes
+// the front job as soon as its device memory fits the HBM budget, so jobs that
+// arrive while others run join the device as slots and memory free up and their
+// kernels overlap with the running ones:
+//  - a PCS job is taken together with the other queued PCS jobs of its shape (up
+//    to the shape's group capacity), and the group is proved as one batched
+//    superstep on the worker's engine for that shape (one launch per stage over
+//    the group's instances);
+//  - a sum-check job is handed to the sum-check lane and the worker moves on: the
+//    lane proves the tables that are waiting in one batched launch (one CTA per
+//    table) on a few streams of its own, and a completion thread publishes each
+//    batch's results when its event fires, so a 2^20 table's tens of milliseconds
+//    of sequential digest never hold a worker.
 //
-// Device memory is per worker and per job shape (a PCS engine or a sum-check
-// table set), kept after the job for the next job of that shape: no allocation
-// or free (each of which waits for the whole device) sits between jobs once the
-// shapes have been seen.  Every byte held, in use or cached, counts against the
-// budget; a worker whose next job does not fit first gives back its own cached
-// shapes, least recently used first.
+// Device memory is per worker and per PCS shape (an engine with room for the
+// shape's group capacity), plus the lane's table slots and the context's domain
+// tables for each log size in use, all kept for later jobs: no allocation or free
+// (each of which waits for the whole device) sits between jobs once the shapes
+// have been seen.  Every byte held counts against the budget; to admit a job that
+// does not fit, the taking worker gives back its own least recently used shapes,
+// then those of idle workers.
 // ===========================================================================
 namespace {
 
@@ -868,72 +920,50 @@ struct ServeJob {
   uint64_t count = 0;           // pcs: coefficient count
   bool zeros = false;           // warm-up job: `count` zero coefficients, no `input`
   uint8_t pub[32] = {0};
-  uint64_t bytes = 0;  // device memory of its shape
   std::chrono::steady_clock::time_point submitted, started, finished;
   int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
   std::string error;
   std::vector<uint8_t> result;
 };
 
-using ShapeKey = std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t>;
+using ShapeKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>;  // PCS: logn, rounds, queries, log_blowup
 
-ShapeKey shape_of(const ServeJob& j) { return std::make_tuple(j.kind, j.logn, j.rounds, j.queries, j.log_blowup); }
+ShapeKey shape_of(const ServeJob& j) { return std::make_tuple(j.logn, j.rounds, j.queries, j.log_blowup); }
+
+// Jobs of one shape proved together, at most: 8 up to 2^17 values, then halving
+// (4 at 2^18, 2 at 2^19), one from 2^20 on, where one job already fills the GPU's
+// launches.
+uint32_t group_capacity(uint32_t logn) { return logn >= 20 ? 1u : logn >= 17 ? (1u << (20 - logn)) : 8u; }
+
+// Device bytes of one PCS instance: input 16N, layers 32N, trees 64N, tree
+// counters, transcript, proof; work lists and slack rounded into 8N.
+uint64_t pcs_instance_bytes(uint32_t logn, uint32_t rounds, uint32_t queries) {
+  const uint64_t N = 1ull << logn;
+  return 120 * N + proof_total_bytes(logn, rounds, queries, 0, false) + 4096;
+}
+uint64_t pcs_engine_bytes(uint32_t logn, uint32_t rounds, uint32_t queries, uint32_t cap) {
+  return cap * pcs_instance_bytes(logn, rounds, queries) + (64ull << 10);
+}
+// Domain tables of a log size (FFT twiddles and their inverses, N - 1 words each).
+uint64_t domain_bytes(uint32_t logn) { return 8ull << logn; }
 
 struct SumcheckBufs {
   DevBuf ev, scratch, rounds, out;
 };
+uint64_t sumcheck_table_bytes(uint32_t logn) { return (8ull << logn) + 12ull * logn + 4096; }
+uint64_t sumcheck_pinned_bytes(uint32_t logn) { return align_up(4ull << logn, 64) + sizeof(SumcheckOut) + 12ull * logn + 64; }
 
-// Device memory of one job shape held by a worker.
+// Device memory of one PCS shape held by a worker.
 struct Resident {
   std::unique_ptr<Engine> eng;
-  std::unique_ptr<SumcheckBufs> sc;
+  uint32_t cap = 1;
   uint64_t bytes = 0;
   uint64_t last_use = 0;
 };
 
-uint64_t pcs_shape_bytes(uint32_t logn, uint32_t rounds, uint32_t queries) {
-  uint64_t N = 1ull << logn;
-  // arena of one engine: input 16N, layers 32N, trees 64N, tree counters 2N,
-  // transcript and proof state; FFT work lists and slack rounded into 8N
-  return 120 * N + proof_total_bytes(logn, rounds, queries, 0, false) + (64ull << 10);
-}
-
-uint64_t sumcheck_shape_bytes(uint32_t logn) { return 8ull << logn | 4096; }
-
-}  // namespace
-
-struct azk_server {
-  azk_ctx* ctx;
-  Sched sched;
-  uint64_t budget;
-  uint32_t slots;
-  std::mutex mu;
-  std::condition_variable cv, done_cv;
-  std::deque<std::shared_ptr<ServeJob>> queue;
-  std::unordered_map<uint64_t, std::shared_ptr<ServeJob>> jobs;
-  uint64_t next_id = 1;
-  uint64_t held = 0;  // device bytes held by all workers (in use and cached)
-  uint64_t running = 0;
-  uint64_t tick = 0;
-  bool stop = false;
-  std::vector<std::map<ShapeKey, Resident>> cache;  // per worker
-  std::vector<uint8_t> busy;                         // per worker: running a job (its cache must stay)
-  // per worker: jobs of zeros it runs once before serving (azk_server_warm), so its
-  // engines, sum-check buffers and pinned staging exist before the first real job
-  std::vector<std::deque<std::shared_ptr<ServeJob>>> warm;
-  uint64_t warm_pending = 0;
-  std::vector<cudaStream_t> streams;  // one per worker
-  std::vector<std::thread> workers;
-  uint64_t completed = 0, elems = 0;
-  std::chrono::steady_clock::time_point first_submit, last_finish;
-  bool any_submit = false;
-};
-
-namespace {
-
-// Page-locked host staging of one worker: job inputs and results cross PCIe from
-// here (copies from pageable memory go through the driver's own staging, which
-// serialises the workers' copies).
+// Page-locked host staging: job inputs and results cross PCIe from here (copies
+// from pageable memory go through the driver's own staging, which serialises the
+// workers' copies).
 struct Staging {
   uint8_t* p = nullptr;
   size_t n = 0;
@@ -953,87 +983,174 @@ struct Staging {
   }
 };
 
-void run_pcs(azk_server* sv, Resident& r, ServeJob& j, Staging& st, cudaStream_t s) {
+// One table slot of the sum-check lane: device buffers for a table of up to
+// 2^cap_log words and page-locked staging for its input and results.
+struct SumcheckSlot {
+  SumcheckBufs bufs;
+  Staging pin;
+  uint32_t cap_log = 0;  // 0: not allocated
+  bool grow = false;     // cap_log was raised: the buffers are reallocated before use
+  std::shared_ptr<ServeJob> job;
+};
+// A lane stream and the batch it runs.
+struct SumcheckStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf jobs;
+  std::vector<int> slots;
+};
+constexpr int kLaneSlots = 96;    // tables in the lane at once
+constexpr int kLaneStreams = 6;   // batches in flight at once
+constexpr int kLaneBatch = 32;    // tables per launch
+
+}  // namespace
+
+struct azk_server {
+  azk_ctx* ctx;
+  Sched sched;
+  uint64_t budget;
+  uint32_t slots;
+  std::mutex mu;
+  std::condition_variable cv, done_cv, lane_cv;
+  std::deque<std::shared_ptr<ServeJob>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<ServeJob>> jobs;
+  uint64_t next_id = 1;
+  uint64_t held = 0;  // device bytes held (engines, lane slots, domain tables)
+  uint64_t running = 0;
+  uint64_t tick = 0;
+  bool stop = false, lane_stop = false;
+  std::vector<std::map<ShapeKey, Resident>> cache;  // per worker
+  std::vector<uint8_t> busy;                         // per worker: running a job (its cache must stay)
+  std::set<uint32_t> domain_logs;                    // log sizes whose domain tables are counted in `held`
+  // per worker: jobs of zeros it runs once before serving (azk_server_warm), so its
+  // engines and pinned staging exist before the first real job
+  std::vector<std::deque<std::shared_ptr<ServeJob>>> warm;
+  uint64_t warm_pending = 0;
+  std::vector<cudaStream_t> streams;  // one per worker
+  std::vector<std::thread> workers;
+  // sum-check lane
+  std::vector<std::unique_ptr<SumcheckSlot>> sc_slot;
+  std::vector<int> sc_free;     // slots without a table
+  std::deque<int> sc_pending;   // slots whose table waits for a launch
+  std::vector<SumcheckStream> sc_stream;
+  std::vector<int> sc_idle;     // lane streams without a batch
+  std::deque<int> sc_inflight;  // lane streams with a batch, in launch order
+  bool launcher_done = false;
+  std::thread sc_launcher, sc_completer;
+  uint64_t completed = 0, elems = 0, groups = 0, grouped = 0;
+  std::chrono::steady_clock::time_point first_submit, last_finish;
+  bool any_submit = false;
+};
+
+namespace {
+
+// Group capacity of a shape under the server's budget: halved until the engine
+// takes at most half the budget.
+uint32_t shape_capacity(const azk_server* sv, const ServeJob& j) {
+  uint32_t cap = group_capacity(j.logn);
+  while (cap > 1 && pcs_engine_bytes(j.logn, j.rounds, j.queries, cap) > sv->budget / 2) cap >>= 1;
+  return cap;
+}
+
+// Proves a group of same-shape PCS jobs on the worker's engine for the shape (made
+// on first use with room for the shape's capacity): inputs staged and copied, one
+// scan launch, one batched superstep over the group's instances, proofs read back.
+void run_pcs_group(azk_server* sv, Resident& r, std::vector<std::shared_ptr<ServeJob>>& g, Staging& st, cudaStream_t s) {
+  const ServeJob& j0 = *g[0];
   if (!r.eng) {
     r.eng = std::make_unique<Engine>();
     Sched sc = sv->sched;
     sc.graph = false;
-    r.eng->init(sv->ctx, {InstanceCfg{j.logn, j.rounds, j.queries, j.log_blowup, 0, {}}}, sc, s, s);
+    std::vector<InstanceCfg> cf(r.cap, InstanceCfg{j0.logn, j0.rounds, j0.queries, j0.log_blowup, 0, {}});
+    r.eng->init(sv->ctx, cf, sc, s, s);
   }
   Engine* e = r.eng.get();
-  const uint64_t in_bytes = 16 * j.count, proof = e->proof_len[0];
-  uint8_t* pin = st.ensure(std::max<uint64_t>(in_bytes, proof) + 64);
-  if (j.zeros)
-    std::memset(pin, 0, in_bytes);
-  else
-    std::memcpy(pin, j.input.data(), in_bytes);
-  uint4* in = e->arena.at<uint4>(e->off_input[0]);
-  AZK_CU(cudaMemcpyAsync(in, pin, in_bytes, cudaMemcpyHostToDevice, e->s_up));
-  e->scan_inputs({j.count});
-  e->set_publics(j.pub);
+  const size_t m = g.size();
+  const uint64_t proof = e->proof_len[0];
+  std::vector<uint64_t> off(m), counts(m);
+  uint64_t in_total = 0;
+  for (size_t i = 0; i < m; i++) {
+    off[i] = in_total;
+    counts[i] = g[i]->count;
+    in_total += align_up(16 * g[i]->count, 64);
+  }
+  // warm-up jobs size the staging for a full group of complete inputs
+  const uint64_t want = std::max<uint64_t>(std::max<uint64_t>(in_total, m * align_up(proof, 64)),
+                                           j0.zeros ? r.cap * std::max<uint64_t>(16ull << j0.logn, align_up(proof, 64)) : 0);
+  uint8_t* pin = st.ensure(want + 64);
+  for (size_t i = 0; i < m; i++) {
+    if (g[i]->zeros)
+      std::memset(pin + off[i], 0, 16 * counts[i]);
+    else
+      std::memcpy(pin + off[i], g[i]->input.data(), 16 * counts[i]);
+    AZK_CU(cudaMemcpyAsync(e->arena.at<uint4>(e->off_input[i]), pin + off[i], 16 * counts[i], cudaMemcpyHostToDevice, e->s_up));
+  }
+  e->scan_inputs(counts);  // waits for the copies
+  std::vector<uint8_t> pubs(32 * m);
+  for (size_t i = 0; i < m; i++) std::memcpy(pubs.data() + 32 * i, g[i]->pub, 32);
+  e->n_act = (uint32_t)m;
+  e->set_publics(pubs.data());
   Timer t;
-  e->run(true, true, nullptr, t);
-  AZK_CU(cudaMemcpyAsync(pin, e->h_inst[0].proof, proof, cudaMemcpyDeviceToHost, e->s));
+  e->run(true, false, nullptr, t);
+  for (size_t i = 0; i < m; i++)
+    AZK_CU(cudaMemcpyAsync(pin + i * align_up(proof, 64), e->h_inst[i].proof, proof, cudaMemcpyDeviceToHost, e->s));
   sync_stream(e->s);
-  j.result.assign(pin, pin + proof);
+  e->fft.check_status(e->s);
+  for (size_t i = 0; i < m; i++) g[i]->result.assign(pin + i * align_up(proof, 64), pin + i * align_up(proof, 64) + proof);
 }
 
-// Sum-check of one table through reusable device buffers: evaluations upload,
-// one single-CTA kernel, results download.  Output words: claimed sum, final
-// evaluation, digest (8 words), sums at 0, sums at 1, challenges (rounds each).
-// `evals` and `pin` (>= 4n + sizeof(SumcheckOut) + 12 log n bytes) may be the same
+// Sum-check of one table through reusable device buffers (the single-table entry
+// point): evaluations upload, one kernel, results download.  Output words: claimed
+// sum, final evaluation, digest (8 words), sums at 0, sums at 1, challenges
+// (rounds each).  `evals` and `pin` (>= sumcheck_pinned_bytes) may be the same
 // page-locked buffer: the evaluations are consumed by the upload before the
 // results land.
+void sumcheck_alloc(SumcheckBufs& b, uint32_t logn) {
+  const uint64_t n = 1ull << logn;
+  b.ev.alloc(4 * n, "Sumcheck.Evals");
+  b.scratch.alloc(4 * n, "Sumcheck.Scratch");
+  b.rounds.alloc(12ull * logn + 64, "Sumcheck.Rounds");
+  b.out.alloc(sizeof(SumcheckOut), "Sumcheck.Out");
+}
+// The SumcheckOut a table's kernel fills (per-round arrays in b.rounds).
+SumcheckOut sumcheck_out_ptrs(const SumcheckBufs& b, uint32_t logn) {
+  SumcheckOut o{};
+  o.r0 = b.rounds.as<uint32_t>();
+  o.r1 = o.r0 + logn;
+  o.challenges = o.r1 + logn;
+  return o;
+}
+std::vector<uint32_t> sumcheck_words(const SumcheckOut& r, const uint32_t* rounds_h, uint32_t logn) {
+  std::vector<uint32_t> words = {r.claimed_sum, r.final_eval};
+  for (int i = 0; i < 4; i++) {
+    words.push_back((uint32_t)r.digest[i]);
+    words.push_back((uint32_t)(r.digest[i] >> 32));
+  }
+  words.insert(words.end(), rounds_h, rounds_h + 3 * logn);
+  return words;
+}
 std::vector<uint32_t> sumcheck_run(SumcheckBufs& b, const uint32_t* evals, uint32_t logn, cudaStream_t s, uint8_t* pin, double* gpu_s = nullptr) {
   const uint64_t n = 1ull << logn;
-  if (!b.ev.p) {
-    b.ev.alloc(4 * n, "Sumcheck.Evals");
-    b.scratch.alloc(4 * n, "Sumcheck.Scratch");
-    b.rounds.alloc(12ull * logn + 64, "Sumcheck.Rounds");
-    b.out.alloc(sizeof(SumcheckOut), "Sumcheck.Out");
-  }
+  if (!b.ev.p) sumcheck_alloc(b, logn);
   AZK_CU(cudaMemcpyAsync(b.ev.p, evals, 4 * n, cudaMemcpyHostToDevice, s));
   SumcheckOut* h = reinterpret_cast<SumcheckOut*>(pin + align_up(4 * n, 64));
   uint32_t* rounds_h = reinterpret_cast<uint32_t*>(h + 1);
-  SumcheckOut ptrs{};
-  ptrs.r0 = b.rounds.as<uint32_t>();
-  ptrs.r1 = ptrs.r0 + logn;
-  ptrs.challenges = ptrs.r1 + logn;
-  *h = ptrs;
+  *h = sumcheck_out_ptrs(b, logn);
   AZK_CU(cudaMemcpyAsync(b.out.p, h, sizeof(SumcheckOut), cudaMemcpyHostToDevice, s));
   std::unique_ptr<GpuTimer> gt;
-  if (gpu_s) gt.reset(new GpuTimer(s));  // the two kernels, digest and rounds
+  if (gpu_s) gt.reset(new GpuTimer(s));
   AZK_CU(launch_sumcheck(b.ev.as<uint32_t>(), logn, b.scratch.as<uint32_t>(), b.out.as<SumcheckOut>(), s));
   if (gt) gt->stop();
   AZK_CU(cudaMemcpyAsync(h, b.out.p, sizeof(SumcheckOut), cudaMemcpyDeviceToHost, s));
   AZK_CU(cudaMemcpyAsync(rounds_h, b.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, s));
   sync_stream(s);
   if (gt) *gpu_s = gt->seconds();
-  const SumcheckOut r = *h;
-  std::vector<uint32_t> rounds(rounds_h, rounds_h + 3 * logn);
-  std::vector<uint32_t> words = {r.claimed_sum, r.final_eval};
-  for (int i = 0; i < 4; i++) {
-    words.push_back((uint32_t)r.digest[i]);
-    words.push_back((uint32_t)(r.digest[i] >> 32));
-  }
-  words.insert(words.end(), rounds.begin(), rounds.end());
-  return words;
+  return sumcheck_words(*h, rounds_h, logn);
 }
 
-uint64_t sumcheck_pinned_bytes(uint32_t logn) { return align_up(4ull << logn, 64) + sizeof(SumcheckOut) + 12ull * logn + 64; }
-
-void run_sumcheck(Resident& res, cudaStream_t s, ServeJob& j, Staging& st) {
-  if (!res.sc) res.sc = std::make_unique<SumcheckBufs>();
-  uint8_t* pin = st.ensure(sumcheck_pinned_bytes(j.logn));
-  std::memcpy(pin, j.input.data(), 4ull << j.logn);
-  std::vector<uint32_t> words = sumcheck_run(*res.sc, reinterpret_cast<const uint32_t*>(pin), j.logn, s, pin);
-  j.result.resize(4 * words.size());
-  std::memcpy(j.result.data(), words.data(), j.result.size());
-}
-
-// Evict the least recently used cached shape of worker `w` into `dropped` (its
-// device memory is freed by the caller after the server lock is released: a free
-// waits for the whole device).  Returns false when the worker caches nothing.
+// Evict the least recently used cached shape of worker `w` into `dropped` (freed by
+// the caller after the server lock is released: a free waits for the whole
+// device).  Returns false when the worker caches nothing.
 bool evict_lru(azk_server* sv, int w, std::vector<Resident>& dropped) {
   auto& cache = sv->cache[w];
   if (cache.empty()) return false;
@@ -1046,80 +1163,328 @@ bool evict_lru(azk_server* sv, int w, std::vector<Resident>& dropped) {
   return true;
 }
 
-// Called with the server lock held.  Takes the front job if its shape is cached
-// by this worker or its bytes fit the budget.  To make room it evicts this
-// worker's least recently used shapes first, then those of idle workers (a worker
-// that is not running a job has nothing in flight on its stream, so its cached
-// memory can go); busy workers keep theirs.  Nothing is taken while the job cannot
+// Make room for `bytes` more: this worker's cached shapes first, then idle
+// workers' (a worker that runs no job has nothing in flight on its stream).
+// Called with the lock held; returns whether the bytes fit.
+bool make_room(azk_server* sv, int w, uint64_t bytes, std::vector<Resident>& dropped) {
+  while (sv->held + bytes > sv->budget && evict_lru(sv, w, dropped)) {
+  }
+  for (uint32_t v = 0; v < sv->slots && sv->held + bytes > sv->budget; v++) {
+    if ((int)v == w || sv->busy[v]) continue;
+    while (sv->held + bytes > sv->budget && evict_lru(sv, (int)v, dropped)) {
+    }
+  }
+  return sv->held + bytes <= sv->budget;
+}
+
+// What a worker takes: a group of PCS jobs of one shape, or one sum-check job with
+// the lane slot it goes into.
+struct Take {
+  std::vector<std::shared_ptr<ServeJob>> group;
+  int slot = -1;
+  bool warm = false;
+};
+
+// Called with the server lock held.  Nothing is taken while the front job cannot
 // fit; a job larger than the budget never enters the queue.  Evicted memory is
 // handed back in `dropped` for the caller to free outside the lock.
-std::shared_ptr<ServeJob> try_take(azk_server* sv, int w, std::vector<Resident>& dropped) {
+bool try_take(azk_server* sv, int w, Take& tk, std::vector<Resident>& dropped) {
   // this worker's warm-up jobs first; one that cannot fit the budget is dropped
   while (!sv->warm[w].empty()) {
     auto j = sv->warm[w].front();
     auto& cache = sv->cache[w];
     ShapeKey key = shape_of(*j);
     if (!cache.count(key)) {
-      if (sv->held + j->bytes > sv->budget) {
+      const uint32_t cap = shape_capacity(sv, *j);
+      const uint64_t bytes = pcs_engine_bytes(j->logn, j->rounds, j->queries, cap) + (sv->domain_logs.count(j->logn) ? 0 : domain_bytes(j->logn));
+      if (sv->held + bytes > sv->budget) {
         sv->warm[w].pop_front();
         sv->warm_pending--;
         sv->done_cv.notify_all();
         continue;
       }
+      if (sv->domain_logs.insert(j->logn).second) sv->held += domain_bytes(j->logn);
       Resident& r = cache[key];
-      r.bytes = j->bytes;
-      sv->held += j->bytes;
+      r.cap = cap;
+      r.bytes = pcs_engine_bytes(j->logn, j->rounds, j->queries, cap);
+      sv->held += r.bytes;
     }
     cache[key].last_use = ++sv->tick;
     sv->warm[w].pop_front();
     sv->busy[w] = 1;
     j->state = 1;
-    return j;
+    tk.group = {j};
+    tk.warm = true;
+    return true;
   }
-  if (sv->queue.empty()) return nullptr;
-  auto& cache = sv->cache[w];
-  const auto& j = sv->queue.front();
-  ShapeKey key = shape_of(*j);
-  if (!cache.count(key)) {
-    while (sv->held + j->bytes > sv->budget && evict_lru(sv, w, dropped)) {
+  if (sv->queue.empty()) return false;
+  std::shared_ptr<ServeJob> j = sv->queue.front();
+  if (j->kind == 1) {
+    // a sum-check goes to a free lane slot; a slot smaller than the table grows
+    if (sv->sc_free.empty()) return false;
+    const int slot = sv->sc_free.back();
+    SumcheckSlot& sl = *sv->sc_slot[slot];
+    if (sl.cap_log < j->logn) {
+      const uint64_t extra = sumcheck_table_bytes(j->logn) - (sl.cap_log ? sumcheck_table_bytes(sl.cap_log) : 0);
+      if (!make_room(sv, w, extra, dropped)) return false;
+      sv->held += extra;
+      sl.cap_log = j->logn;  // the worker reallocates before filling the slot
+      sl.grow = true;
     }
-    for (uint32_t v = 0; v < sv->slots && sv->held + j->bytes > sv->budget; v++) {
-      if ((int)v == w || sv->busy[v]) continue;
-      while (sv->held + j->bytes > sv->budget && evict_lru(sv, (int)v, dropped)) {
+    sv->sc_free.pop_back();
+    sl.job = j;
+    sv->queue.pop_front();
+    sv->running++;
+    sv->busy[w] = 1;
+    j->state = 1;
+    j->started = std::chrono::steady_clock::now();
+    tk.slot = slot;
+    return true;
+  }
+  auto& cache = sv->cache[w];
+  const ShapeKey key = shape_of(*j);
+  if (!cache.count(key)) {
+    const uint32_t cap = shape_capacity(sv, *j);
+    const uint64_t eng = pcs_engine_bytes(j->logn, j->rounds, j->queries, cap);
+    const uint64_t dom = sv->domain_logs.count(j->logn) ? 0 : domain_bytes(j->logn);
+    if (!make_room(sv, w, eng + dom, dropped)) return false;
+    if (dom) {
+      sv->domain_logs.insert(j->logn);
+      sv->held += dom;
+    }
+    Resident& r = cache[key];
+    r.cap = cap;
+    r.bytes = eng;
+    sv->held += eng;
+  }
+  Resident& r = cache[key];
+  r.last_use = ++sv->tick;
+  // the front job and the next queued jobs of its shape, up to the engine's room
+  tk.group.clear();
+  for (auto it = sv->queue.begin(); it != sv->queue.end() && tk.group.size() < r.cap;) {
+    if ((*it)->kind == 0 && shape_of(**it) == key) {
+      tk.group.push_back(*it);
+      it = sv->queue.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  const auto now = std::chrono::steady_clock::now();
+  for (auto& g : tk.group) {
+    g->state = 1;
+    g->started = now;
+  }
+  sv->running += tk.group.size();
+  sv->groups++;
+  sv->grouped += tk.group.size();
+  sv->busy[w] = 1;
+  return true;
+}
+
+// Publish a finished job (lock held).
+void publish(azk_server* sv, ServeJob& j, int outcome, const std::string& error) {
+  j.error = error;
+  j.state = outcome;
+  j.finished = std::chrono::steady_clock::now();
+  j.input.clear();
+  j.input.shrink_to_fit();
+  sv->running--;
+  sv->completed++;
+  if (j.kind == 0 && outcome == 2) sv->elems += 1ull << j.logn;
+  sv->last_finish = j.finished;
+}
+
+// Fill a lane slot with a taken sum-check job's table and queue it for a launch.
+void lane_submit(azk_server* sv, int slot) {
+  SumcheckSlot& sl = *sv->sc_slot[slot];
+  ServeJob& j = *sl.job;
+  std::string error;
+  try {
+    AZK_CU(cudaSetDevice(sv->ctx->device));
+    if (!sl.bufs.ev.p || sl.grow) sumcheck_alloc(sl.bufs, sl.cap_log);
+    sl.grow = false;
+    uint8_t* pin = sl.pin.ensure(sumcheck_pinned_bytes(sl.cap_log));
+    if (j.zeros)
+      std::memset(pin, 0, 4ull << j.logn);
+    else
+      std::memcpy(pin, j.input.data(), 4ull << j.logn);
+  } catch (const Error& e) {
+    error = e.msg;
+  } catch (const std::exception& e) {
+    error = e.what();
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (!error.empty()) {
+    // the slot's memory may be in an unknown state: reallocate it on its next use
+    sl.grow = true;
+    auto job = sl.job;
+    sl.job = nullptr;
+    sv->sc_free.push_back(slot);
+    if (job->id == 0) {
+      job->state = 3;
+      sv->running--;
+      sv->warm_pending--;
+    } else {
+      publish(sv, *job, 3, error);
+    }
+    sv->cv.notify_all();
+    sv->done_cv.notify_all();
+    return;
+  }
+  sv->sc_pending.push_back(slot);
+  sv->lane_cv.notify_all();
+}
+
+// Lane launcher: whenever tables wait and a lane stream is idle, one batched
+// launch proves up to kLaneBatch of them.
+void lane_launcher(azk_server* sv) {
+  cudaSetDevice(sv->ctx->device);
+  for (;;) {
+    int sid = -1;
+    std::vector<int> batch;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->lane_cv.wait(lk, [&] { return (sv->lane_stop && sv->sc_pending.empty()) || (!sv->sc_pending.empty() && !sv->sc_idle.empty()); });
+      if (sv->sc_pending.empty()) {
+        sv->launcher_done = true;
+        sv->lane_cv.notify_all();
+        return;
+      }
+      sid = sv->sc_idle.back();
+      sv->sc_idle.pop_back();
+      while (!sv->sc_pending.empty() && batch.size() < (size_t)kLaneBatch) {
+        batch.push_back(sv->sc_pending.front());
+        sv->sc_pending.pop_front();
       }
     }
-    if (sv->held + j->bytes > sv->budget) return nullptr;
-    Resident& r = cache[key];
-    r.bytes = j->bytes;
-    sv->held += j->bytes;
+    SumcheckStream& st = sv->sc_stream[sid];
+    st.slots = batch;
+    std::string error;
+    try {
+      std::vector<SumcheckJob> jobs;
+      for (int slot : batch) {
+        SumcheckSlot& sl = *sv->sc_slot[slot];
+        const uint32_t logn = sl.job->logn;
+        uint8_t* pin = sl.pin.p;
+        SumcheckOut* h = reinterpret_cast<SumcheckOut*>(pin + align_up(4ull << logn, 64));
+        *h = sumcheck_out_ptrs(sl.bufs, logn);
+        AZK_CU(cudaMemcpyAsync(sl.bufs.ev.p, pin, 4ull << logn, cudaMemcpyHostToDevice, st.s));
+        AZK_CU(cudaMemcpyAsync(sl.bufs.out.p, h, sizeof(SumcheckOut), cudaMemcpyHostToDevice, st.s));
+        jobs.push_back(SumcheckJob{sl.bufs.ev.as<uint32_t>(), sl.bufs.scratch.as<uint32_t>(), sl.bufs.out.as<SumcheckOut>(), logn, 0});
+      }
+      AZK_CU(cudaMemcpyAsync(st.jobs.p, jobs.data(), sizeof(SumcheckJob) * jobs.size(), cudaMemcpyHostToDevice, st.s));
+      AZK_CU(launch_sumcheck_batch(st.jobs.as<SumcheckJob>(), (uint32_t)jobs.size(), st.s));
+      AZK_CU(cudaEventRecord(st.done, st.s));
+    } catch (const Error& e) {
+      error = e.msg.empty() ? "sum-check launch failed" : e.msg;
+    } catch (const std::exception& e) {
+      error = e.what();
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!error.empty()) {
+      for (int slot : batch) {
+        auto job = sv->sc_slot[slot]->job;
+        sv->sc_slot[slot]->job = nullptr;
+        sv->sc_free.push_back(slot);
+        if (job->id == 0) {
+          sv->running--;
+          sv->warm_pending--;
+        } else {
+          publish(sv, *job, 3, error);
+        }
+      }
+      sv->sc_idle.push_back(sid);
+      sv->cv.notify_all();
+      sv->done_cv.notify_all();
+      continue;
+    }
+    sv->sc_inflight.push_back(sid);
+    sv->lane_cv.notify_all();
   }
-  cache[key].last_use = ++sv->tick;
-  auto job = j;
-  sv->queue.pop_front();
-  sv->running++;
-  sv->busy[w] = 1;
-  job->state = 1;
-  job->started = std::chrono::steady_clock::now();
-  return job;
+}
+
+// Lane completer: waits for each launched batch in launch order (a blocking-sync
+// event, no spinning), reads its results back and publishes them.
+void lane_completer(azk_server* sv) {
+  cudaSetDevice(sv->ctx->device);
+  for (;;) {
+    int sid = -1;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->lane_cv.wait(lk, [&] { return !sv->sc_inflight.empty() || sv->launcher_done; });
+      if (sv->sc_inflight.empty()) return;
+      sid = sv->sc_inflight.front();
+      sv->sc_inflight.pop_front();
+    }
+    SumcheckStream& st = sv->sc_stream[sid];
+    std::string error;
+    std::vector<std::vector<uint32_t>> words(st.slots.size());
+    try {
+      AZK_CU(cudaEventSynchronize(st.done));
+      for (size_t k = 0; k < st.slots.size(); k++) {
+        SumcheckSlot& sl = *sv->sc_slot[st.slots[k]];
+        const uint32_t logn = sl.job->logn;
+        SumcheckOut* h = reinterpret_cast<SumcheckOut*>(sl.pin.p + align_up(4ull << logn, 64));
+        uint32_t* rounds_h = reinterpret_cast<uint32_t*>(h + 1);
+        AZK_CU(cudaMemcpyAsync(h, sl.bufs.out.p, sizeof(SumcheckOut), cudaMemcpyDeviceToHost, st.s));
+        AZK_CU(cudaMemcpyAsync(rounds_h, sl.bufs.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, st.s));
+      }
+      sync_stream(st.s);
+      for (size_t k = 0; k < st.slots.size(); k++) {
+        SumcheckSlot& sl = *sv->sc_slot[st.slots[k]];
+        const uint32_t logn = sl.job->logn;
+        SumcheckOut* h = reinterpret_cast<SumcheckOut*>(sl.pin.p + align_up(4ull << logn, 64));
+        words[k] = sumcheck_words(*h, reinterpret_cast<uint32_t*>(h + 1), logn);
+      }
+    } catch (const Error& e) {
+      error = e.msg;
+    } catch (const std::exception& e) {
+      error = e.what();
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (size_t k = 0; k < st.slots.size(); k++) {
+      const int slot = st.slots[k];
+      auto job = sv->sc_slot[slot]->job;
+      sv->sc_slot[slot]->job = nullptr;
+      sv->sc_free.push_back(slot);
+      if (job->id == 0) {  // a warm-up table
+        job->state = error.empty() ? 2 : 3;
+        sv->running--;
+        sv->warm_pending--;
+        continue;
+      }
+      if (error.empty()) {
+        job->result.resize(4 * words[k].size());
+        std::memcpy(job->result.data(), words[k].data(), job->result.size());
+      }
+      publish(sv, *job, error.empty() ? 2 : 3, error);
+    }
+    st.slots.clear();
+    sv->sc_idle.push_back(sid);
+    sv->cv.notify_all();
+    sv->done_cv.notify_all();
+    sv->lane_cv.notify_all();
+  }
 }
 
 void worker_loop(azk_server* sv, int w) {
   cudaSetDevice(sv->ctx->device);
-  // everything this worker runs (uploads, proof kernels, sum-checks) goes on its one
-  // stream: its jobs run one at a time, and one stream per worker keeps each worker
-  // on its own hardware work queue (see azk_server_create)
+  // everything this worker runs (uploads and proof kernels) goes on its one stream:
+  // its groups run one at a time, and one stream per worker keeps each worker on
+  // its own hardware work queue (see azk_server_create)
   cudaStream_t s = sv->streams[w];
   Staging staging;
   for (;;) {
-    std::shared_ptr<ServeJob> job;
+    Take tk;
     Resident* res = nullptr;
     std::vector<Resident> dropped;  // evicted shapes, freed below without the lock
     {
       std::unique_lock<std::mutex> lk(sv->mu);
+      bool got = false;
       for (;;) {
         if (sv->stop && sv->queue.empty() && sv->warm[w].empty()) break;
-        job = try_take(sv, w, dropped);
-        if (job) break;
+        got = try_take(sv, w, tk, dropped);
+        if (got) break;
         if (!dropped.empty()) {  // free what was evicted, then look again
           lk.unlock();
           dropped.clear();
@@ -1128,19 +1493,23 @@ void worker_loop(azk_server* sv, int w) {
         }
         sv->cv.wait(lk);
       }
-      if (!job) break;
-      res = &sv->cache[w][shape_of(*job)];
+      if (!got) break;
+      if (tk.slot < 0) res = &sv->cache[w][shape_of(*tk.group[0])];
     }
     dropped.clear();
+    if (tk.slot >= 0) {  // a sum-check: into the lane, and on to the next job
+      lane_submit(sv, tk.slot);
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->busy[w] = 0;
+      sv->cv.notify_all();
+      continue;
+    }
     // the outcome is published under the lock together with the finish time, so a
     // poll never sees a finished job without its latency
     int outcome = 2;
     std::string error;
     try {
-      if (job->kind == 0)
-        run_pcs(sv, *res, *job, staging, s);
-      else
-        run_sumcheck(*res, s, *job, staging);
+      run_pcs_group(sv, *res, tk.group, staging, s);
     } catch (const Error& e) {
       error = e.msg;
       outcome = 3;
@@ -1148,41 +1517,24 @@ void worker_loop(azk_server* sv, int w) {
       error = e.what();
       outcome = 3;
     }
-    std::vector<Resident> failed;  // a failed job's shape, freed without the lock
+    std::vector<Resident> failed;  // a failed group's shape, freed without the lock
     {
       std::lock_guard<std::mutex> lk(sv->mu);
-      job->error = error;
-      job->state = outcome;
       sv->busy[w] = 0;
-      if (job->id == 0) {  // a warm-up job: not a result anyone polls
-        if (job->state == 3) {
-          auto it = sv->cache[w].find(shape_of(*job));
-          if (it != sv->cache[w].end()) {
-            sv->held -= it->second.bytes;
-            failed.push_back(std::move(it->second));
-            sv->cache[w].erase(it);
-          }
-        }
-        sv->warm_pending--;
-        sv->cv.notify_all();
-        sv->done_cv.notify_all();
-      }
-      if (job->id == 0) continue;
-      job->finished = std::chrono::steady_clock::now();
-      job->input.clear();
-      job->input.shrink_to_fit();
-      if (job->state == 3) {  // drop the shape's memory: it may be in an unknown state
-        auto it = sv->cache[w].find(shape_of(*job));
+      if (outcome == 3) {  // drop the shape's memory: it may be in an unknown state
+        auto it = sv->cache[w].find(shape_of(*tk.group[0]));
         if (it != sv->cache[w].end()) {
           sv->held -= it->second.bytes;
           failed.push_back(std::move(it->second));
           sv->cache[w].erase(it);
         }
       }
-      sv->running--;
-      sv->completed++;
-      if (job->kind == 0 && job->state == 2) sv->elems += 1ull << job->logn;
-      sv->last_finish = job->finished;
+      if (tk.warm) {  // warm-up jobs are not results anyone polls
+        tk.group[0]->state = outcome;
+        sv->warm_pending--;
+      } else {
+        for (auto& j : tk.group) publish(sv, *j, outcome, error);
+      }
     }
     sv->cv.notify_all();
     sv->done_cv.notify_all();
@@ -1194,10 +1546,10 @@ void worker_loop(azk_server* sv, int w) {
   }
 }
 
-uint64_t submit(azk_server* sv, std::shared_ptr<ServeJob> j) {
+uint64_t submit(azk_server* sv, std::shared_ptr<ServeJob> j, uint64_t bytes) {
   std::lock_guard<std::mutex> lk(sv->mu);
-  require(j->bytes <= sv->budget, AZK_ERR_HBM_BUDGET,
-          "job needs " + std::to_string(j->bytes) + " device bytes, more than the server's HBM budget of " + std::to_string(sv->budget));
+  require(bytes <= sv->budget, AZK_ERR_HBM_BUDGET,
+          "job needs " + std::to_string(bytes) + " device bytes, more than the server's HBM budget of " + std::to_string(sv->budget));
   j->id = sv->next_id++;
   j->submitted = std::chrono::steady_clock::now();
   if (!sv->any_submit) {
@@ -1245,26 +1597,40 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     layout(ctx && out && slots >= 1 && slots <= 64 && hbm_budget_bytes > 0);
     auto sv = std::make_unique<azk_server>();
     sv->ctx = ctx;
-    // each job is one instance: the single-tree table (measured on the serving mix:
-    // the lowest latency per job at a throughput equal to the batch table's within
-    // run-to-run spread)
-    sv->sched = resolve_schedule(schedule, kTuned_pcs_single);
+    // a group proves few instances: the single-tree table (measured on the serving
+    // mix: the lowest latency per job at a throughput equal to the batch table's
+    // within run-to-run spread)
+    sv->sched = resolve_schedule(schedule, kTuned_pcs_single, kTunedThreads_pcs_single);
     sv->budget = hbm_budget_bytes;
     sv->slots = slots;
     sv->cache.resize(slots);
+    sv->busy.assign(slots, 0);
     sv->warm.resize(slots);
-    // The workers' streams are created here, one after another, so that with up to
+    AZK_CU(cudaSetDevice(ctx->device));
+    // The workers' streams are created first, one after another, so that with up to
     // CUDA_DEVICE_MAX_CONNECTIONS (32) workers each lands on its own hardware work
-    // queue.  Streams that share a queue wait on each other's dependent launches:
-    // a sum-check's 64 ms digest followed by its rounds kernel then stalls every
-    // stream behind it (measured with two streams per cached engine, ~800 streams:
-    // completions stopped for up to a second at a time).  Highest priority: a
-    // sum-check digest or a job's input scan takes the first free SM slot.
+    // queue.  Streams that share a queue wait on each other's dependent launches;
+    // nothing here issues a launch that waits long on an earlier one in its stream
+    // (the sum-check lane proves a table in one launch).  Highest priority: a job's
+    // input scan takes the first free SM slot.
     int prio_lo = 0, prio_hi = 0;
     AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     sv->streams.assign(slots, nullptr);
     for (uint32_t w = 0; w < slots; w++) AZK_CU(cudaStreamCreateWithPriority(&sv->streams[w], cudaStreamNonBlocking, prio_hi));
+    sv->sc_stream.resize(kLaneStreams);
+    for (int k = 0; k < kLaneStreams; k++) {
+      AZK_CU(cudaStreamCreateWithFlags(&sv->sc_stream[k].s, cudaStreamNonBlocking));
+      AZK_CU(cudaEventCreateWithFlags(&sv->sc_stream[k].done, cudaEventBlockingSync | cudaEventDisableTiming));
+      sv->sc_stream[k].jobs.alloc(sizeof(SumcheckJob) * kLaneBatch, "Sumcheck.LaneJobs");
+      sv->sc_idle.push_back(k);
+    }
+    for (int k = 0; k < kLaneSlots; k++) {
+      sv->sc_slot.push_back(std::make_unique<SumcheckSlot>());
+      sv->sc_free.push_back(kLaneSlots - 1 - k);
+    }
     for (uint32_t w = 0; w < slots; w++) sv->workers.emplace_back(worker_loop, sv.get(), (int)w);
+    sv->sc_launcher = std::thread(lane_launcher, sv.get());
+    sv->sc_completer = std::thread(lane_completer, sv.get());
     *out = sv.release();
   });
 }
@@ -1285,8 +1651,7 @@ azk_status azk_server_submit_pcs(azk_server* sv, uint32_t logn, uint32_t log_blo
     j->input.assign(coeffs, coeffs + 4 * count);
     j->count = count;
     std::memcpy(j->pub, pub, 32);
-    j->bytes = pcs_shape_bytes(logn, rounds, queries);
-    *job_id = submit(sv, j);
+    *job_id = submit(sv, j, pcs_engine_bytes(logn, rounds, queries, 1) + domain_bytes(logn));
   });
 }
 
@@ -1295,7 +1660,43 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
   return guarded(sv ? sv->ctx : nullptr, [&] {
     layout(sv && (n_pcs == 0 || (pcs_logn && pcs_rounds)) && (n_sumcheck == 0 || sumcheck_logn));
     for (uint32_t i = 0; i < n_pcs; i++) validate_params(pcs_logn[i], log_blowup, queries, 0, pcs_rounds[i]);
-    for (uint32_t i = 0; i < n_sumcheck; i++) layout(sumcheck_logn[i] >= 1 && sumcheck_logn[i] <= 28);
+    uint32_t sc_log = 0;
+    for (uint32_t i = 0; i < n_sumcheck; i++) {
+      layout(sumcheck_logn[i] >= 1 && sumcheck_logn[i] <= 28);
+      sc_log = std::max(sc_log, sumcheck_logn[i]);
+    }
+    // the lane's table slots for the largest listed table, as many as fit the budget
+    if (sc_log) {
+      AZK_CU(cudaSetDevice(sv->ctx->device));
+      for (int k = 0; k < kLaneSlots; k++) {
+        SumcheckSlot* sl = nullptr;
+        {
+          // a free slot is taken out of the free list while it is allocated
+          std::lock_guard<std::mutex> lk(sv->mu);
+          auto it = std::find(sv->sc_free.begin(), sv->sc_free.end(), k);
+          if (it == sv->sc_free.end()) continue;
+          sl = sv->sc_slot[k].get();
+          if (sl->cap_log >= sc_log && !sl->grow) continue;
+          const uint64_t extra = sumcheck_table_bytes(sc_log) - (sl->cap_log ? sumcheck_table_bytes(sl->cap_log) : 0);
+          if (sv->held + extra > sv->budget) break;
+          sv->held += extra;
+          sl->cap_log = sc_log;
+          sv->sc_free.erase(it);
+        }
+        try {
+          sumcheck_alloc(sl->bufs, sc_log);
+          sl->grow = false;
+          sl->pin.ensure(sumcheck_pinned_bytes(sc_log));
+        } catch (...) {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          sl->grow = true;
+          sv->sc_free.push_back(k);
+          throw;
+        }
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->sc_free.push_back(k);
+      }
+    }
     std::unique_lock<std::mutex> lk(sv->mu);
     for (uint32_t w = 0; w < sv->slots; w++) {
       for (uint32_t i = 0; i < n_pcs; i++) {
@@ -1305,24 +1706,23 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
         j->rounds = pcs_rounds[i];
         j->queries = queries;
         j->log_blowup = log_blowup;
-        // all 2^logn coefficients (zeros): the worker's pinned staging grows to the
-        // largest input of the shape now, not in the middle of serving, where
-        // freeing the smaller buffer would wait for the whole device
+        // all 2^logn coefficients (zeros): the worker's pinned staging grows to a
+        // full group of the shape's largest inputs now, not in the middle of
+        // serving, where freeing the smaller buffer would wait for the whole device
         j->zeros = true;
         j->count = 1ull << j->logn;
-        j->bytes = pcs_shape_bytes(j->logn, j->rounds, j->queries);
         sv->warm[w].push_back(j);
         sv->warm_pending++;
       }
-      for (uint32_t i = 0; i < n_sumcheck; i++) {
-        auto j = std::make_shared<ServeJob>();
-        j->kind = 1;
-        j->logn = sumcheck_logn[i];
-        j->input.assign(1ull << j->logn, 0u);
-        j->bytes = sumcheck_shape_bytes(j->logn);
-        sv->warm[w].push_back(j);
-        sv->warm_pending++;
-      }
+    }
+    // one table of zeros per listed size through the lane (kernels loaded before serving)
+    for (uint32_t i = 0; i < n_sumcheck; i++) {
+      auto j = std::make_shared<ServeJob>();
+      j->kind = 1;
+      j->logn = sumcheck_logn[i];
+      j->zeros = true;
+      sv->queue.push_front(j);
+      sv->warm_pending++;
     }
     sv->cv.notify_all();
     sv->done_cv.wait(lk, [&] { return sv->warm_pending == 0; });
@@ -1339,8 +1739,7 @@ azk_status azk_server_submit_sumcheck(azk_server* sv, const uint32_t* evals, uin
     j->kind = 1;
     j->logn = ilog2(count);
     j->input.assign(evals, evals + count);
-    j->bytes = sumcheck_shape_bytes(j->logn);
-    *job_id = submit(sv, j);
+    *job_id = submit(sv, j, sumcheck_table_bytes(j->logn));
   });
 }
 
@@ -1395,6 +1794,15 @@ azk_status azk_server_stats(azk_server* sv, uint64_t* completed, uint64_t* elems
   });
 }
 
+azk_status azk_server_group_stats(azk_server* sv, uint64_t* groups, uint64_t* grouped_jobs) {
+  return guarded(sv ? sv->ctx : nullptr, [&] {
+    layout(sv != nullptr);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (groups) *groups = sv->groups;
+    if (grouped_jobs) *grouped_jobs = sv->grouped;
+  });
+}
+
 void azk_server_destroy(azk_server* sv) {
   if (!sv) return;
   {
@@ -1403,6 +1811,17 @@ void azk_server_destroy(azk_server* sv) {
   }
   sv->cv.notify_all();
   for (auto& t : sv->workers) t.join();
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->lane_stop = true;
+  }
+  sv->lane_cv.notify_all();
+  if (sv->sc_launcher.joinable()) sv->sc_launcher.join();
+  if (sv->sc_completer.joinable()) sv->sc_completer.join();
+  for (auto& st : sv->sc_stream) {
+    if (st.done) cudaEventDestroy(st.done);
+    if (st.s) cudaStreamDestroy(st.s);
+  }
   for (auto st : sv->streams)
     if (st) cudaStreamDestroy(st);
   delete sv;

@@ -35,9 +35,9 @@ const azk_ctx::Domain& azk::domain_tables(azk_ctx* ctx, uint32_t logn) {
   return ctx->domains.emplace(logn, d).first->second;
 }
 
-Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults) {
+Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults, const uint16_t* default_threads) {
   Sched r;
-  bool any_layer = false;
+  bool any_layer = false, any_threads = false;
   if (s) {
     if (s->treelet_log) r.tile_log = s->treelet_log;
     if (s->group_log) r.group_log = s->group_log;
@@ -47,10 +47,16 @@ Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults) {
       r.layer_tile[i] = s->layer_treelet[i];
       any_layer |= r.layer_tile[i] != 0;
       require(r.layer_tile[i] <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "layer treelet depth must be in 0...13");
+      const uint16_t th = s->layer_threads[i];
+      require(th == 0 || th == 128 || th == 256 || th == 512, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "layer threads must be 0, 128, 256 or 512");
+      r.layer_threads[i] = th;
+      any_threads |= th != 0;
     }
   }
   if (defaults && !any_layer && !(s && s->treelet_log))
     for (int i = 0; i < 32; i++) r.layer_tile[i] = defaults[i] <= 13 ? defaults[i] : 13;
+  if (default_threads && !any_threads && !(s && s->threads))
+    for (int i = 0; i < 32; i++) r.layer_threads[i] = (default_threads[i] == 128 || default_threads[i] == 256 || default_threads[i] == 512) ? default_threads[i] : 0;
   require(r.tile_log >= 1 && r.tile_log <= 13, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "treelet_log must be in 1...13");
   if (r.group_log > r.tile_log) r.group_log = r.tile_log;
   require(r.group_log >= 1, AZK_ERR_INVALID_KERNEL_CONFIGURATION, "group_log must be >= 1");
@@ -61,6 +67,38 @@ Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults) {
 // ---------------------------------------------------------------------------
 // FFT plans
 // ---------------------------------------------------------------------------
+namespace {
+// cuMemGetAddressRange through the runtime's driver entry point (no link against
+// the driver library): CUresult (*)(CUdeviceptr* base, size_t* size, CUdeviceptr p).
+using MemRangeFn = int (*)(unsigned long long*, size_t*, unsigned long long);
+MemRangeFn mem_range_fn() {
+  static MemRangeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<MemRangeFn>(f);
+  }();
+  return fn;
+}
+}  // namespace
+
+void azk::require_device_range(const void* p, uint64_t off, uint64_t bytes) {
+  layout(p != nullptr, "null device pointer");
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  layout(a + off >= a && a + off + bytes >= a + off, "device range overflows");
+  MemRangeFn fn = mem_range_fn();
+  require(fn != nullptr, AZK_ERR_COMMAND_EXECUTION_FAILED, "cuMemGetAddressRange is not available from the driver");
+  unsigned long long base = 0;
+  size_t size = 0;
+  if (fn(&base, &size, (unsigned long long)(a + off)) != 0)
+    fail(AZK_ERR_INVALID_INPUT_LAYOUT, "resident buffer is not device memory of this context");
+  layout(a + off + bytes <= base + size, "resident buffer range runs past the end of its device allocation");
+}
+
 void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uint8_t>& narrow_flags) {
   jobs.clear();
   work.clear();
@@ -68,11 +106,11 @@ void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uin
   for (size_t i = 0; i < transforms.size() && i < narrow_flags.size(); i++) narrow[i] = narrow_flags[i] ? 1 : 0;
   uint32_t max_passes = 0;
   for (auto& t : transforms) max_passes = std::max(max_passes, fft_high_chunks(t.logn) + 1);
-  step_off.assign(max_passes, 0);
-  step_cnt.assign(max_passes, 0);
-  nstep_off.assign(max_passes, 0);
-  nstep_cnt.assign(max_passes, 0);
+  std::array<uint64_t, kFftKinds> zero{};
+  part_off.assign(max_passes, zero);
+  part_cnt.assign(max_passes, zero);
   inst_range.assign(max_passes, std::vector<std::pair<uint64_t, uint64_t>>(transforms.size(), {0, 0}));
+  inst_kind.assign(max_passes, std::vector<uint8_t>(transforms.size(), 0));
   std::vector<std::vector<uint32_t>> job_at(max_passes, std::vector<uint32_t>(transforms.size(), UINT32_MAX));
   for (size_t i = 0; i < transforms.size(); i++) {
     uint32_t passes = fft_high_chunks(transforms[i].logn) + 1;
@@ -84,35 +122,54 @@ void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uin
     }
   }
   for (uint32_t step = 0; step < max_passes; step++) {
-    for (int part = 0; part < 2; part++) {
-      (part ? nstep_off : step_off)[step] = work.size();
+    for (uint32_t kind = 0; kind < kFftKinds; kind++) {
+      part_off[step][kind] = work.size();
       for (size_t i = 0; i < transforms.size(); i++) {
         uint32_t jid = job_at[step][i];
-        if (jid == UINT32_MAX || narrow[i] != part) continue;
-        uint64_t tiles = fft_pass_tiles(jobs[jid].logn, jobs[jid].pass);
+        if (jid == UINT32_MAX) continue;
+        const FftJob& j = jobs[jid];
+        if (fft_pass_kind(j.logn, j.pass, narrow[i] != 0) != kind) continue;
+        uint64_t tiles = fft_kind_tiles(j.logn, j.pass, kind);
         inst_range[step][i] = {work.size(), tiles};
+        inst_kind[step][i] = (uint8_t)kind;
         for (uint64_t t = 0; t < tiles; t++) work.push_back(make_uint2(jid, (uint32_t)t));
       }
-      (part ? nstep_cnt : step_cnt)[step] = work.size() - (part ? nstep_off : step_off)[step];
+      part_cnt[step][kind] = work.size() - part_off[step][kind];
     }
   }
 }
+// Device lists keep their allocation when the new ones fit (a server group of
+// another size rebuilds the lists without an allocation, which would wait for the
+// whole device).
 void FftPlan::upload(cudaStream_t s) {
-  d_jobs.alloc(std::max<size_t>(1, jobs.size()) * sizeof(FftJob), "fft jobs");
-  d_work.alloc(std::max<size_t>(1, work.size()) * sizeof(uint2), "fft work");
+  const uint64_t jb = std::max<size_t>(1, jobs.size()) * sizeof(FftJob), wb = std::max<size_t>(1, work.size()) * sizeof(uint2);
+  if (d_jobs.bytes < jb) d_jobs.alloc(jb, "fft jobs");
+  if (d_work.bytes < wb) d_work.alloc(wb, "fft work");
+  if (!d_status.p) {
+    d_status.alloc(16, "fft status");
+    AZK_CU(cudaMemsetAsync(d_status.p, 0, 16, s));
+  }
   if (!jobs.empty()) AZK_CU(cudaMemcpyAsync(d_jobs.p, jobs.data(), jobs.size() * sizeof(FftJob), cudaMemcpyHostToDevice, s));
   if (!work.empty()) AZK_CU(cudaMemcpyAsync(d_work.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
 }
-// Steps are aligned at the end: the last step holds every transform's low-stage pass.
 void FftPlan::launch_step(size_t step, cudaStream_t s) const {
-  const bool last = step + 1 == step_cnt.size();
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + step_off[step], (uint32_t)step_cnt[step], false, last, s));
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + nstep_off[step], (uint32_t)nstep_cnt[step], true, last, s));
+  for (uint32_t kind = 0; kind < kFftKinds; kind++)
+    AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + part_off[step][kind], (uint32_t)part_cnt[step][kind], kind,
+                           d_status.as<uint32_t>(), s));
 }
 void FftPlan::launch_step_for(size_t step, size_t t, cudaStream_t s) const {
   auto r = inst_range[step][t];
-  const bool last = step + 1 == step_cnt.size();
-  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, narrow[t] != 0, last, s));
+  AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, inst_kind[step][t], d_status.as<uint32_t>(), s));
+}
+void FftPlan::check_status(cudaStream_t s) {
+  if (!d_status.p) return;
+  uint32_t f = 0;
+  AZK_CU(cudaMemcpyAsync(&f, d_status.p, 4, cudaMemcpyDeviceToHost, s));
+  sync_stream(s);
+  if (f) {
+    AZK_CU(cudaMemsetAsync(d_status.p, 0, 4, s));
+    fail(AZK_ERR_DEVICE_TIMEOUT, "a Circle FFT pass gave up waiting for its bulk tile copies");
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -327,7 +384,7 @@ struct azk_merkle_plan {
   std::mutex mu;
   cudaStream_t s = nullptr;
   uint64_t count, stride, length;
-  uint32_t logn, tile_log;
+  uint32_t logn, tile_log, threads = 256;
   DevBuf leaves, leaf_digests, inner, counters, job, work, root, idx, paths;
   TreeJob h_job{};
   std::vector<uint2> h_work;
@@ -511,6 +568,7 @@ azk_status azk_merkle_plan_create(azk_ctx* ctx, uint64_t count, uint64_t stride,
     if (tl > p->logn) tl = p->logn;
     if (tl == 0 && p->logn > 0) tl = 1;
     p->tile_log = tl;
+    p->threads = treelet_log ? 256 : (p->logn < 32 && kTunedThreads_merkle_raw64[p->logn] ? kTunedThreads_merkle_raw64[p->logn] : 256);
     p->leaves.alloc(count * stride, "Merkle.Leaves");
     p->leaf_digests.alloc(count * 32, "Merkle.LeafDigests");
     p->inner.alloc((count > 1 ? count - 1 : 1) * 32, "Merkle.Inner");
@@ -548,7 +606,7 @@ static void merkle_commit_dev(azk_merkle_plan* p, const uint8_t* dleaves, uint8_
   p->h_job.aligned8 = (((uintptr_t)dleaves & 7) == 0 && (p->stride & 7) == 0) ? 1 : 0;
   AZK_CU(cudaMemcpyAsync(p->job.p, &p->h_job, sizeof(TreeJob), cudaMemcpyHostToDevice, p->s));
   GpuTimer g(p->s);
-  AZK_CU(launch_tree_jobs(p->job.as<TreeJob>(), p->work.as<uint2>(), (uint32_t)p->h_work.size(), p->tile_log, kLeafRaw, 256, p->s));
+  AZK_CU(launch_tree_jobs(p->job.as<TreeJob>(), p->work.as<uint2>(), (uint32_t)p->h_work.size(), p->tile_log, kLeafRaw, p->threads, p->s));
   uint64_t sub = t.ns();
   g.stop();
   AZK_CU(cudaMemcpyAsync(root_out, p->root.p, 32, cudaMemcpyDeviceToHost, p->s));

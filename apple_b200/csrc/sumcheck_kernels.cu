@@ -2,15 +2,12 @@
 // SumcheckOracle.swift:797-868; statement digest :743-754; word digest :1288-1299;
 // transcript frames :1066-1106).
 //
-// Two launches per table.  The statement's word digest is one sequential sponge
-// over the table, so it runs as its own one-warp kernel (the state spread over
-// the warp's lanes) that holds almost nothing of an SM while other jobs' kernels
-// run beside it.  Then one
-// CTA proves the table: each round is a block reduction (sums of the even and odd
-// entries), a transcript round by thread 0 (round frame, challenge frame, squeeze
-// one word mod p) and a fold t'[i] = (1 - r) t[2i] + r t[2i+1].  A table of 2^20
-// words is 4 MiB, so each round is a few microseconds of one SM; keeping the rounds
-// in one CTA needs no grid-wide wait and lets many jobs share the GPU.
+// One CTA of 256 threads per table.  The statement's word digest is one
+// sequential sponge over the table, so it runs on one warp (the state spread over
+// the warp's lanes) while the CTA's other warps wait; then the block proves the
+// rounds.  A table of 2^20 words is 4 MiB, so each round is a few microseconds of
+// one SM; keeping the rounds in one CTA needs no grid-wide wait and lets many jobs
+// share the GPU.
 #include "azk_field.cuh"
 #include "azk_internal.h"
 
@@ -23,6 +20,14 @@ struct SumcheckOut {
   uint32_t* r0;          // rounds
   uint32_t* r1;          // rounds
   uint32_t* challenges;  // rounds
+};
+// One table of a batched launch.
+struct SumcheckJob {
+  const uint32_t* evals;
+  uint32_t* scratch;  // 2^log_n words
+  SumcheckOut* out;
+  uint32_t log_n;
+  uint32_t pad;
 };
 
 __device__ __forceinline__ uint32_t block_sum_m31(uint32_t v, uint32_t* red) {
@@ -199,18 +204,27 @@ __device__ uint64_t digest_words_warp(const uint32_t* words, uint64_t count) {
   return a;
 }
 
-__global__ void __launch_bounds__(32) sumcheck_digest_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, SumcheckOut* __restrict__ out) {
-  const uint64_t d = digest_words_warp(evals, 1ull << log_n);
-  if (threadIdx.x < 4) out->digest[threadIdx.x] = d;
-}
-
-// 512 threads at <= 64 registers: half an SM's register file, so a rounds kernel
-// finds room beside the other jobs' kernels instead of waiting for an empty SM.
-__global__ void __launch_bounds__(512, 2) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
-                                                        SumcheckOut* __restrict__ out) {
+// One table on one CTA: warp 0 computes the statement's word digest (the other
+// warps wait at the barrier, issuing nothing), then the whole block proves the
+// rounds: each round is a block reduction (sums of the even and odd entries), a
+// transcript round by thread 0 (round frame, challenge frame, squeeze one word mod
+// p) and a fold t'[i] = (1 - r) t[2i] + r t[2i+1].  One launch per table (or per
+// batch of tables, one CTA each) leaves no launch in the stream waiting behind the
+// digest, so a stream that shares a hardware work queue with others never holds
+// that queue for the digest's duration.
+__device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch, SumcheckOut* __restrict__ out) {
   __shared__ uint32_t red[32];
   __shared__ uint32_t s_ch;
+  __shared__ uint64_t s_digest[4];
   const uint64_t n = 1ull << log_n;
+  if (threadIdx.x < 32) {
+    const uint64_t d = digest_words_warp(evals, n);
+    if (threadIdx.x < 4) {
+      s_digest[threadIdx.x] = d;
+      out->digest[threadIdx.x] = d;
+    }
+  }
+  __syncthreads();
   // claimed sum
   uint32_t acc = 0;
   for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) acc = m31_add(acc, evals[i]);
@@ -224,7 +238,7 @@ __global__ void __launch_bounds__(512, 2) sumcheck_kernel(const uint32_t* __rest
     fb_u64(f, n);
     fb_u32(f, log_n);
     fb_u32(f, total);
-    for (int i = 0; i < 4; i++) fb_u64(f, out->digest[i]);
+    for (int i = 0; i < 4; i++) fb_u64(f, s_digest[i]);
     tr_absorb(t, f.b, f.n);
   }
   const uint32_t* cur = evals;
@@ -233,8 +247,9 @@ __global__ void __launch_bounds__(512, 2) sumcheck_kernel(const uint32_t* __rest
     const uint64_t half = (n >> r) >> 1;
     uint32_t z = 0, o = 0;
     for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
-      z = m31_add(z, cur[2 * i]);
-      o = m31_add(o, cur[2 * i + 1]);
+      const uint2 pr = *reinterpret_cast<const uint2*>(cur + 2 * i);
+      z = m31_add(z, pr.x);
+      o = m31_add(o, pr.y);
     }
     uint32_t zs = block_sum_m31(z, red);
     uint32_t os = block_sum_m31(o, red);
@@ -260,16 +275,36 @@ __global__ void __launch_bounds__(512, 2) sumcheck_kernel(const uint32_t* __rest
     const uint32_t c = s_ch;
     const uint32_t omc = m31_sub(1, c);
     uint32_t* nxt = bufs[r & 1];
-    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) nxt[i] = m31_add(m31_mul(omc, cur[2 * i]), m31_mul(c, cur[2 * i + 1]));
+    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
+      const uint2 pr = *reinterpret_cast<const uint2*>(cur + 2 * i);
+      nxt[i] = m31_add(m31_mul(omc, pr.x), m31_mul(c, pr.y));
+    }
     __syncthreads();
     cur = nxt;
   }
   if (threadIdx.x == 0) out->final_eval = cur[0];
 }
 
+constexpr int kSumcheckThreads = 256;
+
+__global__ void __launch_bounds__(kSumcheckThreads) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
+                                                                  SumcheckOut* __restrict__ out) {
+  sumcheck_prove_block(evals, log_n, scratch, out);
+}
+
+__global__ void __launch_bounds__(kSumcheckThreads) sumcheck_batch_kernel(const SumcheckJob* __restrict__ jobs) {
+  const SumcheckJob j = jobs[blockIdx.x];
+  sumcheck_prove_block(j.evals, j.log_n, j.scratch, j.out);
+}
+
 cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s) {
-  sumcheck_digest_kernel<<<1, 32, 0, s>>>(evals, log_n, out);
-  sumcheck_kernel<<<1, 512, 0, s>>>(evals, log_n, scratch, out);
+  sumcheck_kernel<<<1, kSumcheckThreads, 0, s>>>(evals, log_n, scratch, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sumcheck_batch(const SumcheckJob* d_jobs, uint32_t count, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  sumcheck_batch_kernel<<<count, kSumcheckThreads, 0, s>>>(d_jobs);
   return cudaGetLastError();
 }
 

@@ -7,7 +7,9 @@
 // on those timings by the kernels below, predicts schedules for shapes it has not
 // timed.  Nothing here changes a result: schedules only reorder identical work.
 #include <algorithm>
+#include <cmath>
 #include <random>
+#include <thread>
 
 #include "azk_field.cuh"
 #include "azk_runtime.h"
@@ -105,6 +107,269 @@ extern "C" azk_status azk_tuner_time_tree(azk_ctx* ctx, uint32_t log_leaves, uin
     }
     std::sort(ts.begin(), ts.end());
     *seconds = ts[ts.size() / 2];
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Correctness-gated race (MetalProofPlanner.measureMerkleCandidate,
+// Planner/MetalProofPlanner.swift:367-418) and randomized validation of a winner
+// (validateMerkleWinnerForPersistence, :447-484).  Every candidate first commits a
+// seeded random input whose roots the host computes with the library's own host
+// Keccak; a candidate whose roots differ is dropped (passed_gate = 0) and never
+// timed, and every timed run is checked again.  Timings: median and 95th
+// percentile of the device time, median host submit time.
+// ---------------------------------------------------------------------------
+namespace {
+
+// 64-byte message (eight lanes) -> SHA3-256 digest, one permutation.
+void host_sha3_64(const uint64_t (&m)[8], uint64_t (&d)[4]) {
+  uint64_t a[25] = {0};
+  for (int i = 0; i < 8; i++) a[i] = m[i];
+  a[8] = 0x06;
+  a[16] = 0x8000000000000000ull;
+  keccak_f1600(a);
+  for (int i = 0; i < 4; i++) d[i] = a[i];
+}
+
+// Roots of `concurrent` trees as the tree kernel builds them, on all host cores.
+struct TreeInput {
+  uint32_t log_leaves, leaf_bytes, fold, concurrent;
+  std::vector<uint32_t> prev, out, inv, ch;  // device contents copied to the host
+};
+
+std::vector<uint64_t> host_roots(const TreeInput& in) {
+  const uint64_t n = 1ull << in.log_leaves;
+  const uint64_t elems = in.leaf_bytes == 16 ? n : 4 * n;
+  std::vector<uint64_t> roots(4ull * in.concurrent);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  for (uint32_t c = 0; c < in.concurrent; c++) {
+    std::vector<uint64_t> lvl(4 * n);
+    auto leaf = [&](uint64_t i) {
+      uint64_t d[4];
+      if (in.leaf_bytes == 64) {
+        uint64_t m[8];
+        const uint32_t* w = in.out.data() + 4 * (c * elems + 4 * i);
+        for (int k = 0; k < 8; k++) m[k] = (uint64_t)w[2 * k] | ((uint64_t)w[2 * k + 1] << 32);
+        host_sha3_64(m, d);
+      } else {
+        uint32_t v[4];
+        if (in.fold) {
+          const uint32_t* p = in.prev.data() + 4 * (c * 2 * elems + 2 * i);
+          qm31 r = fri_fold_pair(qm31{p[0], p[1], p[2], p[3]}, qm31{p[4], p[5], p[6], p[7]}, in.inv[i], qm31{in.ch[0], in.ch[1], in.ch[2], in.ch[3]});
+          v[0] = r.a, v[1] = r.b, v[2] = r.c, v[3] = r.d;
+        } else {
+          const uint32_t* p = in.out.data() + 4 * (c * elems + i);
+          for (int k = 0; k < 4; k++) v[k] = p[k];
+        }
+        sha3_16((uint64_t)v[0] | ((uint64_t)v[1] << 32), (uint64_t)v[2] | ((uint64_t)v[3] << 32), d);
+      }
+      for (int k = 0; k < 4; k++) lvl[4 * i + k] = d[k];
+    };
+    std::vector<std::thread> ts;
+    for (unsigned t = 0; t < hw; t++)
+      ts.emplace_back([&, t] {
+        for (uint64_t i = t; i < n; i += hw) leaf(i);
+      });
+    for (auto& t : ts) t.join();
+    for (uint64_t m = n; m > 1; m >>= 1) {
+      std::vector<uint64_t> up(4 * (m / 2));
+      std::vector<std::thread> tp;
+      const unsigned use = m >= 8192 ? hw : 1;
+      for (unsigned t = 0; t < use; t++)
+        tp.emplace_back([&, t] {
+          for (uint64_t i = t; i < m / 2; i += use) {
+            uint64_t msg[8], d[4];
+            for (int k = 0; k < 4; k++) msg[k] = lvl[4 * (2 * i) + k], msg[4 + k] = lvl[4 * (2 * i + 1) + k];
+            host_sha3_64(msg, d);
+            for (int k = 0; k < 4; k++) up[4 * i + k] = d[k];
+          }
+        });
+      for (auto& t : tp) t.join();
+      lvl.swap(up);
+    }
+    for (int k = 0; k < 4; k++) roots[4 * c + k] = lvl[k];
+  }
+  return roots;
+}
+
+// Device buffers and jobs of one tree shape, filled from `seed`.
+struct TreeBench {
+  azk_ctx* ctx;
+  cudaStream_t s;
+  uint32_t log_leaves, leaf_bytes, fold, concurrent, kind;
+  uint64_t n, elems;
+  DevBuf prev, out, inv, ch, inner, cnt, jobs, roots, work;
+  std::vector<TreeJob> hj;
+  TreeBench(azk_ctx* c, uint32_t lg, uint32_t lb, uint32_t f, uint32_t conc)
+      : ctx(c), s(c->stream), log_leaves(lg), leaf_bytes(lb), fold(f), concurrent(conc) {
+    n = 1ull << lg;
+    elems = lb == 16 ? n : 4 * n;
+    kind = lb == 64 ? kLeafRaw : (f ? kLeafFold : kLeafQM31);
+    prev.alloc(16 * 2 * elems * conc, "Tuner.Prev");
+    out.alloc(16 * elems * conc, "Tuner.Out");
+    inv.alloc(4 * n + 16, "Tuner.Inv");
+    ch.alloc(16, "Tuner.Challenge");
+    inner.alloc(32 * n * conc, "Tuner.Inner");
+    cnt.alloc(4 * tree_counter_count(lg, 1) * conc, "Tuner.Counters");
+    jobs.alloc(sizeof(TreeJob) * conc, "Tuner.Jobs");
+    roots.alloc(32ull * conc, "Tuner.Roots");
+  }
+  void fill(uint32_t seed) {
+    auto f = [&](DevBuf& b, uint32_t sd, uint32_t nz) {
+      uint64_t words = b.bytes / 4;
+      fill_random_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(b.as<uint32_t>(), words, sd, nz);
+      AZK_CU(cudaGetLastError());
+    };
+    f(prev, seed * 4 + 11, 0);
+    f(out, seed * 4 + 13, 0);
+    f(inv, seed * 4 + 17, 1);
+    f(ch, seed * 4 + 19, 0);
+  }
+  TreeInput host_copy() {
+    TreeInput in{log_leaves, leaf_bytes, fold, concurrent, {}, {}, {}, {}};
+    in.prev.resize(prev.bytes / 4);
+    in.out.resize(out.bytes / 4);
+    in.inv.resize(inv.bytes / 4);
+    in.ch.resize(4);
+    AZK_CU(cudaMemcpyAsync(in.prev.data(), prev.p, prev.bytes, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaMemcpyAsync(in.out.data(), out.p, out.bytes, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaMemcpyAsync(in.inv.data(), inv.p, inv.bytes, cudaMemcpyDeviceToHost, s));
+    AZK_CU(cudaMemcpyAsync(in.ch.data(), ch.p, 16, cudaMemcpyDeviceToHost, s));
+    sync_stream(s);
+    return in;
+  }
+  // jobs and work list for one schedule; returns the number of work items
+  uint32_t setup(uint32_t tl, uint32_t gl) {
+    hj.assign(concurrent, TreeJob{});
+    std::vector<uint2> w;
+    for (uint32_t c = 0; c < concurrent; c++) {
+      TreeJob& j = hj[c];
+      j.logn = log_leaves;
+      j.kind = kind;
+      j.tile_log = tl;
+      j.group_log = gl;
+      if (kind == kLeafRaw) {
+        j.raw = reinterpret_cast<const uint8_t*>(out.as<uint4>() + c * elems);
+        j.stride = 64;
+        j.len = 64;
+        j.suffix = 0x06;
+        j.aligned8 = 1;
+      } else if (kind == kLeafQM31) {
+        j.layer = out.as<uint4>() + c * elems;
+      } else {
+        j.layer = prev.as<uint4>() + c * 2 * elems;
+        j.inv = inv.as<uint32_t>();
+        j.fold_ch = ch.as<uint32_t>();
+        j.out_layer = out.as<uint4>() + c * elems;
+      }
+      j.inner = inner.as<uint64_t>() + 4 * n * c;
+      j.counters = cnt.as<uint32_t>() + tree_counter_count(log_leaves, 1) * c;
+      j.root_action = kRootNone;
+      j.root_out = roots.as<uint64_t>() + 4 * c;
+      for (uint64_t t = 0; t < (1ull << (log_leaves - tl)); t++) w.push_back(make_uint2(c, (uint32_t)t));
+    }
+    AZK_CU(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+    if (work.bytes < w.size() * sizeof(uint2)) work.alloc(w.size() * sizeof(uint2), "Tuner.Work");
+    AZK_CU(cudaMemcpyAsync(jobs.p, hj.data(), sizeof(TreeJob) * concurrent, cudaMemcpyHostToDevice, s));
+    AZK_CU(cudaMemcpyAsync(work.p, w.data(), w.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    return (uint32_t)w.size();
+  }
+  std::vector<uint64_t> run_roots(uint32_t nwork, uint32_t tl, uint32_t threads, double* gpu_s, double* submit_s) {
+    AZK_CU(cudaMemsetAsync(roots.p, 0, roots.bytes, s));
+    Timer t;
+    GpuTimer g(s);
+    AZK_CU(launch_tree_jobs(jobs.as<TreeJob>(), work.as<uint2>(), nwork, tl, kind, threads, s));
+    if (submit_s) *submit_s = t.seconds();
+    g.stop();
+    std::vector<uint64_t> r(4ull * concurrent);
+    AZK_CU(cudaMemcpyAsync(r.data(), roots.p, roots.bytes, cudaMemcpyDeviceToHost, s));
+    sync_stream(s);
+    if (gpu_s) *gpu_s = g.seconds();
+    return r;
+  }
+};
+
+void check_tree_shape(uint32_t log_leaves, uint32_t leaf_bytes, uint32_t concurrent) {
+  layout(log_leaves >= 1 && log_leaves <= 24 && concurrent >= 1 && concurrent <= 4096);
+  layout(leaf_bytes == 16 || leaf_bytes == 64);
+  layout((1ull << log_leaves) * concurrent <= (1ull << 24), "at most 2^24 leaves in one race");
+}
+void check_candidate(const azk_tuner_candidate& c, uint32_t log_leaves) {
+  require(c.tile_log >= 1 && c.tile_log <= 13 && c.group_log >= 1 && (c.threads == 128 || c.threads == 256 || c.threads == 512),
+          AZK_ERR_INVALID_KERNEL_CONFIGURATION, "candidate: tile_log 1..13, group_log >= 1, threads 128/256/512");
+  (void)log_leaves;
+}
+
+}  // namespace
+
+extern "C" azk_status azk_tuner_race_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent,
+                                          const azk_tuner_candidate* candidates, uint32_t count, uint32_t warmup_runs, uint32_t measured_runs,
+                                          uint64_t seed, azk_tuner_measurement* out, uint32_t* winner) {
+  return guarded(ctx, [&] {
+    layout(ctx && candidates && out && winner && count >= 1 && measured_runs >= 1);
+    check_tree_shape(log_leaves, leaf_bytes, concurrent);
+    for (uint32_t i = 0; i < count; i++) check_candidate(candidates[i], log_leaves);
+    AZK_CU(cudaSetDevice(ctx->device));
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    TreeBench tb(ctx, log_leaves, leaf_bytes, fold, concurrent);
+    tb.fill((uint32_t)(seed * 2654435761u) | 1u);
+    const std::vector<uint64_t> want = host_roots(tb.host_copy());
+    double best = -1.0;
+    *winner = UINT32_MAX;
+    for (uint32_t i = 0; i < count; i++) {
+      const azk_tuner_candidate& c = candidates[i];
+      azk_tuner_measurement& m = out[i];
+      m = azk_tuner_measurement{};
+      const uint32_t tl = std::min(c.tile_log, log_leaves);
+      const uint32_t gl = std::max<uint32_t>(1, std::min(c.group_log, tl));
+      const uint32_t nwork = tb.setup(tl, gl);
+      // the gate, then warm-up and measured runs, each checked
+      bool ok = tb.run_roots(nwork, tl, c.threads, nullptr, nullptr) == want;
+      for (uint32_t r = 0; ok && r < warmup_runs; r++) ok = tb.run_roots(nwork, tl, c.threads, nullptr, nullptr) == want;
+      std::vector<double> g, sub;
+      for (uint32_t r = 0; ok && r < measured_runs; r++) {
+        double gs = 0, ss = 0;
+        ok = tb.run_roots(nwork, tl, c.threads, &gs, &ss) == want;
+        g.push_back(gs);
+        sub.push_back(ss);
+      }
+      m.passed_gate = ok ? 1 : 0;
+      if (!ok) continue;
+      std::sort(g.begin(), g.end());
+      std::sort(sub.begin(), sub.end());
+      m.runs = (uint32_t)g.size();
+      m.median_gpu_s = g[g.size() / 2];
+      m.p95_gpu_s = g[std::min<size_t>(g.size() - 1, (size_t)std::ceil(0.95 * (double)g.size()) - 1)];
+      m.median_submit_s = sub[sub.size() / 2];
+      // the winner: lowest median device time plus host submit time
+      const double score = m.median_gpu_s + m.median_submit_s;
+      if (best < 0 || score < best) {
+        best = score;
+        *winner = i;
+      }
+    }
+    require(*winner != UINT32_MAX, AZK_ERR_CORRECTNESS_VALIDATION_FAILED, "no candidate schedule reproduced the host roots");
+  });
+}
+
+extern "C" azk_status azk_tuner_validate_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent,
+                                              const azk_tuner_candidate* winner, uint32_t batches, uint64_t seed) {
+  return guarded(ctx, [&] {
+    layout(ctx && winner);
+    check_tree_shape(log_leaves, leaf_bytes, concurrent);
+    check_candidate(*winner, log_leaves);
+    AZK_CU(cudaSetDevice(ctx->device));
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    TreeBench tb(ctx, log_leaves, leaf_bytes, fold, concurrent);
+    const uint32_t tl = std::min(winner->tile_log, log_leaves);
+    const uint32_t gl = std::max<uint32_t>(1, std::min(winner->group_log, tl));
+    for (uint32_t b = 0; b < batches; b++) {
+      tb.fill((uint32_t)((seed + 0x9E37u * (b + 1)) * 2654435761u) | 1u);
+      const std::vector<uint64_t> want = host_roots(tb.host_copy());
+      const uint32_t nwork = tb.setup(tl, gl);
+      require(tb.run_roots(nwork, tl, winner->threads, nullptr, nullptr) == want, AZK_ERR_CORRECTNESS_VALIDATION_FAILED,
+              "winning schedule failed randomized validation batch " + std::to_string(b));
+    }
   });
 }
 

@@ -373,6 +373,157 @@ def circle_merkle_fold_chain(ctx: Context, log_size: int, evaluations, log_blowu
     return fin, [cm[32 * k:32 * k + 32].tobytes() for k in range(rounds)], ch
 
 
+class QM31FRIFoldPlan(_Plan):
+    """QM31FRIFoldPlan (QM31FRIFold.swift:960-1338): one fold of `input_count` values."""
+
+    _destroy = "azk_qm31_fold_plan_destroy"
+
+    def __init__(self, ctx: Context, input_count: int):
+        super().__init__(ctx)
+        self.input_count, self.output_count = input_count, input_count // 2
+        self._check(lib().azk_qm31_fold_plan_create(ctx.handle, input_count, ctypes.byref(self._h)))
+
+    def execute(self, evaluations, inverse_points, challenge) -> np.ndarray:
+        ev, inv, ch = _q(evaluations), _q(inverse_points), _q(challenge)
+        if len(ev) != self.input_count or len(inv) != self.output_count or len(ch) != 1:
+            raise AZKError(1, "evaluations / inverse points do not match the plan's counts")
+        out = np.empty((self.output_count, 4), np.uint32)
+        self._check(lib().azk_qm31_fold_plan_execute(self._h, _ptr(ev), _ptr(inv), _ptr(ch), _ptr(out), ctypes.byref(self.last_stats)))
+        return out
+
+    def execute_resident(self, dev_evaluations, dev_inverse_points, dev_out, challenge, evaluations_offset=0, inverse_offset=0, out_offset=0) -> Stats:
+        ch = _q(challenge)
+        st = Stats()
+        self._check(lib().azk_qm31_fold_plan_execute_resident(self._h, dev_evaluations, evaluations_offset, dev_inverse_points, inverse_offset, dev_out,
+                                                              out_offset, _ptr(ch), ctypes.byref(st)))
+        return st
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_qm31_fold_plan_clear(self._h))
+
+
+class QM31FRIFoldChainPlan(_Plan):
+    """QM31FRIFoldChainPlan (QM31FRIFold.swift:1359-2931): `round_count` folds with
+    explicit challenges, transcript-derived challenges from given commitments, or
+    Merkle-bound commitments and challenges; host and resident forms."""
+
+    _destroy = "azk_fold_chain_plan_destroy"
+
+    def __init__(self, ctx: Context, input_count: int, round_count: int):
+        super().__init__(ctx)
+        self.input_count, self.round_count = input_count, round_count
+        self._check(lib().azk_fold_chain_plan_create(ctx.handle, input_count, round_count, ctypes.byref(self._h)))
+        o, i, l = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().azk_fold_chain_plan_info(self._h, ctypes.byref(o), ctypes.byref(i), ctypes.byref(l)))
+        self.output_count, self.total_inverse_domain_count, self.layer_log_count = o.value, i.value, l.value
+
+    def _inputs(self, evaluations, inverse_layers):
+        ev = _q(evaluations)
+        inv = np.concatenate([_q(l) for l in inverse_layers]) if len(inverse_layers) else np.zeros((0, 4), np.uint32)
+        if len(ev) != self.input_count or len(inverse_layers) != self.round_count or len(inv) != self.total_inverse_domain_count:
+            raise AZKError(1, "evaluations / inverse-domain layers do not match the plan's counts")
+        return ev, np.ascontiguousarray(inv)
+
+    def execute(self, evaluations, inverse_layers, challenges) -> np.ndarray:
+        ev, inv = self._inputs(evaluations, inverse_layers)
+        ch = _q(challenges)
+        if len(ch) != self.round_count:
+            raise AZKError(1, "one challenge per round")
+        out = np.empty((self.output_count, 4), np.uint32)
+        self._check(lib().azk_fold_chain_plan_execute(self._h, _ptr(ev), _ptr(inv), _ptr(ch), _ptr(out), ctypes.byref(self.last_stats)))
+        return out
+
+    def execute_resident(self, dev_evaluations, dev_inverse_layers, dev_final, challenges, evaluations_offset=0, inverse_offset=0,
+                         final_offset=0) -> Stats:
+        ch = _q(challenges)
+        st = Stats()
+        self._check(lib().azk_fold_chain_plan_execute_resident(self._h, dev_evaluations, evaluations_offset, dev_inverse_layers, inverse_offset,
+                                                               dev_final, final_offset, _ptr(ch), ctypes.byref(st)))
+        return st
+
+    def execute_transcript_derived(self, evaluations, inverse_layers, commitments):
+        """Returns (final layer, challenges)."""
+        ev, inv = self._inputs(evaluations, inverse_layers)
+        cm = _u8(b"".join(commitments))
+        if len(commitments) != self.round_count or any(len(c) != 32 for c in commitments):
+            raise AZKError(1, "one 32-byte commitment per round")
+        out = np.empty((self.output_count, 4), np.uint32)
+        ch = np.empty((self.round_count, 4), np.uint32)
+        self._check(lib().azk_fold_chain_plan_execute_transcript(self._h, _ptr(ev), _ptr(inv), _ptr(cm), _ptr(out), _ptr(ch),
+                                                                 ctypes.byref(self.last_stats)))
+        return out, ch
+
+    def execute_transcript_derived_resident(self, dev_evaluations, dev_inverse_layers, dev_commitments, dev_final, commitment_stride=32,
+                                            evaluations_offset=0, inverse_offset=0, commitments_offset=0, final_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_fold_chain_plan_execute_transcript_resident(self._h, dev_evaluations, evaluations_offset, dev_inverse_layers, inverse_offset,
+                                                                          dev_commitments, commitments_offset, commitment_stride, dev_final,
+                                                                          final_offset, ctypes.byref(st)))
+        return st
+
+    def _merkle_out(self):
+        return (np.empty((self.output_count, 4), np.uint32), np.empty(32 * self.round_count, np.uint8),
+                np.empty((self.round_count, 4), np.uint32))
+
+    def _split(self, cm):
+        return [cm[32 * k:32 * k + 32].tobytes() for k in range(self.round_count)]
+
+    def execute_merkle_transcript_derived(self, evaluations, inverse_layers):
+        """Returns (final layer, commitments, challenges)."""
+        ev, inv = self._inputs(evaluations, inverse_layers)
+        out, cm, ch = self._merkle_out()
+        self._check(lib().azk_fold_chain_plan_execute_merkle(self._h, _ptr(ev), _ptr(inv), _ptr(out), _ptr(cm), _ptr(ch), ctypes.byref(self.last_stats)))
+        return out, self._split(cm), ch
+
+    def execute_merkle_transcript_derived_readback(self, dev_evaluations, dev_inverse_layers, evaluations_offset=0, inverse_offset=0):
+        out, cm, ch = self._merkle_out()
+        self._check(lib().azk_fold_chain_plan_execute_merkle_readback(self._h, dev_evaluations, evaluations_offset, dev_inverse_layers, inverse_offset,
+                                                                      _ptr(out), _ptr(cm), _ptr(ch), ctypes.byref(self.last_stats)))
+        return out, self._split(cm), ch
+
+    def execute_merkle_transcript_derived_resident(self, dev_evaluations, dev_inverse_layers, dev_commitments, dev_final, dev_layer_log=None,
+                                                   dev_first_commitment=None, commitment_stride=32, evaluations_offset=0, inverse_offset=0,
+                                                   commitments_offset=0, layer_log_offset=0, first_commitment_offset=0, final_offset=0) -> Stats:
+        st = Stats()
+        self._check(lib().azk_fold_chain_plan_execute_merkle_resident(self._h, dev_evaluations, evaluations_offset, dev_inverse_layers, inverse_offset,
+                                                                      dev_commitments, commitments_offset, commitment_stride, dev_layer_log,
+                                                                      layer_log_offset, dev_first_commitment, first_commitment_offset, dev_final,
+                                                                      final_offset, ctypes.byref(st)))
+        return st
+
+    def challenges(self) -> np.ndarray:
+        ch = np.empty((self.round_count, 4), np.uint32)
+        self._check(lib().azk_fold_chain_plan_challenges(self._h, _ptr(ch)))
+        return ch
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_fold_chain_plan_clear(self._h))
+
+
+class CircleFRIResidentQueryExtractor(_Plan):
+    """CircleFRIResidentQueryExtractorV1 (CircleFRIFoldPlan.swift:1027-1231): query
+    openings from committed layers on the device, in the proof codec's encoding."""
+
+    _destroy = "azk_query_extractor_destroy"
+
+    def __init__(self, ctx: Context, log_size: int, round_count: int):
+        super().__init__(ctx)
+        self.log_size, self.round_count = log_size, round_count
+        self.query_bytes = int(lib().azk_query_extractor_query_bytes(log_size, round_count))
+        self._check(lib().azk_query_extractor_create(ctx.handle, log_size, round_count, ctypes.byref(self._h)))
+
+    def extract_queries(self, dev_layers, commitments, query_pair_indices, layers_offset=0) -> bytes:
+        cm = _u8(b"".join(commitments))
+        if len(commitments) != self.round_count or any(len(c) != 32 for c in commitments):
+            raise AZKError(1, "one 32-byte commitment per round")
+        idx = np.ascontiguousarray(query_pair_indices, dtype=np.uint64)
+        out = np.empty(max(1, len(idx) * self.query_bytes), np.uint8)
+        n = ctypes.c_uint64(out.nbytes)
+        self._check(lib().azk_query_extractor_extract(self._h, dev_layers, layers_offset, _ptr(cm), _ptr(idx), len(idx), _ptr(out), ctypes.byref(n),
+                                                      ctypes.byref(self.last_stats)))
+        return out[: n.value].tobytes()
+
+
 def probe_int_issue(ctx: Context) -> float:
     """Sustained LOP3+SHF 32-bit op rate of the device (ops/s)."""
     v = ctypes.c_double()
@@ -392,6 +543,8 @@ def _sched(schedule):
     s = Schedule(schedule.get("treelet_log", 0), schedule.get("group_log", 0), schedule.get("threads", 0), schedule.get("use_graph", 1))
     for lg, tl in dict(schedule.get("layer_treelet", {})).items():
         s.layer_treelet[int(lg)] = int(tl)
+    for lg, th in dict(schedule.get("layer_threads", {})).items():
+        s.layer_threads[int(lg)] = int(th)
     _keep.append(s)
     return ctypes.byref(s)
 
@@ -555,6 +708,11 @@ class ProofServer:
 
     def _check(self, rc):
         check(rc, self.ctx.handle)
+
+    def group_stats(self) -> dict:
+        g, j = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().azk_server_group_stats(self._h, ctypes.byref(g), ctypes.byref(j)))
+        return {"groups": g.value, "grouped_jobs": j.value, "mean_group": j.value / g.value if g.value else 0.0}
 
     def submit_pcs(self, log_size: int, log_blowup: int, queries: int, rounds: int, coefficients, public_digest: bytes) -> int:
         c = _q(coefficients)

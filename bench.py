@@ -331,7 +331,7 @@ def serving_mix(n_jobs, seed, lo=12, hi=22, sumcheck_every=5):
     return jobs
 
 
-def run_serving(azk, ctx, args, batched_jobs_per_s):
+def run_serving(azk, ctx, args, batched_jobs_per_s, batched_elems_per_s=None):
     """Continuous-batching server on the serving mix.  A backlog and an overloaded
     Poisson run give the server's throughput on this mix; Poisson arrivals at
     `--serve-load` x the batched superstep's jobs/s (the 512-instance leg) give
@@ -421,6 +421,7 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
     s1 = server.stats()
     lat = np.array([r[1] + lag for r, lag in zip(res, lags)])
     kinds = np.array([j[0] for j in mix])
+    groups = server.group_stats()
     server.close()
 
     def pct(v):
@@ -441,6 +442,8 @@ def run_serving(azk, ctx, args, batched_jobs_per_s):
         "latency_all": pct(lat), "latency_pcs": pct(lat[kinds == "pcs"]), "latency_sumcheck": pct(lat[kinds == "sc"]),
         "submit_lag_p99_ms": float(np.percentile(lags, 99) * 1e3), "warmup_s": t_warm,
         "held_gb": s1["held_bytes"] / 2**30,
+        "pcs_groups": groups,
+        "saturated_vs_batched_superstep": sat_elems_s / batched_elems_per_s if batched_elems_per_s else None,
     }
 
 
@@ -683,7 +686,7 @@ def main():
 
     serving = None
     if not args.no_serve and world == 1:
-        serving = run_serving(azk, ctx, args, len(logs) * args.steps / t_dev)
+        serving = run_serving(azk, ctx, args, len(logs) * args.steps / t_dev, value / world)
         print(f"[bench] serving {serving}", file=sys.stderr, flush=True)
 
     line = None

@@ -181,6 +181,89 @@ azk_status azk_qm31_transcript_challenges(azk_ctx* ctx, uint64_t input_count, co
 azk_status azk_circle_merkle_fold_chain(azk_ctx* ctx, uint32_t log_size, const uint32_t* evaluations, uint32_t log_blowup, uint32_t queries,
                                         uint32_t grinding_bits, const uint8_t public_digest[32], uint32_t rounds, uint32_t* final_out,
                                         uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* ---- fold plan handles ----
+ * Resident entry points take (device pointer, byte offset) pairs: each range must
+ * lie inside one device allocation and offsets are multiples of 16 bytes; ranges
+ * the reference forbids to overlap are rejected with AZK_ERR_INVALID_INPUT_LAYOUT
+ * (QM31FRIFold.swift:1236-1294, 2707-2909).  QM31 inverse-domain points are given
+ * as full QM31 values (n/2 per round, concatenated round after round). */
+
+/* QM31FRIFoldPlan (QM31FRIFold.swift:960-1338): one fold of `input_count` (even,
+ * > 1) values. */
+typedef struct azk_qm31_fold_plan azk_qm31_fold_plan;
+azk_status azk_qm31_fold_plan_create(azk_ctx* ctx, uint64_t input_count, azk_qm31_fold_plan** out);
+/* execute(evaluations:inverseDomainPoints:challenge:) (:1027-1055): host arrays. */
+azk_status azk_qm31_fold_plan_execute(azk_qm31_fold_plan* plan, const uint32_t* evaluations, const uint32_t* inverse_points, const uint32_t challenge[4],
+                                      uint32_t* out, azk_stats* stats);
+/* executeResident (:1078-1103): the output may overlap neither input. */
+azk_status azk_qm31_fold_plan_execute_resident(azk_qm31_fold_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                               const void* dev_inverse_points, uint64_t inverse_offset, void* dev_out, uint64_t out_offset,
+                                               const uint32_t challenge[4], azk_stats* stats);
+azk_status azk_qm31_fold_plan_clear(azk_qm31_fold_plan* plan);
+void azk_qm31_fold_plan_destroy(azk_qm31_fold_plan* plan);
+
+/* QM31FRIFoldChainPlan (QM31FRIFold.swift:1359-2931): `rounds` folds of
+ * `input_count` values (every round's input count even and > 1).  The layer log
+ * of the Merkle-bound mode holds each round's input layer, round r at element
+ * offset n + n/2 + ... (r terms); azk_fold_chain_plan_info gives the final-layer,
+ * inverse-domain and layer-log value counts. */
+typedef struct azk_fold_chain_plan azk_fold_chain_plan;
+azk_status azk_fold_chain_plan_create(azk_ctx* ctx, uint64_t input_count, uint32_t rounds, azk_fold_chain_plan** out);
+azk_status azk_fold_chain_plan_info(azk_fold_chain_plan* plan, uint64_t* output_count, uint64_t* inverse_domain_count, uint64_t* layer_log_count);
+/* Explicit challenges (execute / executeResident, :1544-1568, 1693-1721). */
+azk_status azk_fold_chain_plan_execute(azk_fold_chain_plan* plan, const uint32_t* evaluations, const uint32_t* inverse_layers, const uint32_t* challenges,
+                                       uint32_t* final_out, azk_stats* stats);
+azk_status azk_fold_chain_plan_execute_resident(azk_fold_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                const void* dev_inverse_layers, uint64_t inverse_offset, void* dev_final, uint64_t final_offset,
+                                                const uint32_t* challenges, azk_stats* stats);
+/* Challenges derived from caller-given 32-byte round commitments through the QM31
+ * fold transcript (executeTranscriptDerived[Resident], :1582-1614, 1723-1750);
+ * resident commitments sit at `commitment_stride` (>= 32) bytes apart. */
+azk_status azk_fold_chain_plan_execute_transcript(azk_fold_chain_plan* plan, const uint32_t* evaluations, const uint32_t* inverse_layers,
+                                                  const uint8_t* commitments, uint32_t* final_out, uint32_t* challenges_out, azk_stats* stats);
+azk_status azk_fold_chain_plan_execute_transcript_resident(azk_fold_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                           const void* dev_inverse_layers, uint64_t inverse_offset, const void* dev_commitments,
+                                                           uint64_t commitments_offset, uint64_t commitment_stride, void* dev_final, uint64_t final_offset,
+                                                           azk_stats* stats);
+/* Merkle-bound chain: each round's layer committed (SHA3 Merkle, 16-byte QM31
+ * leaves), the root absorbed and the challenge squeezed on the device; input count
+ * a power of two (executeMerkleTranscriptDerived, :1637-1671). */
+azk_status azk_fold_chain_plan_execute_merkle(azk_fold_chain_plan* plan, const uint32_t* evaluations, const uint32_t* inverse_layers, uint32_t* final_out,
+                                              uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* Resident inputs, results read back (executeMerkleTranscriptDerivedReadback, :1828-1855). */
+azk_status azk_fold_chain_plan_execute_merkle_readback(azk_fold_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                       const void* dev_inverse_layers, uint64_t inverse_offset, uint32_t* final_out,
+                                                       uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* Fully resident (executeMerkleTranscriptDerivedResident, :1752-1787): commitments
+ * written to dev_commitments at `commitment_stride`; dev_layer_log (may be NULL)
+ * receives each round's input layer.  With dev_first_commitment (NULL for none;
+ * then dev_layer_log is required) round 0's commitment is that 32-byte root instead
+ * of a tree, and the layer log's first layer may be the evaluations themselves
+ * (executeMerkleTranscriptDerivedResidentWithPrecomputedFirstCommitment, :1789-1826). */
+azk_status azk_fold_chain_plan_execute_merkle_resident(azk_fold_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                       const void* dev_inverse_layers, uint64_t inverse_offset, void* dev_commitments,
+                                                       uint64_t commitments_offset, uint64_t commitment_stride, void* dev_layer_log, uint64_t layer_log_offset,
+                                                       const void* dev_first_commitment, uint64_t first_commitment_offset, void* dev_final,
+                                                       uint64_t final_offset, azk_stats* stats);
+/* Challenges of the plan's last execution (4 limbs per round). */
+azk_status azk_fold_chain_plan_challenges(azk_fold_chain_plan* plan, uint32_t* challenges_out);
+azk_status azk_fold_chain_plan_clear(azk_fold_chain_plan* plan);
+void azk_fold_chain_plan_destroy(azk_fold_chain_plan* plan);
+
+/* CircleFRIResidentQueryExtractorV1 (CircleFRIFoldPlan.swift:1027-1231): query
+ * openings from committed layers already on the device (layer k of 2^(log_size-k)
+ * QM31 values at element offset 2N - 2N/2^k, layers 0 .. rounds-1).  Every layer's
+ * Merkle root must equal commitments[k] (else AZK_ERR_CORRECTNESS_VALIDATION_FAILED);
+ * each pair index is below N/2.  Output: the queries in the proof codec's query
+ * encoding (CircleProofFormat.swift:527-614), azk_query_extractor_query_bytes bytes
+ * each, concatenated. */
+typedef struct azk_query_extractor azk_query_extractor;
+azk_status azk_query_extractor_create(azk_ctx* ctx, uint32_t log_size, uint32_t rounds, azk_query_extractor** out);
+uint64_t azk_query_extractor_query_bytes(uint32_t log_size, uint32_t rounds);
+azk_status azk_query_extractor_extract(azk_query_extractor* extractor, const void* dev_layers, uint64_t layers_offset, const uint8_t* commitments,
+                                       const uint64_t* pair_indices, uint64_t count, uint8_t* queries_out, uint64_t* out_len, azk_stats* stats);
+void azk_query_extractor_destroy(azk_query_extractor* extractor);
+
 /* Sustained LOP3 + SHF (funnel shift) issue rate of the device, 32-bit ops per
  * second, from a probe kernel of independent chains: the integer roofline of
  * the Keccak-bound kernels (no counterpart in the reference). */
@@ -199,6 +282,10 @@ typedef struct azk_schedule {
   /* Per-layer override: layer_treelet[L] (nonzero) is the treelet depth for a
    * committed layer of 2^L leaves; the autotuner fills this table. */
   uint8_t layer_treelet[32];
+  /* Per-layer threads per CTA of the commit kernel (128, 256 or 512; 0 = `threads`)
+   * for a committed layer of 2^L leaves; a launch that commits several layers takes
+   * the entry of its largest one.  The autotuner fills this table too. */
+  uint16_t layer_threads[32];
 } azk_schedule;
 
 azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,
@@ -293,11 +380,15 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evaluations, uint64_
 
 /* ---- continuous-batching server (no counterpart in the reference) ----
  * Jobs enter one FIFO queue; `slots` workers, each with its own CUDA stream, take
- * the next job as soon as its device memory fits `hbm_budget_bytes`, so jobs that
+ * the front job as soon as its device memory fits `hbm_budget_bytes`, so jobs that
  * arrive while others run are admitted as slots and memory free up and their
- * kernels overlap on the device.  A job larger than the whole budget is refused
- * with AZK_ERR_HBM_BUDGET at submission.  Results equal those of the single-job
- * entry points (each job's kernels are the same; only their overlap differs). */
+ * kernels overlap on the device.  A worker takes a PCS job together with the other
+ * queued PCS jobs of its shape (up to 8 below 2^18 values, fewer above) and proves
+ * them as one batched superstep; sum-check jobs go to a lane that proves the
+ * waiting tables in batched launches on its own streams.  A job larger than the
+ * whole budget is refused with AZK_ERR_HBM_BUDGET at submission.  Results equal
+ * those of the single-job entry points (the same kernels; only their grouping and
+ * overlap differ). */
 typedef struct azk_server azk_server;
 azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t slots, const azk_schedule* schedule, azk_server** out);
 /* Before serving: every worker runs, once, a job of zeros of each listed shape (PCS
@@ -323,6 +414,8 @@ azk_status azk_server_poll(azk_server* sv, uint64_t job_id, int* state, double* 
 azk_status azk_server_release(azk_server* sv, uint64_t job_id);
 azk_status azk_server_wait_all(azk_server* sv);
 azk_status azk_server_stats(azk_server* sv, uint64_t* completed, uint64_t* elems, double* span_s, uint64_t* reserved_bytes);
+/* PCS groups proved so far and the jobs they held (jobs / groups = mean group size). */
+azk_status azk_server_group_stats(azk_server* sv, uint64_t* groups, uint64_t* grouped_jobs);
 void azk_server_destroy(azk_server* sv);
 
 /* ---- autotuner and learned cost model (the reference's planner races a few
@@ -333,6 +426,31 @@ void azk_server_destroy(azk_server* sv);
  * each leaf as a fold of a previous layer first) or 64 (raw 64-byte leaves). */
 azk_status azk_tuner_time_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent, uint32_t tile_log,
                                uint32_t group_log, uint32_t threads, uint32_t reps, double* seconds);
+
+/* One schedule of the commit kernel, and what a race measured for it. */
+typedef struct azk_tuner_candidate {
+  uint32_t tile_log, group_log, threads, reserved;
+} azk_tuner_candidate;
+typedef struct azk_tuner_measurement {
+  double median_gpu_s, p95_gpu_s, median_submit_s;
+  uint32_t passed_gate; /* 0: the candidate's roots differed from the host's; not timed */
+  uint32_t runs;
+} azk_tuner_measurement;
+/* Correctness-gated race over candidate schedules for one tree shape
+ * (MetalProofPlanner.measureMerkleCandidate, Planner/MetalProofPlanner.swift:367-418):
+ * a seeded random input is committed by every candidate and its roots compared with
+ * the host's (the library's own host Keccak); passing candidates run warmup_runs +
+ * measured_runs more times, each checked, and *winner is the one with the lowest
+ * median device time plus median submit time.  Fails with
+ * AZK_ERR_CORRECTNESS_VALIDATION_FAILED if no candidate passes. */
+azk_status azk_tuner_race_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent,
+                               const azk_tuner_candidate* candidates, uint32_t count, uint32_t warmup_runs, uint32_t measured_runs, uint64_t seed,
+                               azk_tuner_measurement* out, uint32_t* winner);
+/* Randomized validation of a winner before it is persisted
+ * (validateMerkleWinnerForPersistence, :447-484): `batches` fresh seeded inputs, each
+ * committed and compared with the host's roots. */
+azk_status azk_tuner_validate_tree(azk_ctx* ctx, uint32_t log_leaves, uint32_t leaf_bytes, uint32_t fold, uint32_t concurrent,
+                                   const azk_tuner_candidate* winner, uint32_t batches, uint64_t seed);
 
 typedef struct azk_mlp azk_mlp;
 /* Fully connected network dims[0] -> ... -> dims[n_layers] (= 1), ReLU hidden

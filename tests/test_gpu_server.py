@@ -161,3 +161,44 @@ def test_idle_workers_give_back_memory_for_a_larger_job(ctx):
     assert got[bid][0] == azk.CirclePCSFRIProver(ctx, 16, 2, big["queries"], big["rounds"]).prove_coefficients(big["coeffs"], big["pub"])
     for j, i in zip(small, ids):
         assert first[i][0] == azk.CirclePCSFRIProver(ctx, j["log_size"], 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])
+
+
+def test_queued_jobs_of_one_shape_are_proved_as_one_group(ctx, oracle):
+    """Same-shape PCS jobs waiting together are taken as one group and proved by one
+    batched superstep; every job's proof is still the one it gives alone, and a job
+    of another shape queued among them keeps its own bytes."""
+    rng = np.random.default_rng(0x6A0)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=4 << 30, slots=1)
+    jobs = [_pcs_job(rng, 12) for _ in range(12)] + [_pcs_job(rng, 14)] + [_pcs_job(rng, 12) for _ in range(5)]
+    ids = [server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]) for j in jobs]
+    sc = rng.integers(0, P, 1 << 12, dtype=np.uint32)
+    sid = server.submit_sumcheck(sc)
+    res = _wait(server, ids + [sid])
+    gs = server.group_stats()
+    server.close()
+    assert gs["grouped_jobs"] == len(jobs) and gs["groups"] < len(jobs)
+    for j, i in zip(jobs, ids):
+        assert res[i][0] == azk.CirclePCSFRIProver(ctx, j["log_size"], 2, j["queries"], j["rounds"]).prove_coefficients(j["coeffs"], j["pub"])
+    full = np.zeros((1 << 12, 4), np.uint32)
+    full[: len(jobs[0]["coeffs"])] = jobs[0]["coeffs"]
+    assert res[ids[0]][0] == oracle.prove(12, oracle.fft_evaluate(12, full), 2, jobs[0]["queries"], jobs[0]["pub"], jobs[0]["rounds"]).proof
+    want = oracle.sumcheck_multilinear(sc)
+    assert res[sid][0]["initial_digest"] == want["initial_digest"] and np.array_equal(res[sid][0]["challenges"], want["challenges"])
+
+
+def test_sumcheck_lane_batches_many_tables(ctx, oracle):
+    """Many sum-check tables in flight at once (several per batched launch) each give
+    the oracle's proof."""
+    rng = np.random.default_rng(0x5C5)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=4 << 30, slots=2)
+    tables = [rng.integers(0, P, 1 << int(rng.integers(8, 15)), dtype=np.uint32) for _ in range(40)]
+    ids = [server.submit_sumcheck(t) for t in tables]
+    res = _wait(server, ids)
+    server.close()
+    for t, i in zip(tables, ids):
+        want = oracle.sumcheck_multilinear(t)
+        got = res[i][0]
+        assert got["claimed_sum"] == want["claimed_sum"] and got["final"] == want["final"]
+        assert got["initial_digest"] == want["initial_digest"]
+        for key in ("r0", "r1", "challenges"):
+            assert np.array_equal(got[key], want[key])

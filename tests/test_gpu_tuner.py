@@ -95,3 +95,38 @@ def test_layer_table_schedules_give_identical_proofs(ctx, oracle):
     table = {lg: max(1, lg - 4) for lg in range(1, 15)}
     p = azk.CirclePCSFRIProver(ctx, 14, 2, 16, 8, schedule=dict(layer_treelet=table))
     assert p.prove_evaluations(ev, pub) == oracle.prove(14, ev, 2, 16, pub, 8).proof
+
+
+@pytest.mark.parametrize("shape", [(10, 16, 1, 1), (12, 16, 0, 8), (11, 64, 0, 2)])
+def test_race_gates_on_host_roots_and_validates_winner(ctx, shape):
+    """Every candidate schedule reproduces the host's roots (none fails the gate),
+    the winner has the lowest device-plus-submit median, and it survives randomized
+    validation on fresh inputs."""
+    cands = [(t, th) for t in (2, min(6, shape[0]), min(9, shape[0])) for th in (128, 256, 512)]
+    ms, win = T.race(ctx, shape, cands, warmup=1, runs=5, seed=3)
+    assert all(m["passed_gate"] and m["runs"] == 5 for m in ms)
+    score = [m["median_gpu_s"] + m["median_submit_s"] for m in ms]
+    assert win == int(np.argmin(score))
+    assert all(m["p95_gpu_s"] >= m["median_gpu_s"] > 0 for m in ms)
+    T.validate(ctx, shape, cands[win], batches=3, seed=11)
+
+
+def test_plan_races_model_candidates_and_persists(ctx, tmp_path):
+    shapes = [(lg, 16, 1, 1) for lg in (8, 9, 10, 11, 12)]
+    recs = T.collect(ctx, shapes, threads=(128, 256), reps=2)
+    tuner = T.Tuner(ctx, recs)
+    tuner.train(steps=800)
+    store = T.PlanStore(str(tmp_path / "plans.json"))
+    got = tuner.plan((10, 16, 1, 1), store=store, top=3)
+    assert store.winner((10, 16, 1, 1)) == tuple(got)
+    rec = store.records[store.key((10, 16, 1, 1))]
+    assert rec["candidates"] == 3 and rec["failed_gate"] == 0
+    store.save()
+    again = T.PlanStore(str(tmp_path / "plans.json"))
+    assert tuner.plan((10, 16, 1, 1), store=again) == tuple(got)  # reused, no race
+    # sustained slower live timings make the record stale; the next plan races again
+    for _ in range(again.min_samples):
+        again.record_live((10, 16, 1, 1), 3 * rec["median_gpu_s"], rec["median_submit_s"])
+    assert (10, 16, 1, 1) in again.stale_shapes()
+    tuner.plan((10, 16, 1, 1), store=again, top=2)
+    assert again.records[again.key((10, 16, 1, 1))]["candidates"] == 2 and not again.stale_shapes()

@@ -33,3 +33,29 @@ def test_exported_tables_are_valid_depths():
     assert rep["records"] >= 2000
     # the learned choice beats the fixed-depth heuristic on the held-out sizes
     assert rep["regret_unseen"]["model"]["mean"] < rep["regret_unseen"]["heuristic"]["mean"]
+
+
+def test_plan_store_drift_policy(tmp_path):
+    """Live timings near the raced median keep a plan; a sustained shift beyond the
+    threshold marks it stale only after the minimum number of samples; a new race
+    clears the observation (PlanDatabase.recordLiveObservation semantics)."""
+    store = T.PlanStore(str(tmp_path / "p.json"), alpha=0.2, min_samples=8, threshold=0.25)
+    shape = (14, 16, 1, 1)
+    meas = [{"tile": 9, "threads": 256, "passed_gate": True, "median_gpu_s": 1e-3, "p95_gpu_s": 1.2e-3, "median_submit_s": 1e-5, "runs": 5}]
+    store.record_race(shape, meas, 0)
+    for k in range(20):
+        st = store.record_live(shape, 1e-3 * (1.05 if k % 2 else 0.95), 1e-5)
+    assert not st["stale"] and not store.stale_shapes()
+    for k in range(7):
+        st = store.record_live(shape, 2e-3, 1e-5)
+    assert st["stale"]
+    fresh = T.PlanStore(str(tmp_path / "q.json"), min_samples=8)
+    fresh.record_race(shape, meas, 0)
+    for k in range(7):
+        assert not fresh.record_live(shape, 5e-3, 1e-5)["stale"]  # fewer samples than the minimum
+    assert fresh.record_live(shape, 5e-3, 1e-5)["stale"]
+    store.save()
+    again = T.PlanStore(str(tmp_path / "p.json"))
+    assert again.stale_shapes() == [shape] and again.winner(shape) == (9, 256)
+    again.record_race(shape, meas, 0)
+    assert not again.stale_shapes()
