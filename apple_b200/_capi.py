@@ -38,7 +38,7 @@ class Stats(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     _fields_ = [("treelet_log", ctypes.c_uint32), ("group_log", ctypes.c_uint32), ("threads", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
-                ("layer_treelet", ctypes.c_uint8 * 32), ("layer_threads", ctypes.c_uint16 * 32)]
+                ("layer_treelet", ctypes.c_uint8 * 32), ("layer_threads", ctypes.c_uint16 * 32), ("persistent_trees", ctypes.c_uint32)]
 
 
 class TunerCandidate(ctypes.Structure):

@@ -198,8 +198,10 @@ cudaError_t launch_keccak_permute(const uint8_t* in, uint64_t in_stride, uint8_t
                                   uint32_t threads, cudaStream_t s);
 cudaError_t launch_hash_batch(const uint8_t* in, uint64_t stride, uint32_t len, uint32_t suffix, uint8_t* out, uint64_t out_stride,
                               uint64_t count, uint32_t threads, cudaStream_t s);
+// `d_queue` (two zeroed words, or null): launch the persistent form, whose resident
+// CTAs pull work items from that counter; null: one CTA per work item.
 cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t raw_kind,
-                             uint32_t threads, cudaStream_t s);
+                             uint32_t threads, cudaStream_t s, uint32_t* d_queue = nullptr);
 cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, uint32_t nidx, uint64_t* d_out, cudaStream_t s);
 cudaError_t launch_domain_tables(uint32_t logn, uint32_t* d_tw, uint32_t* d_inv, cudaStream_t s);
 cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
@@ -220,20 +222,23 @@ uint64_t witness_partial_values(uint64_t n);
 // kFftM31Low: the low-stage last pass of one-limb transforms above 2^12, bulk-copied
 // tiles in a persistent kernel (fft_m31_low_tma_kernel), which raises *status when
 // a bounded wait on its copies runs out.
-enum FftKind : uint32_t { kFftQM31 = 0, kFftM31Small = 1, kFftM31Tile = 2, kFftM31Low = 3, kFftKinds = 4 };
+// kFftQ4Tile: four-limb tiles of transforms of 2^12 values or more that are not
+// lifted M31 polynomials (fft_q_tile_kernel); kFftQM31 then serves the smaller ones.
+enum FftKind : uint32_t { kFftQM31 = 0, kFftM31Small = 1, kFftM31Tile = 2, kFftM31Low = 3, kFftQ4Tile = 4, kFftKinds = 5 };
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t kind, uint32_t* d_status, cudaStream_t s);
 cudaError_t prepare_fft_m31_kernels();
 cudaError_t launch_fft_m31_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 cudaError_t launch_fft_m31_low(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t* d_status, cudaStream_t s);
+cudaError_t launch_fft_q_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 // Which kernel runs pass `pass` of a transform of 2^logn values, and how many
 // work items (tiles) it has.
 inline uint32_t fft_pass_kind(uint32_t logn, uint32_t pass, bool narrow) {
-  if (!narrow) return kFftQM31;
+  if (!narrow) return logn < kFftLowBits ? kFftQM31 : kFftQ4Tile;
   if (logn < kFftLowBits) return kFftM31Small;
   return (pass == fft_high_chunks(logn) && pass > 0) ? kFftM31Low : kFftM31Tile;
 }
 inline uint64_t fft_kind_tiles(uint32_t logn, uint32_t pass, uint32_t kind) {
-  return (kind == kFftM31Tile || kind == kFftM31Low) ? (1ull << (logn - kFftLowBits)) : fft_pass_tiles(logn, pass);
+  return (kind == kFftM31Tile || kind == kFftM31Low || kind == kFftQ4Tile) ? (1ull << (logn - kFftLowBits)) : fft_pass_tiles(logn, pass);
 }
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets

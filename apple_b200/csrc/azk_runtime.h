@@ -222,6 +222,7 @@ struct Sched {
   bool graph = true;
   uint8_t layer_tile[32] = {0};
   uint16_t layer_threads[32] = {0};
+  bool persistent_trees = false;
 };
 // A schedule with no treelet depth and no layer table takes `defaults` (a tuned
 // per-layer table from azk_tuned.h) when one is given, and with no thread count

@@ -454,6 +454,8 @@ cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t 
       return launch_fft_m31_tiles(d_jobs, d_work, nwork, s);
     case kFftM31Low:
       return launch_fft_m31_low(d_jobs, d_work, nwork, d_status, s);
+    case kFftQ4Tile:
+      return launch_fft_q_tiles(d_jobs, d_work, nwork, s);
     default:
       return cudaErrorInvalidValue;
   }

@@ -16,7 +16,7 @@
 // straight from the domain table: the 2^(3-k) twiddles of the stage on owned bit
 // k are consecutive table entries, loaded as one vector.
 //
-// Two kernels:
+// Kernels:
 //  - fft_m31_tile_kernel: one CTA per tile.  First passes read the a limbs of the
 //    QM31 coefficients (only the nonzero prefix), later high-stage passes the
 //    one-word exchange buffer; the pass writes the exchange buffer, or the QM31
@@ -28,6 +28,8 @@
 //    next tile as soon as the current tile's first sub-pass has read its copy, so
 //    the load runs under the remaining sub-passes.  Every wait on the mbarrier is
 //    bounded: a wait that runs out raises `status` and the CTA returns.
+//  - fft_q_tile_kernel: the same tiles over QM31 values (inputs that are not lifted
+//    M31 polynomials), in place in the codeword buffer between passes.
 #include "azk_field.cuh"
 #include "azk_internal.h"
 
@@ -102,8 +104,15 @@ __device__ __forceinline__ Pass make_pass(const FftJob& job, uint64_t tile) {
 // The stage of sub-pass Q on owned bit K (L bit 4Q + K) over the thread's 16
 // values v[b] (bit k of b = L bit 4Q + k; Lbase = the thread's L with those bits
 // zero): 8 butterflies with the 2^(3-K) twiddles of the stage's blocks above it.
-template <int Q, int K>
-__device__ __forceinline__ void stage(uint32_t (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw) {
+__device__ __forceinline__ void bfly(qm31& l, qm31& r, uint32_t t) {
+  const qm31 rt = q_mul_m31(r, t);
+  const qm31 a = q_add(l, rt);
+  r = q_sub(l, rt);
+  l = a;
+}
+
+template <int Q, int K, class V>
+__device__ __forceinline__ void stage(V (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw) {
   const uint32_t j = 4 * Q + K - p.c;  // row bit = stage s_lo + j
   const uint32_t s = p.s_lo + j;
   const uint64_t base = twoff(p.logn, s) + (p.hi << (p.m - 1 - j)) + ((uint64_t)(Lbase >> p.c) >> (j + 1));
@@ -118,8 +127,8 @@ __device__ __forceinline__ void stage(uint32_t (&v)[16], uint32_t Lbase, const P
 
 // Stages of sub-pass Q from owned bit `kstart` down; owned bits below the pass's
 // column count are columns (no butterflies).
-template <int Q>
-__device__ __forceinline__ void subpass(uint32_t (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw, int kstart) {
+template <int Q, class V>
+__device__ __forceinline__ void subpass(V (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw, int kstart) {
   if (kstart >= 3 && 4 * Q + 3 >= p.c) stage<Q, 3>(v, Lbase, p, tw);
   if (kstart >= 2 && 4 * Q + 2 >= p.c) stage<Q, 2>(v, Lbase, p, tw);
   if (kstart >= 1 && 4 * Q + 1 >= p.c) stage<Q, 1>(v, Lbase, p, tw);
@@ -220,6 +229,89 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob*
   finish_tile(Y, job, p, last);
 }
 
+// ---------------------------------------------------------------------------
+// Four-limb (QM31) tiles for transforms of 2^12 values or more whose inputs are
+// not lifted M31 polynomials: the same sub-passes over 16-byte values.  The
+// shared buffer holds 4096 values (64 KB) placed by swq, which flips bits 0-2 by
+// bits 4-6, so the 16-byte accesses of all three sub-passes (a quarter warp spans
+// L bits 0-2 in sub-passes 2 and 1 and bits 4-6 in sub-pass 0) fall in 8 distinct
+// 16-byte bank groups.  The first pass reads the coefficients (the nonzero prefix)
+// and writes the codeword buffer; later passes read and write it in place (each
+// tile only its own values).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t swq(uint32_t L) { return L ^ ((L >> 4) & 7u); }
+__device__ __forceinline__ qm31 to_q(uint4 v) { return qm31{v.x, v.y, v.z, v.w}; }
+__device__ __forceinline__ uint4 from_q(qm31 v) { return make_uint4(v.a, v.b, v.c, v.d); }
+
+__global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  extern __shared__ __align__(16) uint4 Yq[];  // kTile values
+  const uint2 w = work[blockIdx.x];
+  const FftJob& job = jobs[w.x];
+  const Pass p = make_pass(job, w.y);
+  const uint64_t N = 1ull << p.logn;
+  const bool first = job.pass == 0;
+  const bool last = job.pass == fft_high_chunks(p.logn);
+  const uint64_t count = (job.info != nullptr && job.info->count != 0) ? job.info->count : N;
+  const bool top_zero = first && p.m >= 2 && count <= (N >> 2);
+  const uint32_t t = threadIdx.x;
+  const uint32_t LA = t;
+  qm31 v[16];
+  if (first) {
+    const int loads = top_zero ? 4 : 16;
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+      if (b >= loads) {
+        v[b] = v[b & 3];
+        continue;
+      }
+      const uint64_t gi = p.gidx(LA | ((uint32_t)b << 8));
+      v[b] = gi < count ? to_q(__ldg(job.in + gi)) : qm31{0u, 0u, 0u, 0u};
+    }
+  } else {
+#pragma unroll
+    for (int b = 0; b < 16; b++) v[b] = to_q(job.out[p.gidx(LA | ((uint32_t)b << 8))]);
+  }
+  subpass<2>(v, LA, p, job.tw, top_zero ? 1 : 3);
+  if (p.c >= 8) {
+#pragma unroll
+    for (int b = 0; b < 16; b++) job.out[p.gidx(LA | ((uint32_t)b << 8))] = from_q(v[b]);
+    return;
+  }
+#pragma unroll
+  for (int b = 0; b < 16; b++) Yq[swq(LA | ((uint32_t)b << 8))] = from_q(v[b]);
+  __syncthreads();
+  const uint32_t LB = (t & 15u) | ((t >> 4) << 8);
+#pragma unroll
+  for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LB | ((uint32_t)b << 4))]);
+  subpass<1>(v, LB, p, job.tw, 3);
+  if (p.c >= 4) {
+#pragma unroll
+    for (int b = 0; b < 16; b++) job.out[p.gidx(LB | ((uint32_t)b << 4))] = from_q(v[b]);
+    return;
+  }
+#pragma unroll
+  for (int b = 0; b < 16; b++) Yq[swq(LB | ((uint32_t)b << 4))] = from_q(v[b]);
+  __syncthreads();
+  const uint32_t LC = t << 4;
+#pragma unroll
+  for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LC | (uint32_t)b)]);
+  subpass<0>(v, LC, p, job.tw, 3);
+  if (!last) {
+#pragma unroll
+    for (int b = 0; b < 16; b++) job.out[p.gidx(LC | (uint32_t)b)] = from_q(v[b]);
+    return;
+  }
+  // the last pass (c = 0): coalesced rows through the shared buffer
+#pragma unroll
+  for (int b = 0; b < 16; b++) Yq[swq(LC | (uint32_t)b)] = from_q(v[b]);
+  __syncthreads();
+#pragma unroll 4
+  for (uint32_t r = 0; r < 16; r++) {
+    const uint32_t L = t + kThreads * r;
+    job.out[p.gbase + L] = Yq[swq(L)];
+  }
+}
+
 // ---- bulk copy + mbarrier (PTX ISA: cp.async.bulk, mbarrier) ----
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -309,7 +401,8 @@ int g_low_grid[64] = {0};  // resident CTAs of the persistent kernel, per device
 
 cudaError_t prepare_fft_m31_kernels() {
   int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e;
+  cudaError_t e = cudaFuncSetAttribute(fft_q_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kTile * sizeof(uint4)));
+  if (e != cudaSuccess) return e;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_m31_low_tma_kernel, kThreads, 0)) != cudaSuccess) return e;
@@ -320,6 +413,12 @@ cudaError_t prepare_fft_m31_kernels() {
 cudaError_t launch_fft_m31_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s) {
   if (nwork == 0) return cudaSuccess;
   fft_m31_tile_kernel<<<nwork, kThreads, 0, s>>>(d_jobs, d_work);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fft_q_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s) {
+  if (nwork == 0) return cudaSuccess;
+  fft_q_tile_kernel<<<nwork, kThreads, kTile * sizeof(uint4), s>>>(d_jobs, d_work);
   return cudaGetLastError();
 }
 

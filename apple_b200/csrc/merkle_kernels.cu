@@ -292,6 +292,32 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) tree_tiles_kernel(cons
   tree_tile_body<KIND, THREADS>(jobs[w.x], w.y);
 }
 
+// Persistent form: a grid of the resident CTAs pulls work items from a device
+// counter (queue[0]) until the list is done.  Nothing waits on anything: the
+// last-arriver climb is unchanged, and the last CTA to leave (queue[1] counts
+// them) resets both counters, so a captured launch sequence replays.
+template <uint32_t KIND, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) tree_queue_kernel(const TreeJob* __restrict__ jobs, const uint2* __restrict__ work,
+                                                                            uint32_t nwork, uint32_t* __restrict__ queue) {
+  __shared__ uint32_t s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();  // every thread has the item (and the last one's shared memory is free)
+    if (item >= nwork) break;
+    const uint2 w = work[item];
+    tree_tile_body<KIND, THREADS>(jobs[w.x], w.y);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+      queue[0] = 0;
+      queue[1] = 0;
+    }
+  }
+}
+
 // Single job passed by value, tile = blockIdx.x: needs no job or work-list buffer.
 template <uint32_t KIND, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) tree_direct_kernel(const TreeJob job) {
@@ -305,6 +331,10 @@ template <uint32_t KIND>
 static cudaError_t prepare_kind() {
   cudaError_t e = cudaSuccess;
   for (auto k : {tree_tiles_kernel<KIND, 128>, tree_tiles_kernel<KIND, 256>, tree_tiles_kernel<KIND, 512>}) {
+    cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTreeSmem);
+    if (r != cudaSuccess) e = r;
+  }
+  for (auto k : {tree_queue_kernel<KIND, 128>, tree_queue_kernel<KIND, 256>, tree_queue_kernel<KIND, 512>}) {
     cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTreeSmem);
     if (r != cudaSuccess) e = r;
   }
@@ -323,9 +353,34 @@ cudaError_t prepare_tree_kernels() {
   return e;
 }
 
+// Resident CTAs of a persistent launch: the occupancy of the kernel at this
+// shared-memory size times the SMs, no more than the work items.
+template <class K>
+static uint32_t resident_grid(K kernel, int threads, size_t smem, uint32_t nwork) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+    if (sms < 1) sms = 148;
+  }
+  const uint64_t g = (uint64_t)sms * (uint64_t)per_sm;
+  return (uint32_t)(g < nwork ? g : nwork);
+}
+
 template <uint32_t KIND>
-static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t threads, cudaStream_t s) {
+static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t threads, uint32_t* queue,
+                               cudaStream_t s) {
   size_t smem = max_tile_log >= 2 ? ((size_t)12 << max_tile_log) : 48;  // T/4 digests + T/8 digests
+  if (queue) {
+    if (threads == 128)
+      tree_queue_kernel<KIND, 128><<<resident_grid(tree_queue_kernel<KIND, 128>, 128, smem, nwork), 128, smem, s>>>(d_jobs, d_work, nwork, queue);
+    else if (threads == 512)
+      tree_queue_kernel<KIND, 512><<<resident_grid(tree_queue_kernel<KIND, 512>, 512, smem, nwork), 512, smem, s>>>(d_jobs, d_work, nwork, queue);
+    else
+      tree_queue_kernel<KIND, 256><<<resident_grid(tree_queue_kernel<KIND, 256>, 256, smem, nwork), 256, smem, s>>>(d_jobs, d_work, nwork, queue);
+    return cudaGetLastError();
+  }
   if (threads == 128)
     tree_tiles_kernel<KIND, 128><<<nwork, 128, smem, s>>>(d_jobs, d_work);
   else if (threads == 512)
@@ -336,16 +391,16 @@ static cudaError_t launch_kind(const TreeJob* d_jobs, const uint2* d_work, uint3
 }
 
 cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t max_tile_log, uint32_t kind, uint32_t threads,
-                             cudaStream_t s) {
+                             cudaStream_t s, uint32_t* d_queue) {
   if (nwork == 0) return cudaSuccess;
   if (max_tile_log > kMaxTreeLog) return cudaErrorInvalidValue;
   switch (kind) {
-    case kLeafRaw: return launch_kind<kLeafRaw>(d_jobs, d_work, nwork, max_tile_log, threads, s);
-    case kLeafQM31: return launch_kind<kLeafQM31>(d_jobs, d_work, nwork, max_tile_log, threads, s);
-    case kLeafFold: return launch_kind<kLeafFold>(d_jobs, d_work, nwork, max_tile_log, threads, s);
-    case kLeafDigest: return launch_kind<kLeafDigest>(d_jobs, d_work, nwork, max_tile_log, threads, s);
-    case kLeafQM31x4: return launch_kind<kLeafQM31x4>(d_jobs, d_work, nwork, max_tile_log, threads, s);
-    case kLeafFoldx4: return launch_kind<kLeafFoldx4>(d_jobs, d_work, nwork, max_tile_log, threads, s);
+    case kLeafRaw: return launch_kind<kLeafRaw>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
+    case kLeafQM31: return launch_kind<kLeafQM31>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
+    case kLeafFold: return launch_kind<kLeafFold>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
+    case kLeafDigest: return launch_kind<kLeafDigest>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
+    case kLeafQM31x4: return launch_kind<kLeafQM31x4>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
+    case kLeafFoldx4: return launch_kind<kLeafFoldx4>(d_jobs, d_work, nwork, max_tile_log, threads, d_queue, s);
     default: return cudaErrorInvalidValue;
   }
 }

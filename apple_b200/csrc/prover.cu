@@ -68,7 +68,7 @@ struct Engine {
   std::vector<uint64_t> off_input, off_layers, off_trees, off_tr, off_ch, off_cm, off_qp, off_claim, off_proof, off_cnt;
   std::vector<uint64_t> proof_len, proof_off;
   uint64_t proof_total = 0;
-  uint64_t off_inst = 0, off_flag = 0, off_info = 0;
+  uint64_t off_inst = 0, off_flag = 0, off_info = 0, off_queue = 0;  // off_queue: two words per round (persistent trees)
 
   std::vector<PcsInstance> h_inst;
   // FFT
@@ -258,6 +258,7 @@ struct Engine {
     off_inst = arena.reserve(sizeof(PcsInstance) * n);
     off_flag = arena.reserve(16);
     off_info = arena.reserve(sizeof(InputInfo) * n);
+    off_queue = arena.reserve(8ull * (rmax + 1));
     arena.commit("PCS.Arena");
     // counters and inputs start at zero
     AZK_CU(cudaMemsetAsync(arena.buf.p, 0, arena.used, s));
@@ -410,7 +411,7 @@ struct Engine {
   void launch_tree_range(uint32_t k, uint64_t off, uint64_t cnt, uint32_t lg) {
     if (!cnt) return;
     AZK_CU(launch_tree_jobs(d_tree_jobs.as<TreeJob>(), d_tree_work.as<uint2>() + off, (uint32_t)cnt, tstep_tile[k], tree_kind(k),
-                            tree_threads(sched, lg), s));
+                            tree_threads(sched, lg), s, sched.persistent_trees ? arena.at<uint32_t>(off_queue) + 2 * k : nullptr));
   }
   uint32_t layer_log(uint32_t i, uint32_t k) const { return cfg[i].logn - k - (leaf_values == 4 ? 2 : 0); }
   void launch_fold_range(uint64_t off, uint64_t cnt) {

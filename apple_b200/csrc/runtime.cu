@@ -43,6 +43,7 @@ Sched azk::resolve_schedule(const azk_schedule* s, const uint8_t* defaults, cons
     if (s->group_log) r.group_log = s->group_log;
     if (s->threads) r.threads = s->threads;
     r.graph = s->use_graph != 0;
+    r.persistent_trees = s->persistent_trees != 0;
     for (int i = 0; i < 32; i++) {
       r.layer_tile[i] = s->layer_treelet[i];
       any_layer |= r.layer_tile[i] != 0;
@@ -401,10 +402,15 @@ struct azk_codeword_plan {
   uint32_t logn;
   DevBuf coeff, out;
   FftPlan fft;
+  azk_witness_plan* wit = nullptr;  // monomials -> FFT basis on the device (made on first use)
   ~azk_codeword_plan() {
+    if (wit) azk_witness_plan_destroy(wit);
     if (s) cudaStreamDestroy(s);
   }
 };
+// Host monomial columns -> interleaved FFT-basis coefficients in device memory
+// `dout` (2 * capacity QM31), through the witness plan's kernels; returns when done.
+static void witness_columns_to_device(azk_witness_plan* w, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny, void* dout);
 
 static cudaStream_t new_stream() {
   cudaStream_t s;
@@ -825,13 +831,35 @@ azk_status azk_codeword_plan_execute(azk_codeword_plan* p, const uint32_t* coeff
   });
 }
 
+// execute(polynomial:) (CircleCodeword.swift:460-475): the monomial columns become
+// FFT-basis coefficients on the device (the witness plan's closed-form Chebyshev
+// and line-basis kernels, domains up to 2^22), then the FFT.  Larger domains keep
+// the reference's host conversion (CircleCodeword.swift:187-263).
 azk_status azk_codeword_plan_execute_polynomial(azk_codeword_plan* p, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny, uint32_t* codeword,
                                                 azk_stats* st) {
   return guarded(p ? p->ctx : nullptr, [&] {
     layout(p && codeword && (x || !nx) && (y || !ny));
-    std::vector<uint32_t> c = fft_basis_from_monomials(p->logn, x, nx, y, ny);
-    azk_status s = azk_codeword_plan_execute(p, c.data(), c.size() / 4, codeword, st);
-    if (s != AZK_OK) fail(s, azk_last_error_message(p->ctx));
+    if (p->logn > 22 || nx + ny == 0) {
+      std::vector<uint32_t> c = fft_basis_from_monomials(p->logn, x, nx, y, ny);
+      azk_status s = azk_codeword_plan_execute(p, c.data(), c.size() / 4, codeword, st);
+      if (s != AZK_OK) fail(s, azk_last_error_message(p->ctx));
+      return;
+    }
+    const uint64_t half = (1ull << p->logn) / 2;
+    layout(nx <= half && ny <= half, "each coefficient column holds at most half the domain size");
+    for (uint64_t i = 0; i < 4 * nx; i++) layout(x[i] < kP, "input contains a non-canonical field element");
+    for (uint64_t i = 0; i < 4 * ny; i++) layout(y[i] < kP, "input contains a non-canonical field element");
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    if (!p->wit) {
+      azk_status s = azk_witness_plan_create(p->ctx, p->logn, &p->wit);
+      if (s != AZK_OK) fail(s, azk_last_error_message(p->ctx));
+    }
+    witness_columns_to_device(p->wit, x, nx, y, ny, p->coeff.p);
+    codeword_run(p, p->coeff.as<uint4>(), p->out.as<uint4>(), st, t);
+    AZK_CU(cudaMemcpyAsync(codeword, p->out.p, 16ull << p->logn, cudaMemcpyDeviceToHost, p->s));
+    sync_stream(p->s);
   });
 }
 
@@ -876,6 +904,15 @@ static void witness_run(azk_witness_plan* p, const uint4* x, uint64_t nx, const 
                                   p->px.as<uint4>(), p->py.as<uint4>(), p->cx.as<uint4>(), p->cy.as<uint4>(), out, p->s));
   g.stop();
   fill_stats(st, t, 0, g.seconds());
+}
+
+static void witness_columns_to_device(azk_witness_plan* w, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny, void* dout) {
+  std::lock_guard<std::mutex> lk(w->mu);
+  Timer t;
+  if (nx) AZK_CU(cudaMemcpyAsync(w->xin.p, x, 16 * nx, cudaMemcpyHostToDevice, w->s));
+  if (ny) AZK_CU(cudaMemcpyAsync(w->yin.p, y, 16 * ny, cudaMemcpyHostToDevice, w->s));
+  witness_run(w, w->xin.as<uint4>(), nx, w->yin.as<uint4>(), ny, static_cast<uint4*>(dout), nullptr, t);
+  sync_stream(w->s);
 }
 
 extern "C" {

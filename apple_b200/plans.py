@@ -545,6 +545,7 @@ def _sched(schedule):
         s.layer_treelet[int(lg)] = int(tl)
     for lg, th in dict(schedule.get("layer_threads", {})).items():
         s.layer_threads[int(lg)] = int(th)
+    s.persistent_trees = int(schedule.get("persistent_trees", 0))
     _keep.append(s)
     return ctypes.byref(s)
 

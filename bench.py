@@ -148,6 +148,15 @@ def tuned_tables():
         return None
 
 
+def tuned_thread_tables():
+    """The tuned per-layer thread counts the library was built with, if any."""
+    try:
+        with open(os.path.join(ROOT, "apple_b200", "tuned_b200.json")) as f:
+            return {k: {int(lg): int(t) for lg, t in v.items()} for k, v in json.load(f).get("thread_tables", {}).items()}
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -447,6 +456,165 @@ def run_serving(azk, ctx, args, batched_jobs_per_s, batched_elems_per_s=None):
     }
 
 
+def _hashlib_merkle_check(leaf, index, siblings, root) -> bool:
+    """A Merkle opening checked with Python's hashlib (independent of this library):
+    SHA3-256 of the leaf, then of (left || right) up the path."""
+    import hashlib
+
+    cur = hashlib.sha3_256(leaf).digest()
+    for level, sib in enumerate(siblings):
+        cur = hashlib.sha3_256(cur + sib if ((index >> level) & 1) == 0 else sib + cur).digest()
+    return cur == root
+
+
+def run_primitives(azk, ctx, device, reps=5, seed=0xA11CE002):
+    """The survey's C2/C3 primitives at full size with inputs resident in HBM
+    (seeded random bytes and M31 values drawn on the device): Keccak-f[1600] over
+    2^24 states, SHA3-256 over 2^24 messages of 32/64/128/136 bytes, the SHA3
+    Merkle commitment of 2^24 64-byte leaves with 1024 openings, one log-22 Circle
+    PCS proof (16 rounds, 64 queries), the QM31 and Circle folds of 2^24 values and
+    the 2^20 multilinear sum-check.  Device time (CUDA events) is the median of
+    `reps` launches after warm-up.  SHA3 digests and Merkle openings are checked
+    here with hashlib on 1024 sampled items; the other rows keep samples for the
+    CPU oracle, which checks them in the CPU leg."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    n = 1 << 24
+    rng = np.random.default_rng(seed)
+    peak = azk.probe_int_issue(ctx) / 4320.0
+    hbm, _ = measured_peaks()
+    rows, samples = {}, {}
+
+    def med(f):
+        f()
+        f()
+        return statistics.median(f() for _ in range(reps))
+
+    def rand_u8(count):
+        return torch.randint(0, 256, (count,), dtype=torch.uint8, device=dev, generator=gen)
+
+    # Keccak-f[1600]: 2^24 states of 200 bytes in, 200 out
+    st, out = rand_u8(200 * n), torch.empty(200 * n, dtype=torch.uint8, device=dev)
+    plan = azk.KeccakF1600PermutationPlan(ctx, n)
+    t = med(lambda: plan.permute_resident(st.data_ptr(), out.data_ptr()).gpu_s)
+    idx = np.sort(rng.choice(n, 1024, replace=False))
+    ti = torch.as_tensor(idx, device=dev)
+    samples["keccak"] = (st.view(n, 200)[ti].cpu().numpy(), out.view(n, 200)[ti].cpu().numpy())
+    rows["keccak_f1600_2e24"] = {"seconds": t, "perms_per_s": n / t, "frac_int_roofline": n / t / peak, "hbm_gbs": 400 * n / t / 1e9}
+    del st, out, plan
+    # SHA3-256 of 2^24 messages per length (136 bytes take two permutations)
+    import hashlib
+
+    sha_ok = True
+    for length in (32, 64, 128, 136):
+        msgs, dig = rand_u8(length * n), torch.empty(32 * n, dtype=torch.uint8, device=dev)
+        plan = azk.SHA3FixedOneBlockHashPlan(ctx, n, length, length)
+        t = med(lambda: plan.hash_resident(msgs.data_ptr(), dig.data_ptr()).gpu_s)
+        m_s, d_s = msgs.view(n, length)[ti].cpu().numpy(), dig.view(n, 32)[ti].cpu().numpy()
+        ok = all(hashlib.sha3_256(m_s[k].tobytes()).digest() == d_s[k].tobytes() for k in range(len(idx)))
+        sha_ok &= ok
+        perms = n * (2 if length == 136 else 1)
+        rows[f"sha3_256_2e24_{length}B"] = {"seconds": t, "hashes_per_s": n / t, "frac_int_roofline": perms / t / peak, "sample_equal_hashlib": ok}
+        del msgs, dig, plan
+    # Merkle over 2^24 x 64-byte leaves with 1024 openings
+    leaves = rand_u8(64 * n)
+    plan = azk.SHA3RawLeavesMerkleCommitPlan(ctx, n, 64, 64)
+    root = None
+
+    def commit():
+        nonlocal root
+        root = plan.commit_resident(leaves.data_ptr())
+        return plan.last_stats.gpu_s
+
+    t = med(commit)
+    oidx = rng.integers(0, n, size=1024)
+    paths = plan.open_resident(oidx)
+    t_open = plan.last_stats.gpu_s or plan.last_stats.cpu_wall_s
+    lv = leaves.view(n, 64)[torch.as_tensor(oidx, device=dev)].cpu().numpy()
+    open_ok = all(_hashlib_merkle_check(lv[k].tobytes(), int(oidx[k]), paths[k], root) for k in range(len(oidx)))
+    rows["merkle_2e24_64B"] = {"seconds": t, "perms_per_s": (2 * n - 1) / t, "frac_int_roofline": (2 * n - 1) / t / peak,
+                               "openings": 1024, "openings_s": t_open, "openings_verify_hashlib": open_ok}
+    del leaves, plan
+    # one log-22 PCS proof from coefficients (blowup 4, 16 rounds, 64 queries)
+    lg = 22
+    coeffs = np.zeros(((1 << lg) >> 2, 4), np.uint32)
+    coeffs[:, 0] = uniform_m31(seed ^ 0xC3, len(coeffs))
+    pub = public_digests(1, seed ^ 0xC3)
+    prover = azk.CirclePCSFRIProver(ctx, lg, 2, 64, 16)
+    proof = None
+
+    def prove():
+        nonlocal proof
+        proof = prover.prove_coefficients(coeffs, pub)
+        return prover.last_stats.gpu_s
+
+    t = med(prove)
+    perms = sum(2 * ((1 << lg) >> k) - 1 + 3 for k in range(16))
+    samples["c3"] = (coeffs, pub, proof)
+    rows["pcs_prove_log22"] = {"seconds": t, "elems_per_s": (1 << lg) / t, "frac_int_roofline": perms / t / peak, "proof_bytes": len(proof),
+                               "wall_s": prover.last_stats.cpu_wall_s}
+    del prover
+    # QM31 fold of 2^24 values with QM31 inverse points (16n + 8n read, 8n write)
+    ev = torch.randint(0, 2**31 - 1, (n * 4,), dtype=torch.int32, device=dev, generator=gen)
+    inv = torch.randint(1, 2**31 - 1, (n * 2,), dtype=torch.int32, device=dev, generator=gen)
+    fo = torch.empty(n * 2, dtype=torch.int32, device=dev)
+    ch = np.array([[11, 13, 17, 19]], np.uint32)
+    fplan = azk.QM31FRIFoldPlan(ctx, n)
+    t = med(lambda: fplan.execute_resident(ev.data_ptr(), inv.data_ptr(), fo.data_ptr(), ch).gpu_s)
+    fidx = torch.as_tensor(idx[:256] // 2, device=dev)
+    samples["fold"] = (ev.view(n // 2, 8)[fidx].cpu().numpy().view(np.uint32), inv.view(n // 2, 4)[fidx].cpu().numpy().view(np.uint32),
+                       fo.view(n // 2, 4)[fidx].cpu().numpy().view(np.uint32), ch)
+    rows["qm31_fold_2e24"] = {"seconds": t, "hbm_gbs": 32 * n / t / 1e9, "frac_hbm": 32 * n / t / 1e9 / hbm,
+                              "algorithmic": "16n + 8n read + 8n write bytes (n inputs)"}
+    del ev, inv, fo, fplan
+    # M31 multilinear sum-check of 2^20 evaluations (sequential digest + 20 rounds)
+    sc = uniform_m31(seed ^ 0x5C, 1 << 20)
+    res = None
+
+    def sumcheck():
+        nonlocal res
+        t0 = time.perf_counter()
+        res = azk.sumcheck_prove(ctx, sc)
+        return time.perf_counter() - t0
+
+    t = med(sumcheck)
+    samples["sumcheck"] = (sc, res)
+    rows["sumcheck_2e20"] = {"wall_s": t, "digest_permutations": (50 + 4 * len(sc)) // 136 + 1}
+    torch.cuda.empty_cache()  # give the device memory of the inputs back before serving
+    return {"rows": rows, "int_peak_perms_per_s": peak, "hbm_peak_gbs": hbm,
+            "checks_here": {"sha3_sample_equal_hashlib": sha_ok, "merkle_openings_verify_hashlib": open_ok}}, samples
+
+
+def check_primitive_samples(samples) -> dict:
+    """The CPU oracle on the primitives' samples (runs in the CPU leg)."""
+    from oracle import pyoracle as O
+
+    out = {}
+    if "keccak" in samples:
+        s_in, s_out = samples["keccak"]
+        out["keccak_sample_equal"] = bool(np.array_equal(O.keccak_f1600(s_in.reshape(-1)).reshape(s_out.shape), s_out))
+    if "fold" in samples:
+        ev, inv, got, ch = samples["fold"]
+        want = np.stack([O.fold(ev[k].reshape(2, 4), inv[k:k + 1], ch[0])[0] for k in range(len(ev))])
+        out["qm31_fold_sample_equal"] = bool(np.array_equal(want, got))
+    if "c3" in samples:
+        coeffs, pub, proof = samples["c3"]
+        full = np.zeros((1 << 22, 4), np.uint32)
+        full[: len(coeffs)] = coeffs
+        r = O.prove(22, O.fft_evaluate(22, full), 2, 64, pub, 16)
+        out["pcs_log22_proof_equal"] = r.proof == proof
+        out["pcs_log22_verified"] = O.verify(proof, pub)
+    if "sumcheck" in samples:
+        ev, res = samples["sumcheck"]
+        want = O.sumcheck_multilinear(ev)
+        out["sumcheck_equal"] = (res["claimed_sum"] == want["claimed_sum"] and res["final"] == want["final"]
+                                 and res["initial_digest"] == want["initial_digest"] and np.array_equal(res["challenges"], want["challenges"]))
+    return out
+
+
 def plain_values_ok(v):
     return v is not None and v > 0
 
@@ -487,6 +655,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=5)
     ap.add_argument("--plain-warmup", type=int, default=1)
     ap.add_argument("--cpu-max-log", type=int, default=64, help="largest log size in the CPU oracle's sample")
+    ap.add_argument("--tuner-ab", type=int, default=1, help="time the plain form and single trees at a fixed depth beside the tuned tables")
+    ap.add_argument("--primitives", type=int, default=1, help="measure the C2/C3 primitives at full size (outputs sample-checked)")
     ap.add_argument("--literal-max-log", type=int, default=14, help="largest log size the literal single-thread CPU form proves")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
@@ -617,6 +787,20 @@ def main():
 
     proof_total = batch.proof_total
 
+    # ---- the commit launches as persistent work-queue grids instead of one CTA per
+    # treelet (same schedule otherwise) ----
+    persistent = None
+    if args.compare_schedules:
+        bqp = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=dict(sched, persistent_trees=1))
+        bqp.upload(host_rows, offsets, counts)
+        bqp.prove(pubs)
+        ptq = [bqp.prove(pubs).gpu_s for _ in range(3)]
+        del bqp
+        t_pq = max_over_ranks(dist, statistics.median(ptq), local)
+        persistent = {"value": world * elems / t_pq, "unit": UNIT, "ms_per_step": 1000 * t_pq,
+                      "over_static_grid": (world * elems / t_pq) / value,
+                      "schedule": "each round's commit launch a grid of the resident CTAs pulling treelets from a device counter"}
+
     # ---- the same superstep with one fixed treelet depth everywhere (the schedule
     # without the tuner), and the plain per-instance form on its own best schedule
     # (the single-instance tuned table) ----
@@ -651,6 +835,32 @@ def main():
         del bp
     t_plain = max_over_ranks(dist, statistics.median(plain_times), local) if plain_times else float("nan")
 
+    # ---- where the tuned tables matter: the plain form at one fixed depth, and
+    # single fold-and-commit trees of 2^12 ... 2^16 leaves (the server's typical
+    # layers), tuned depth and threads against depth 12 at 256 threads ----
+    tuner_ab = None
+    if args.tuner_ab and not args.treelet_log:
+        from apple_b200 import autotune as T
+
+        tables = tuned_tables() or {}
+        bq = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=dict(treelet_log=12, group_log=args.group_log, threads=args.threads, use_graph=0))
+        bq.upload(host_rows, offsets, counts)
+        bq.prove(pubs, plain=True)
+        pt = [bq.prove(pubs, plain=True).gpu_s for _ in range(3)]
+        del bq
+        t_plain12 = max_over_ranks(dist, statistics.median(pt), local)
+        trees = {}
+        single = tables.get("pcs_single", {})
+        single_threads = (tuned_thread_tables() or {}).get("pcs_single", {})
+        for lg in range(12, 17):
+            tl, th = int(single.get(lg, 12)), int(single_threads.get(lg, 0) or 256)
+            t_tuned = T.time_tree(ctx, lg, 16, 1, 1, tl, th, reps=7)
+            t_fixed = T.time_tree(ctx, lg, 16, 1, 1, min(12, lg), 256, reps=7)
+            trees[lg] = {"tuned": [tl, th], "tuned_us": 1e6 * t_tuned, "depth12_us": 1e6 * t_fixed, "tuned_over_depth12": t_fixed / t_tuned}
+        tuner_ab = {"plain_depth12_ms": 1000 * t_plain12, "plain_tuned_over_depth12": t_plain12 / t_plain if plain_times else None,
+                    "single_trees": trees,
+                    "note": "device time of one fold-and-commit tree of 2^k 16-byte leaves (median of 7); plain form: whole superstep, median of 3"}
+
     # ---- the same superstep with 64-byte Merkle leaves (4 QM31 per leaf): the
     # survey's second C4 row; bit-exact against the oracle's 64-byte-leaf chain, no
     # verifier proof format ----
@@ -684,6 +894,11 @@ def main():
     fft_gbs_dense = work["fft_bytes"] / prof["fft_s"] / 1e9 if prof["fft_s"] > 0 else 0.0
     traffic = profile_traffic()
 
+    primitives, prim_samples = None, {}
+    if args.primitives and world == 1:
+        primitives, prim_samples = run_primitives(azk, ctx, local)
+        print(f"[bench] primitives {primitives}", file=sys.stderr, flush=True)
+
     serving = None
     if not args.no_serve and world == 1:
         serving = run_serving(azk, ctx, args, len(logs) * args.steps / t_dev, value / world)
@@ -709,6 +924,11 @@ def main():
                       "check": "proof bytes of the stratified sample equal the oracle's; every proof of the superstep is accepted by "
                                "the oracle's verifier; the plain form's proofs equal the batched form's"}
             parity_ok = parity["equal"] and parity["verified_all"] and not plain_mismatch
+            if primitives is not None:
+                primitives["checks_oracle"] = check_primitive_samples(prim_samples)
+                prim_ok = all(primitives["checks_oracle"].values()) and all(primitives["checks_here"].values())
+                parity["primitives_equal"] = prim_ok
+                parity_ok = parity_ok and prim_ok
             cpu = {"value": e / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port", "cpu_model": cpu_model(),
                    "sample": f"one instance of each log size {logs[sample[0]]}..{logs[sample[-1]]} of the workload (its size mix; "
                              f"sum 2^logN = {e}), FFT + prove with the C++ oracle on {O.num_threads()} threads ({dt:.1f} s)"}
@@ -736,6 +956,9 @@ def main():
             "leaf64": leaf64,
             "untuned": {"value": untuned_value, "unit": UNIT, "schedule": "treelet depth 12 on every layer",
                         "tuned_over_untuned": value / untuned_value if untuned_value else None},
+            "tuner_ab": tuner_ab,
+            "persistent_trees": persistent,
+            "primitives": primitives,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e2e_report,
                     "mode": "two provers taking turns on the GPU (one prover's copies overlap the other's superstep; the first upload and the last download are inside the timed region)" if e2e_pipe else "serial",
                     "serial_value": e2e_serial, "serial_ms_per_step": 1000 * t_e2e},

@@ -286,6 +286,9 @@ typedef struct azk_schedule {
    * for a committed layer of 2^L leaves; a launch that commits several layers takes
    * the entry of its largest one.  The autotuner fills this table too. */
   uint16_t layer_threads[32];
+  /* Nonzero: each round's commit launch is a persistent grid of the resident CTAs
+   * pulling treelets from a device work counter, instead of one CTA per treelet. */
+  uint32_t persistent_trees;
 } azk_schedule;
 
 azk_status azk_pcs_prover_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,

@@ -49,6 +49,18 @@ def test_codeword_polynomial_matches_direct(ctx, oracle, log_size):
     assert np.array_equal(plan.execute(x[:1]), oracle.evaluate_direct(log_size, x[:1], []))
 
 
+@pytest.mark.parametrize("log_size,nx,ny", [(12, 2048, 2048), (14, 8192, 8192), (14, 5000, 1), (16, 3, 700)])
+def test_codeword_polynomial_long_columns(ctx, oracle, log_size, nx, ny):
+    """execute(polynomial:) converts monomials to the FFT basis on the device (the
+    witness kernels); the codeword equals the oracle's conversion + FFT, for full
+    half-domain columns as well as ragged ones."""
+    rng = np.random.default_rng(log_size * 100 + nx)
+    x = rng.integers(0, G.P, size=(nx, 4), dtype=np.uint32)
+    y = rng.integers(0, G.P, size=(ny, 4), dtype=np.uint32)
+    want = oracle.fft_evaluate(log_size, oracle.fft_basis_coefficients(log_size, x, y))
+    assert np.array_equal(azk.CircleCodewordPlan(ctx, log_size).execute(x, y), want)
+
+
 @pytest.mark.parametrize("log_size", [10, 14])
 def test_codeword_golden_digest(ctx, oracle, golden, log_size):
     v = golden[f"bench_codeword_prover_log{log_size}"]

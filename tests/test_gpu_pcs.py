@@ -70,7 +70,10 @@ def test_prover_matches_oracle(ctx, oracle, log_size, rounds, queries):
     assert cm == r.commitments and np.array_equal(ch, r.challenges) and np.array_equal(fl, r.final_layer) and qp == r.query_pairs
 
 
-@pytest.mark.parametrize("schedule", [dict(treelet_log=1, group_log=1, threads=128), dict(treelet_log=5, group_log=3, threads=256),
+@pytest.mark.parametrize("schedule", [dict(treelet_log=3, group_log=2, threads=256, persistent_trees=1),
+                                      dict(treelet_log=11, group_log=5, threads=512, persistent_trees=1),
+                                      dict(layer_treelet={15: 9, 14: 9, 13: 7}, layer_threads={15: 512, 14: 128, 12: 512}),
+                                      dict(treelet_log=1, group_log=1, threads=128), dict(treelet_log=5, group_log=3, threads=256),
                                       dict(treelet_log=11, group_log=11, threads=512), dict(treelet_log=8, group_log=2, threads=256),
                                       dict(treelet_log=13, group_log=13, threads=256), dict(treelet_log=2, group_log=1, threads=512)])
 def test_prover_schedules_do_not_change_bytes(ctx, oracle, schedule):
@@ -140,6 +143,28 @@ def test_batch_matches_oracle_uneven(ctx, oracle, plain):
         ev = oracle.fft_evaluate(lg, coeffs)
         r = oracle.prove(lg, ev, 2, 16, pubs[32 * i:32 * i + 32], rounds[i])
         assert proofs[i] == r.proof, i
+
+
+def test_batch_persistent_trees_graph_replay(ctx, oracle):
+    """The persistent work-queue commit launches (counters reset by the last CTA out)
+    give the oracle's proofs, and again on graph replay and in the plain form."""
+    logs = [12, 9, 14, 10, 11, 13]
+    rounds = [lg - 6 for lg in logs]
+    flat, offs, cnts = _batch_inputs(logs, 21)
+    b = azk.BatchProver(ctx, logs, rounds, 2, 8, schedule=dict(group_log=12, threads=256, use_graph=1, persistent_trees=1))
+    b.upload(flat, offs, cnts)
+    pubs = bytes((3 * i) & 0xFF for i in range(32 * len(logs)))
+    b.prove(pubs)
+    first = b.proofs()
+    for i, lg in enumerate(logs):
+        c = np.zeros((1 << lg, 4), np.uint32)
+        c[: cnts[i]] = flat[offs[i]:offs[i] + cnts[i]]
+        assert first[i] == oracle.prove(lg, oracle.fft_evaluate(lg, c), 2, 8, pubs[32 * i:32 * i + 32], rounds[i]).proof
+    b.prove(pubs)
+    b.prove(pubs)
+    assert b.proofs() == first
+    b.prove(pubs, plain=True)
+    assert b.proofs() == first
 
 
 def test_batch_graph_replay_and_plain_agree(ctx):
