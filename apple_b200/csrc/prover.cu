@@ -1164,16 +1164,38 @@ bool evict_lru(azk_server* sv, int w, std::vector<Resident>& dropped) {
   return true;
 }
 
+// Device memory given back under the lock and freed after it (a free waits for the
+// whole device): evicted PCS engines and the buffers of free lane slots.
+struct Dropped {
+  std::vector<Resident> engines;
+  std::vector<SumcheckBufs> tables;
+  bool empty() const { return engines.empty() && tables.empty(); }
+  void clear() {
+    engines.clear();
+    tables.clear();
+  }
+};
+
 // Make room for `bytes` more: this worker's cached shapes first, then idle
-// workers' (a worker that runs no job has nothing in flight on its stream).
+// workers' (a worker that runs no job has nothing in flight on its stream), then
+// the buffers of free lane slots (reallocated when a table needs them again).
 // Called with the lock held; returns whether the bytes fit.
-bool make_room(azk_server* sv, int w, uint64_t bytes, std::vector<Resident>& dropped) {
-  while (sv->held + bytes > sv->budget && evict_lru(sv, w, dropped)) {
+bool make_room(azk_server* sv, int w, uint64_t bytes, Dropped& dropped) {
+  while (sv->held + bytes > sv->budget && evict_lru(sv, w, dropped.engines)) {
   }
   for (uint32_t v = 0; v < sv->slots && sv->held + bytes > sv->budget; v++) {
     if ((int)v == w || sv->busy[v]) continue;
-    while (sv->held + bytes > sv->budget && evict_lru(sv, (int)v, dropped)) {
+    while (sv->held + bytes > sv->budget && evict_lru(sv, (int)v, dropped.engines)) {
     }
+  }
+  for (size_t k = 0; k < sv->sc_free.size() && sv->held + bytes > sv->budget; k++) {
+    SumcheckSlot& sl = *sv->sc_slot[sv->sc_free[k]];
+    if (!sl.cap_log) continue;
+    sv->held -= sumcheck_table_bytes(sl.cap_log);
+    dropped.tables.push_back(std::move(sl.bufs));
+    sl.bufs = SumcheckBufs{};
+    sl.cap_log = 0;
+    sl.grow = false;
   }
   return sv->held + bytes <= sv->budget;
 }
@@ -1189,7 +1211,7 @@ struct Take {
 // Called with the server lock held.  Nothing is taken while the front job cannot
 // fit; a job larger than the budget never enters the queue.  Evicted memory is
 // handed back in `dropped` for the caller to free outside the lock.
-bool try_take(azk_server* sv, int w, Take& tk, std::vector<Resident>& dropped) {
+bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
   // this worker's warm-up jobs first; one that cannot fit the budget is dropped
   while (!sv->warm[w].empty()) {
     auto j = sv->warm[w].front();
@@ -1223,16 +1245,20 @@ bool try_take(azk_server* sv, int w, Take& tk, std::vector<Resident>& dropped) {
   if (j->kind == 1) {
     // a sum-check goes to a free lane slot; a slot smaller than the table grows
     if (sv->sc_free.empty()) return false;
+    // the slot leaves the free list first, so making room never takes its buffers
     const int slot = sv->sc_free.back();
+    sv->sc_free.pop_back();
     SumcheckSlot& sl = *sv->sc_slot[slot];
     if (sl.cap_log < j->logn) {
       const uint64_t extra = sumcheck_table_bytes(j->logn) - (sl.cap_log ? sumcheck_table_bytes(sl.cap_log) : 0);
-      if (!make_room(sv, w, extra, dropped)) return false;
+      if (!make_room(sv, w, extra, dropped)) {
+        sv->sc_free.push_back(slot);
+        return false;
+      }
       sv->held += extra;
       sl.cap_log = j->logn;  // the worker reallocates before filling the slot
       sl.grow = true;
     }
-    sv->sc_free.pop_back();
     sl.job = j;
     sv->queue.pop_front();
     sv->running++;
@@ -1478,7 +1504,7 @@ void worker_loop(azk_server* sv, int w) {
   for (;;) {
     Take tk;
     Resident* res = nullptr;
-    std::vector<Resident> dropped;  // evicted shapes, freed below without the lock
+    Dropped dropped;  // evicted memory, freed below without the lock
     {
       std::unique_lock<std::mutex> lk(sv->mu);
       bool got = false;
@@ -1662,8 +1688,11 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
     layout(sv && (n_pcs == 0 || (pcs_logn && pcs_rounds)) && (n_sumcheck == 0 || sumcheck_logn));
     for (uint32_t i = 0; i < n_pcs; i++) validate_params(pcs_logn[i], log_blowup, queries, 0, pcs_rounds[i]);
     uint32_t sc_log = 0;
+    std::vector<uint32_t> sc_logs;  // listed tables that fit the budget
     for (uint32_t i = 0; i < n_sumcheck; i++) {
       layout(sumcheck_logn[i] >= 1 && sumcheck_logn[i] <= 28);
+      if (sumcheck_table_bytes(sumcheck_logn[i]) > sv->budget) continue;
+      sc_logs.push_back(sumcheck_logn[i]);
       sc_log = std::max(sc_log, sumcheck_logn[i]);
     }
     // the lane's table slots for the largest listed table, as many as fit the budget
@@ -1717,10 +1746,10 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
       }
     }
     // one table of zeros per listed size through the lane (kernels loaded before serving)
-    for (uint32_t i = 0; i < n_sumcheck; i++) {
+    for (uint32_t lg : sc_logs) {
       auto j = std::make_shared<ServeJob>();
       j->kind = 1;
-      j->logn = sumcheck_logn[i];
+      j->logn = lg;
       j->zeros = true;
       sv->queue.push_front(j);
       sv->warm_pending++;
