@@ -254,7 +254,11 @@ struct ScanJob {
 };
 cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_n, uint32_t* d_bad, cudaStream_t s);
 cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
-cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s);
+// QM31 fold with QM31 inverse points.  With a status word the inputs are staged by
+// bulk copies (persistent grid; a bounded wait that runs out raises *d_status).
+cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s,
+                                 uint32_t* d_status = nullptr);
+cudaError_t prepare_fold_kernels();
 cudaError_t launch_pcs_prefix(PcsInstance* d_inst, uint32_t ninst, cudaStream_t s);
 cudaError_t launch_pcs_finalize(PcsInstance* d_inst, const uint32_t* d_ids, uint32_t nids, cudaStream_t s);
 cudaError_t launch_pcs_grind(PcsInstance* d_inst, uint32_t id, uint64_t start, uint64_t count, unsigned long long* d_found, cudaStream_t s);

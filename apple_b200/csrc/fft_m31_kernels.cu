@@ -27,9 +27,11 @@
 //    copy (cp.async.bulk, completion counted on an mbarrier) that is issued for the
 //    next tile as soon as the current tile's first sub-pass has read its copy, so
 //    the load runs under the remaining sub-passes.  Every wait on the mbarrier is
-//    bounded: a wait that runs out raises `status` and the CTA returns.
+//    bounded: a wait that runs out raises `status`, and the CTA returns after one
+//    more bounded wait for the copy it was waiting on.
 //  - fft_q_tile_kernel: the same tiles over QM31 values (inputs that are not lifted
 //    M31 polynomials), in place in the codeword buffer between passes.
+#include "azk_bulk.cuh"
 #include "azk_field.cuh"
 #include "azk_internal.h"
 
@@ -312,39 +314,6 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   }
 }
 
-// ---- bulk copy + mbarrier (PTX ISA: cp.async.bulk, mbarrier) ----
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: gives up after about 2^31 SM cycles (about a second).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > (1ll << 31)) return false;
-  return true;
-}
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)), "l"(src),
-               "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-
 // Queue the bulk copy of work item `item`'s input tile (4096 contiguous words of the
 // exchange buffer: the low pass has c = 0 and s_lo = 0, so tile w is words
 // [4096 w, 4096 w + 4096); 16 KB, 16-byte aligned) into X.
@@ -382,7 +351,12 @@ __global__ void __launch_bounds__(kThreads, 5) fft_m31_low_tma_kernel(const FftJ
     for (int b = 0; b < 16; b++) Y[swz(t | ((uint32_t)b << 8))] = v[b];
     // X has been read by every thread: the next tile's copy may land in it
     if (__syncthreads_or(!ok)) {
-      if (t == 0) atomicOr(status, 1u);
+      // the copy that did not complete may still land: wait for it once more
+      // (bounded) before the CTA gives up its shared memory
+      if (t == 0) {
+        atomicOr(status, 1u);
+        mbar_wait(&bar, phase ^ 1u);
+      }
       return;
     }
     const uint32_t next = item + gridDim.x;
