@@ -1001,7 +1001,7 @@ struct SumcheckStream {
   std::vector<int> slots;
 };
 constexpr int kLaneSlots = 96;    // tables in the lane at once
-constexpr int kLaneStreams = 6;   // batches in flight at once
+constexpr int kLaneStreams = 32;  // batches in flight at once
 constexpr int kLaneBatch = 32;    // tables per launch
 
 }  // namespace
@@ -1241,7 +1241,14 @@ bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
     return true;
   }
   if (sv->queue.empty()) return false;
-  std::shared_ptr<ServeJob> j = sv->queue.front();
+  // the front job; when it is a sum-check and every lane slot holds a table, the
+  // first queued proof job instead (a full lane never holds proof jobs back)
+  auto pick = sv->queue.begin();
+  if ((*pick)->kind == 1 && sv->sc_free.empty()) {
+    while (pick != sv->queue.end() && (*pick)->kind == 1) ++pick;
+    if (pick == sv->queue.end()) return false;
+  }
+  std::shared_ptr<ServeJob> j = *pick;
   if (j->kind == 1) {
     // a sum-check goes to a free lane slot; a slot smaller than the table grows
     if (sv->sc_free.empty()) return false;
@@ -1260,7 +1267,7 @@ bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
       sl.grow = true;
     }
     sl.job = j;
-    sv->queue.pop_front();
+    sv->queue.erase(pick);
     sv->running++;
     sv->busy[w] = 1;
     j->state = 1;
@@ -1638,15 +1645,17 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     // CUDA_DEVICE_MAX_CONNECTIONS (32) workers each lands on its own hardware work
     // queue.  Streams that share a queue wait on each other's dependent launches;
     // nothing here issues a launch that waits long on an earlier one in its stream
-    // (the sum-check lane proves a table in one launch).  Highest priority: a job's
-    // input scan takes the first free SM slot.
+    // (the sum-check lane proves a table in one launch).  Priorities: the lane's
+    // tables (one CTA each, the longest jobs) take the first free SM slot, then the
+    // workers' launches (a job's input scan ahead of default-priority work).
     int prio_lo = 0, prio_hi = 0;
     AZK_CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    const int prio_worker = prio_hi < prio_lo ? prio_hi + 1 : prio_hi;
     sv->streams.assign(slots, nullptr);
-    for (uint32_t w = 0; w < slots; w++) AZK_CU(cudaStreamCreateWithPriority(&sv->streams[w], cudaStreamNonBlocking, prio_hi));
+    for (uint32_t w = 0; w < slots; w++) AZK_CU(cudaStreamCreateWithPriority(&sv->streams[w], cudaStreamNonBlocking, prio_worker));
     sv->sc_stream.resize(kLaneStreams);
     for (int k = 0; k < kLaneStreams; k++) {
-      AZK_CU(cudaStreamCreateWithFlags(&sv->sc_stream[k].s, cudaStreamNonBlocking));
+      AZK_CU(cudaStreamCreateWithPriority(&sv->sc_stream[k].s, cudaStreamNonBlocking, prio_hi));
       AZK_CU(cudaEventCreateWithFlags(&sv->sc_stream[k].done, cudaEventBlockingSync | cudaEventDisableTiming));
       sv->sc_stream[k].jobs.alloc(sizeof(SumcheckJob) * kLaneBatch, "Sumcheck.LaneJobs");
       sv->sc_idle.push_back(k);

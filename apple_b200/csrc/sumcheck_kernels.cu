@@ -204,56 +204,74 @@ __device__ uint64_t digest_words_warp(const uint32_t* words, uint64_t count) {
   return a;
 }
 
-// One table on one CTA: warp 0 computes the statement's word digest (the other
-// warps wait at the barrier, issuing nothing), then the whole block proves the
-// rounds: each round is a block reduction (sums of the even and odd entries), a
-// transcript round by thread 0 (round frame, challenge frame, squeeze one word mod
-// p) and a fold t'[i] = (1 - r) t[2i] + r t[2i+1].  One launch per table (or per
-// batch of tables, one CTA each) leaves no launch in the stream waiting behind the
-// digest, so a stream that shares a hardware work queue with others never holds
-// that queue for the digest's duration.
+// Even and odd sums of the 4-word groups [4j, 4j + 4) for j = t0, t0 + step, ...
+// < quarter: eight 16-byte loads in flight per thread.
+__device__ __forceinline__ void pair_sums(const uint4* __restrict__ q, uint64_t quarter, uint64_t t0, uint64_t step, uint32_t& z, uint32_t& o) {
+  for (uint64_t j = t0; j < quarter; j += 8 * step) {
+    uint4 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint64_t jj = j + k * step;
+      v[k] = jj < quarter ? __ldg(q + jj) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      z = m31_add(z, m31_add(v[k].x, v[k].z));
+      o = m31_add(o, m31_add(v[k].y, v[k].w));
+    }
+  }
+}
+
+// One table on one CTA.  Warp 0 computes the statement's word digest while the
+// other warps sum the table's even and odd entries (round 0's two sums; together
+// the claimed sum), which need no challenge.  Then each round is a transcript
+// round by thread 0 (round frame, challenge frame, squeeze one word mod p) and
+// one pass over the table that folds it, t'[i] = (1 - r) t[2i] + r t[2i+1], and
+// sums the folded table's even and odd entries for the next round, so after the
+// digest the table is read once per round.  One launch per table (or per batch of
+// tables, one CTA each) leaves no launch in the stream waiting behind the digest,
+// so a stream that shares a hardware work queue with others never holds that
+// queue for the digest's duration.
 __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch, SumcheckOut* __restrict__ out) {
   __shared__ uint32_t red[32];
   __shared__ uint32_t s_ch;
   __shared__ uint64_t s_digest[4];
   const uint64_t n = 1ull << log_n;
-  if (threadIdx.x < 32) {
+  const uint32_t t = threadIdx.x;
+  uint32_t z = 0, o = 0;
+  if (t < 32) {
     const uint64_t d = digest_words_warp(evals, n);
-    if (threadIdx.x < 4) {
-      s_digest[threadIdx.x] = d;
-      out->digest[threadIdx.x] = d;
+    if (t < 4) {
+      s_digest[t] = d;
+      out->digest[t] = d;
     }
+  } else if (n >= 4) {
+    pair_sums(reinterpret_cast<const uint4*>(evals), n >> 2, t - 32, blockDim.x - 32, z, o);
+  } else if (n == 2 && t == 32) {
+    z = evals[0];
+    o = evals[1];
   }
-  __syncthreads();
-  // claimed sum
-  uint32_t acc = 0;
-  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) acc = m31_add(acc, evals[i]);
-  uint32_t total = block_sum_m31(acc, red);
-  if (threadIdx.x == 0) out->claimed_sum = total;
-  Transcript t;
-  if (threadIdx.x == 0) {
-    tr_reset(t);
+  uint32_t zs = block_sum_m31(z, red);
+  uint32_t os = block_sum_m31(o, red);
+  // block_sum_m31's value is valid in thread 0, which alone runs the transcript
+  const uint32_t total = n == 1 ? evals[0] : m31_add(zs, os);
+  Transcript tr;
+  if (t == 0) {
+    out->claimed_sum = total;
+    tr_reset(tr);
     FrameBuf f;
     sc_frame(f, 0);
     fb_u64(f, n);
     fb_u32(f, log_n);
     fb_u32(f, total);
     for (int i = 0; i < 4; i++) fb_u64(f, s_digest[i]);
-    tr_absorb(t, f.b, f.n);
+    tr_absorb(tr, f.b, f.n);
   }
   const uint32_t* cur = evals;
   uint32_t* bufs[2] = {scratch, scratch + (n >> 1)};
   for (uint32_t r = 0; r < log_n; r++) {
     const uint64_t half = (n >> r) >> 1;
-    uint32_t z = 0, o = 0;
-    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
-      const uint2 pr = *reinterpret_cast<const uint2*>(cur + 2 * i);
-      z = m31_add(z, pr.x);
-      o = m31_add(o, pr.y);
-    }
-    uint32_t zs = block_sum_m31(z, red);
-    uint32_t os = block_sum_m31(o, red);
-    if (threadIdx.x == 0) {
+    if (t == 0) {
       out->r0[r] = zs;
       out->r1[r] = os;
       FrameBuf f;
@@ -261,13 +279,13 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
       fb_u32(f, r);
       fb_u32(f, zs);
       fb_u32(f, os);
-      tr_absorb(t, f.b, f.n);
+      tr_absorb(tr, f.b, f.n);
       sc_frame(f, 2);
       fb_u32(f, r);
       fb_u32(f, kP);
-      tr_absorb(t, f.b, f.n);
+      tr_absorb(tr, f.b, f.n);
       uint32_t c;
-      tr_squeeze_u32(t, 1, kP, &c);
+      tr_squeeze_u32(tr, 1, kP, &c);
       out->challenges[r] = c;
       s_ch = c;
     }
@@ -275,14 +293,40 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
     const uint32_t c = s_ch;
     const uint32_t omc = m31_sub(1, c);
     uint32_t* nxt = bufs[r & 1];
-    for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
-      const uint2 pr = *reinterpret_cast<const uint2*>(cur + 2 * i);
-      nxt[i] = m31_add(m31_mul(omc, pr.x), m31_mul(c, pr.y));
+    z = 0;
+    o = 0;
+    if (half >= 2) {
+      // groups of 4 entries fold into 2: 16-byte loads, 8-byte stores, 8 in flight
+      const uint4* q = reinterpret_cast<const uint4*>(cur);
+      uint2* w = reinterpret_cast<uint2*>(nxt);
+      const uint64_t quarter = half >> 1;
+      for (uint64_t j = t; j < quarter; j += 8 * (uint64_t)blockDim.x) {
+        uint4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint64_t jj = j + (uint64_t)k * blockDim.x;
+          v[k] = jj < quarter ? q[jj] : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint64_t jj = j + (uint64_t)k * blockDim.x;
+          const uint32_t e = m31_add(m31_mul(omc, v[k].x), m31_mul(c, v[k].y));
+          const uint32_t d = m31_add(m31_mul(omc, v[k].z), m31_mul(c, v[k].w));
+          if (jj < quarter) {
+            w[jj] = make_uint2(e, d);
+            z = m31_add(z, e);
+            o = m31_add(o, d);
+          }
+        }
+      }
+    } else if (t == 0) {
+      nxt[0] = m31_add(m31_mul(omc, cur[0]), m31_mul(c, cur[1]));
     }
-    __syncthreads();
+    zs = block_sum_m31(z, red);  // synchronises: nxt is complete
+    os = block_sum_m31(o, red);
     cur = nxt;
   }
-  if (threadIdx.x == 0) out->final_eval = cur[0];
+  if (t == 0) out->final_eval = cur[0];
 }
 
 constexpr int kSumcheckThreads = 256;
