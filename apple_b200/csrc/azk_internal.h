@@ -254,11 +254,7 @@ struct ScanJob {
 };
 cudaError_t launch_scan_inputs(const ScanJob* d_jobs, uint32_t njobs, uint64_t max_n, uint32_t* d_bad, cudaStream_t s);
 cudaError_t launch_fold_jobs(const FoldJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
-// QM31 fold with QM31 inverse points.  With a status word the inputs are staged by
-// bulk copies (persistent grid; a bounded wait that runs out raises *d_status).
-cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s,
-                                 uint32_t* d_status = nullptr);
-cudaError_t prepare_fold_kernels();
+cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s);
 cudaError_t launch_pcs_prefix(PcsInstance* d_inst, uint32_t ninst, cudaStream_t s);
 cudaError_t launch_pcs_finalize(PcsInstance* d_inst, const uint32_t* d_ids, uint32_t nids, cudaStream_t s);
 cudaError_t launch_pcs_grind(PcsInstance* d_inst, uint32_t id, uint64_t start, uint64_t count, unsigned long long* d_found, cudaStream_t s);
@@ -270,6 +266,31 @@ cudaError_t launch_qm31_transcript_prefix(Transcript* d_t, uint64_t input_count,
 cudaError_t launch_transcript_rounds_given(Transcript* d_t, uint32_t kind, const uint64_t* d_roots, uint32_t rounds, uint64_t input_count,
                                            uint32_t* d_ch, cudaStream_t s);
 cudaError_t launch_check_canonical(const uint32_t* d_words, uint64_t nwords, uint32_t* d_flag, cudaStream_t s);
-cudaError_t launch_sumcheck_round(const uint32_t* in, uint64_t n, uint32_t* partials, uint32_t nblocks, cudaStream_t s);
+
+// M31 multilinear sum-check of one table per CTA (sumcheck_kernels.cu).  The kernel
+// writes *out and the three per-round arrays it points to (log_n words each); all
+// may be device memory or page-locked host memory.
+struct SumcheckOut {
+  uint32_t claimed_sum;
+  uint32_t final_eval;
+  uint64_t digest[4];
+  uint32_t* r0;          // sums of the even entries, per round
+  uint32_t* r1;          // sums of the odd entries, per round
+  uint32_t* challenges;  // per round
+};
+struct SumcheckJob {
+  const uint32_t* evals;
+  uint32_t* scratch;  // 2^log_n words
+  SumcheckOut* out;
+  uint32_t log_n;
+  uint32_t pad;
+};
+// Tables of one batched launch, passed by value (one CTA each).
+constexpr uint32_t kSumcheckBatchMax = 32;
+struct SumcheckBatch {
+  SumcheckJob job[kSumcheckBatchMax];
+};
+cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s);
+cudaError_t launch_sumcheck_batch(const SumcheckBatch& batch, uint32_t count, cudaStream_t s);
 
 }  // namespace azk

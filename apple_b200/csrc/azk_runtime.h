@@ -268,21 +268,6 @@ struct FftPlan {
   void check_status(cudaStream_t s);
 };
 
-// A device word that kernels with bounded waits raise when a wait runs out.
-struct StatusWord {
-  DevBuf d;
-  uint32_t* get(cudaStream_t s) {
-    if (!d.p) {
-      d.alloc(16, "status word");
-      AZK_CU(cudaMemsetAsync(d.p, 0, 16, s));
-    }
-    return d.as<uint32_t>();
-  }
-  // After the stream's kernels: fails with AZK_ERR_DEVICE_TIMEOUT (and clears the
-  // word) when one of them raised it.
-  void check(cudaStream_t s, const char* what);
-};
-
 // Monomial -> interleaved circle FFT-basis coefficients, host-side like the
 // reference's CircleCodewordPlan (CircleCodeword.swift:100-127, 187-263).
 std::vector<uint32_t> fft_basis_from_monomials(uint32_t logn, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny);

@@ -5,7 +5,6 @@
 // CircleCodeword.swift:129-171 (Metal: HashMerkleKernels.metal:1720-1879); FFT
 // CircleCodeword.swift:72-98 (Metal :1881-1943); fold QM31FRIFold.swift:11-44
 // (Metal :1987-2032); transcript and proof layout CircleProofFormat.swift:475-983.
-#include "azk_bulk.cuh"
 #include "azk_field.cuh"
 #include "azk_internal.h"
 
@@ -439,7 +438,6 @@ cudaError_t prepare_fft_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(fft_pass_m31_kernel<kFftThreadsM31>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemM31);
   if (e != cudaSuccess) return e;
-  if ((e = prepare_fold_kernels()) != cudaSuccess) return e;
   return prepare_fft_m31_kernels();
 }
 
@@ -526,109 +524,8 @@ __global__ void __launch_bounds__(256) fold_qm31_inv_kernel(const uint4* __restr
   }
 }
 
-// The same fold with its inputs staged by bulk copies.  A chunk is 512 outputs:
-// their 1,024 input values (16 KB, contiguous) and 512 inverse points (8 KB,
-// contiguous), each one cp.async.bulk into shared memory, completion counted on
-// the stage's mbarrier.  Two stages per CTA and a persistent grid (resident CTAs
-// only): while a CTA folds chunk c from one stage, chunk c + grid is landing in
-// the other, and the copy of chunk c + 2 grid is issued as soon as every thread
-// has read chunk c.  Outputs are written straight from registers (consecutive
-// threads, consecutive 16-byte vectors).  Every wait is bounded: one that runs out
-// raises `status`, waits once more (bounded) for the copies still in flight and
-// returns.
-constexpr uint32_t kFoldStage = 512;                           // outputs per staged chunk
-constexpr uint32_t kFoldStageVec = 3 * kFoldStage;             // 16-byte vectors per stage
-constexpr size_t kFoldBulkSmem = 2 * kFoldStageVec * 16 + 16;  // two stages + two mbarriers
-
-__device__ __forceinline__ void fold_fetch(const uint4* __restrict__ prev, const uint4* __restrict__ inv, uint64_t n_out, uint64_t c, uint4* stage,
-                                           uint64_t* bar) {
-  const uint64_t o0 = c * kFoldStage;
-  const uint32_t cnt = (uint32_t)(n_out - o0 < kFoldStage ? n_out - o0 : kFoldStage);
-  mbar_expect_tx(bar, cnt * 48u);
-  bulk_copy_g2s(stage, prev + 2 * o0, cnt * 32u, bar);
-  bulk_copy_g2s(stage + 2 * kFoldStage, inv + o0, cnt * 16u, bar);
-}
-
-__global__ void __launch_bounds__(256, 4) fold_qm31_inv_bulk_kernel(const uint4* __restrict__ prev, const uint4* __restrict__ inv,
-                                                                    const uint32_t* __restrict__ chp, uint4* __restrict__ out, uint64_t n_out,
-                                                                    uint32_t* __restrict__ status) {
-  extern __shared__ __align__(128) uint4 S[];  // [stage][1024 inputs | 512 inverse points], then the mbarriers
-  uint64_t* bar = reinterpret_cast<uint64_t*>(S + 2 * kFoldStageVec);
-  __shared__ uint32_t s_ch[4];
-  const uint32_t t = threadIdx.x;
-  const uint64_t nchunks = (n_out + kFoldStage - 1) / kFoldStage;
-  uint64_t c = blockIdx.x;
-  if (c >= nchunks) return;
-  if (t == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fold_fetch(prev, inv, n_out, c, S, &bar[0]);
-    if (c + gridDim.x < nchunks) fold_fetch(prev, inv, n_out, c + gridDim.x, S + kFoldStageVec, &bar[1]);
-  }
-  if (t < 4) s_ch[t] = __ldcg(chp + t);
-  __syncthreads();
-  const qm31 ch = {s_ch[0], s_ch[1], s_ch[2], s_ch[3]};
-  for (uint32_t it = 0; c < nchunks; it++, c += gridDim.x) {
-    const uint32_t st = it & 1u, par = (it >> 1) & 1u;
-    const bool ok = mbar_wait(&bar[st], par);
-    if (__syncthreads_or(!ok)) {
-      if (t == 0) {
-        atomicOr(status, 1u);
-        mbar_wait(&bar[st], par);
-        if (c + gridDim.x < nchunks) mbar_wait(&bar[st ^ 1u], ((it + 1) >> 1) & 1u);
-      }
-      return;
-    }
-    const uint4* P = S + st * kFoldStageVec;
-    const uint4* I = P + 2 * kFoldStage;
-    const uint64_t o0 = c * kFoldStage;
-    const uint32_t cnt = (uint32_t)(n_out - o0 < kFoldStage ? n_out - o0 : kFoldStage);
-#pragma unroll
-    for (uint32_t k = 0; k < kFoldStage / 256; k++) {
-      const uint32_t o = t + 256 * k;
-      if (o < cnt) {
-        const uint4 p = P[2 * o], q = P[2 * o + 1], w = I[o];
-        qm31 pos = {p.x, p.y, p.z, p.w}, neg = {q.x, q.y, q.z, q.w};
-        qm31 odd = q_mul(q_sub(pos, neg), qm31{w.x, w.y, w.z, w.w});
-        qm31 r = q_half(q_add(q_add(pos, neg), q_mul(ch, odd)));
-        out[o0 + o] = make_uint4(r.a, r.b, r.c, r.d);
-      }
-    }
-    __syncthreads();  // every thread has read stage st
-    const uint64_t nx = c + 2 * (uint64_t)gridDim.x;
-    if (t == 0 && nx < nchunks) {
-      fence_proxy_async_smem();
-      fold_fetch(prev, inv, n_out, nx, S + st * kFoldStageVec, &bar[st]);
-    }
-  }
-}
-
-int g_fold_grid[64] = {0};  // resident CTAs of the bulk-staged fold, per device
-
-cudaError_t prepare_fold_kernels() {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e = cudaFuncSetAttribute(fold_qm31_inv_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFoldBulkSmem);
-  if (e != cudaSuccess) return e;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fold_qm31_inv_bulk_kernel, 256, kFoldBulkSmem)) != cudaSuccess) return e;
-  if (dev >= 0 && dev < 64) g_fold_grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
-  return cudaSuccess;
-}
-
-// Bulk-staged when a status word is given and both input bases are 16-byte
-// aligned, otherwise the plain-load kernel.
-cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s,
-                                 uint32_t* d_status) {
+cudaError_t launch_fold_qm31_inv(const uint4* prev, const uint4* inv, const uint32_t* ch, uint4* out, uint64_t n_out, cudaStream_t s) {
   if (n_out == 0) return cudaSuccess;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const int grid = (dev >= 0 && dev < 64) ? g_fold_grid[dev] : 0;
-  if (d_status && grid > 0 && ((reinterpret_cast<uintptr_t>(prev) | reinterpret_cast<uintptr_t>(inv)) & 15) == 0) {
-    const uint64_t chunks = (n_out + kFoldStage - 1) / kFoldStage;
-    fold_qm31_inv_bulk_kernel<<<(unsigned)std::min<uint64_t>(chunks, (uint64_t)grid), 256, kFoldBulkSmem, s>>>(prev, inv, ch, out, n_out, d_status);
-    return cudaGetLastError();
-  }
   uint64_t blocks = (n_out + 511) / 512;
   if (blocks > 148 * 16) blocks = 148 * 16;
   fold_qm31_inv_kernel<<<(unsigned)blocks, 256, 0, s>>>(prev, inv, ch, out, n_out);

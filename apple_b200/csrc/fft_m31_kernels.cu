@@ -103,6 +103,19 @@ __device__ __forceinline__ Pass make_pass(const FftJob& job, uint64_t tile) {
   return p;
 }
 
+// The low-stage pass of a transform above 2^12 (s_lo = 0, m = 12, c = 0): the same
+// geometry as make_pass, with the constants visible to the compiler.
+__device__ __forceinline__ Pass low_pass(const FftJob& job, uint64_t tile) {
+  Pass p;
+  p.logn = job.logn;
+  p.s_lo = 0;
+  p.m = kFftLowBits;
+  p.c = 0;
+  p.hi = tile;
+  p.gbase = tile << kFftLowBits;
+  return p;
+}
+
 // The stage of sub-pass Q on owned bit K (L bit 4Q + K) over the thread's 16
 // values v[b] (bit k of b = L bit 4Q + k; Lbase = the thread's L with those bits
 // zero): 8 butterflies with the 2^(3-K) twiddles of the stage's blocks above it.
@@ -113,13 +126,37 @@ __device__ __forceinline__ void bfly(qm31& l, qm31& r, uint32_t t) {
   l = a;
 }
 
-template <int Q, int K, class V>
-__device__ __forceinline__ void stage(V (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw) {
-  const uint32_t j = 4 * Q + K - p.c;  // row bit = stage s_lo + j
+// Twiddles of one sub-pass, loaded ahead of the butterflies that use them (before
+// the barrier or bulk-copy wait that precedes the sub-pass, so their latency hides
+// behind it): t[K] holds the 2^(3-K) twiddles of the stage on owned bit K.
+struct TwSet {
+  uint32_t t[4][8];
+};
+
+// Stage j = 4Q + K - c of the pass (global stage s_lo + j): its twiddles for the
+// thread's values start at tw[off(s) + (hi << (m-1-j)) + ((Lbase >> c) >> (j+1))].
+template <int Q, int K>
+__device__ __forceinline__ void tw_stage(uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw, uint32_t (&t)[8]) {
+  const uint32_t j = 4 * Q + K - p.c;
   const uint32_t s = p.s_lo + j;
   const uint64_t base = twoff(p.logn, s) + (p.hi << (p.m - 1 - j)) + ((uint64_t)(Lbase >> p.c) >> (j + 1));
-  uint32_t t[8];
   load_tw<3 - K>(tw + base, t);
+}
+
+// The stages of sub-pass Q run from owned bit `kstart` down; owned bits below the
+// pass's column count are columns (no butterflies, no twiddles).
+template <int Q>
+__device__ __forceinline__ void tw_load(TwSet& w, uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw, int kstart) {
+  if (kstart >= 3 && 4 * Q + 3 >= p.c) tw_stage<Q, 3>(Lbase, p, tw, w.t[3]);
+  if (kstart >= 2 && 4 * Q + 2 >= p.c) tw_stage<Q, 2>(Lbase, p, tw, w.t[2]);
+  if (kstart >= 1 && 4 * Q + 1 >= p.c) tw_stage<Q, 1>(Lbase, p, tw, w.t[1]);
+  if (4 * Q >= p.c) tw_stage<Q, 0>(Lbase, p, tw, w.t[0]);
+}
+
+// The stage on owned bit K over the thread's 16 values v[b] (bit k of b = L bit
+// 4Q + k): 8 butterflies with the 2^(3-K) twiddles of the stage's blocks above it.
+template <int K, class V>
+__device__ __forceinline__ void stage(V (&v)[16], const uint32_t (&t)[8]) {
 #pragma unroll
   for (int b = 0; b < 16; b++) {
     if (b & (1 << K)) continue;
@@ -127,27 +164,28 @@ __device__ __forceinline__ void stage(V (&v)[16], uint32_t Lbase, const Pass& p,
   }
 }
 
-// Stages of sub-pass Q from owned bit `kstart` down; owned bits below the pass's
-// column count are columns (no butterflies).
 template <int Q, class V>
-__device__ __forceinline__ void subpass(V (&v)[16], uint32_t Lbase, const Pass& p, const uint32_t* __restrict__ tw, int kstart) {
-  if (kstart >= 3 && 4 * Q + 3 >= p.c) stage<Q, 3>(v, Lbase, p, tw);
-  if (kstart >= 2 && 4 * Q + 2 >= p.c) stage<Q, 2>(v, Lbase, p, tw);
-  if (kstart >= 1 && 4 * Q + 1 >= p.c) stage<Q, 1>(v, Lbase, p, tw);
-  if (4 * Q >= p.c) stage<Q, 0>(v, Lbase, p, tw);
+__device__ __forceinline__ void subpass(V (&v)[16], const TwSet& w, const Pass& p, int kstart) {
+  if (kstart >= 3 && 4 * Q + 3 >= p.c) stage<3>(v, w.t[3]);
+  if (kstart >= 2 && 4 * Q + 2 >= p.c) stage<2>(v, w.t[2]);
+  if (kstart >= 1 && 4 * Q + 1 >= p.c) stage<1>(v, w.t[1]);
+  if (4 * Q >= p.c) stage<0>(v, w.t[0]);
 }
 
-// Sub-passes 1 and 0 after sub-pass 2 has left its values in `Y` (synchronised),
-// then the pass's output: the exchange buffer (high-stage passes, from the last
-// sub-pass that has stages) or the QM31 codeword (the transform's last pass, from
-// `Y` in coalesced rows).  `last` passes have c = 0.
-__device__ __forceinline__ void finish_tile(uint32_t* Y, const FftJob& job, const Pass& p, bool last) {
+// Sub-passes 1 and 0 after sub-pass 2 has left its values in `Y` (synchronised;
+// `w1` holds sub-pass 1's twiddles, loaded before that barrier), then the pass's
+// output: the exchange buffer (high-stage passes, from the last sub-pass that has
+// stages) or the QM31 codeword (the transform's last pass, from `Y` in coalesced
+// rows).  `last` passes have c = 0.
+__device__ __forceinline__ uint32_t sub1_base(uint32_t t) { return (t & 15u) | ((t >> 4) << 8); }
+
+__device__ __forceinline__ void finish_tile(uint32_t* Y, const FftJob& job, const Pass& p, bool last, const TwSet& w1) {
   const uint32_t t = threadIdx.x;
   uint32_t v[16];
-  const uint32_t LB = (t & 15u) | ((t >> 4) << 8);
+  const uint32_t LB = sub1_base(t);
 #pragma unroll
   for (int b = 0; b < 16; b++) v[b] = Y[swz(LB | ((uint32_t)b << 4))];
-  subpass<1>(v, LB, p, job.tw, 3);
+  subpass<1>(v, w1, p, 3);
   if (p.c >= 4) {  // no stages among L bits 0-3: the pass ends here (never the last pass)
 #pragma unroll
     for (int b = 0; b < 16; b++) job.narrow[p.gidx(LB | ((uint32_t)b << 4))] = v[b];
@@ -155,14 +193,16 @@ __device__ __forceinline__ void finish_tile(uint32_t* Y, const FftJob& job, cons
   }
 #pragma unroll
   for (int b = 0; b < 16; b++) Y[swz(LB | ((uint32_t)b << 4))] = v[b];
-  __syncthreads();
   const uint32_t LC = t << 4;
+  TwSet w0;
+  tw_load<0>(w0, LC, p, job.tw, 3);
+  __syncthreads();
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const uint4 q = *reinterpret_cast<const uint4*>(Y + swz(LC | (4u * r)));
     v[4 * r] = q.x, v[4 * r + 1] = q.y, v[4 * r + 2] = q.z, v[4 * r + 3] = q.w;
   }
-  subpass<0>(v, LC, p, job.tw, 3);
+  subpass<0>(v, w0, p, 3);
   if (!last) {
     // c >= 2: four consecutive L are four consecutive, 16-byte aligned global words
 #pragma unroll
@@ -196,6 +236,8 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob*
   const bool top_zero = first && p.m >= 2 && count <= (N >> 2);
   const uint32_t t = threadIdx.x;
   const uint32_t LA = t;
+  TwSet w2;
+  tw_load<2>(w2, LA, p, job.tw, top_zero ? 1 : 3);
   uint32_t v[16];
   if (first) {
     const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
@@ -219,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob*
 #pragma unroll
     for (int b = 0; b < 16; b++) v[b] = __ldg(job.narrow + p.gidx(LA | ((uint32_t)b << 8)));
   }
-  subpass<2>(v, LA, p, job.tw, top_zero ? 1 : 3);
+  subpass<2>(v, w2, p, top_zero ? 1 : 3);
   if (p.c >= 8) {  // every stage among L bits 8-11 (a high-stage pass of at most 4 stages)
 #pragma unroll
     for (int b = 0; b < 16; b++) job.narrow[p.gidx(LA | ((uint32_t)b << 8))] = v[b];
@@ -227,8 +269,10 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob*
   }
 #pragma unroll
   for (int b = 0; b < 16; b++) Y[swz(LA | ((uint32_t)b << 8))] = v[b];
+  TwSet w1;
+  tw_load<1>(w1, sub1_base(t), p, job.tw, 3);
   __syncthreads();
-  finish_tile(Y, job, p, last);
+  finish_tile(Y, job, p, last, w1);
 }
 
 // ---------------------------------------------------------------------------
@@ -257,6 +301,8 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   const bool top_zero = first && p.m >= 2 && count <= (N >> 2);
   const uint32_t t = threadIdx.x;
   const uint32_t LA = t;
+  TwSet tws;
+  tw_load<2>(tws, LA, p, job.tw, top_zero ? 1 : 3);
   qm31 v[16];
   if (first) {
     const int loads = top_zero ? 4 : 16;
@@ -273,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
 #pragma unroll
     for (int b = 0; b < 16; b++) v[b] = to_q(job.out[p.gidx(LA | ((uint32_t)b << 8))]);
   }
-  subpass<2>(v, LA, p, job.tw, top_zero ? 1 : 3);
+  subpass<2>(v, tws, p, top_zero ? 1 : 3);
   if (p.c >= 8) {
 #pragma unroll
     for (int b = 0; b < 16; b++) job.out[p.gidx(LA | ((uint32_t)b << 8))] = from_q(v[b]);
@@ -281,11 +327,12 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   }
 #pragma unroll
   for (int b = 0; b < 16; b++) Yq[swq(LA | ((uint32_t)b << 8))] = from_q(v[b]);
+  const uint32_t LB = sub1_base(t);
+  tw_load<1>(tws, LB, p, job.tw, 3);
   __syncthreads();
-  const uint32_t LB = (t & 15u) | ((t >> 4) << 8);
 #pragma unroll
   for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LB | ((uint32_t)b << 4))]);
-  subpass<1>(v, LB, p, job.tw, 3);
+  subpass<1>(v, tws, p, 3);
   if (p.c >= 4) {
 #pragma unroll
     for (int b = 0; b < 16; b++) job.out[p.gidx(LB | ((uint32_t)b << 4))] = from_q(v[b]);
@@ -293,11 +340,12 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   }
 #pragma unroll
   for (int b = 0; b < 16; b++) Yq[swq(LB | ((uint32_t)b << 4))] = from_q(v[b]);
-  __syncthreads();
   const uint32_t LC = t << 4;
+  tw_load<0>(tws, LC, p, job.tw, 3);
+  __syncthreads();
 #pragma unroll
   for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LC | (uint32_t)b)]);
-  subpass<0>(v, LC, p, job.tw, 3);
+  subpass<0>(v, tws, p, 3);
   if (!last) {
 #pragma unroll
     for (int b = 0; b < 16; b++) job.out[p.gidx(LC | (uint32_t)b)] = from_q(v[b]);
@@ -323,7 +371,7 @@ __device__ __forceinline__ void fetch_low_tile(const FftJob* __restrict__ jobs, 
   bulk_copy_g2s(X, job.narrow + ((uint64_t)w.y << kFftLowBits), kTile * 4, bar);
 }
 
-__global__ void __launch_bounds__(kThreads, 5) fft_m31_low_tma_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work, uint32_t nwork,
+__global__ void __launch_bounds__(kThreads, 4) fft_m31_low_tma_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work, uint32_t nwork,
                                                                       uint32_t* __restrict__ status) {
   __shared__ __align__(128) uint32_t X[kTile];  // bulk-copy landing buffer (linear)
   __shared__ __align__(16) uint32_t Y[kTile];   // swizzled working buffer
@@ -340,15 +388,19 @@ __global__ void __launch_bounds__(kThreads, 5) fft_m31_low_tma_kernel(const FftJ
   for (; item < nwork; item += gridDim.x) {
     const uint2 w = work[item];
     const FftJob& job = jobs[w.x];
-    const Pass p = make_pass(job, w.y);
+    const Pass p = low_pass(job, w.y);
+    TwSet w2;
+    tw_load<2>(w2, t, p, job.tw, 3);
     const bool ok = mbar_wait(&bar, phase);
     phase ^= 1u;
     uint32_t v[16];
 #pragma unroll
     for (int b = 0; b < 16; b++) v[b] = X[t + kThreads * b];
-    subpass<2>(v, t, p, job.tw, 3);
+    subpass<2>(v, w2, p, 3);
 #pragma unroll
     for (int b = 0; b < 16; b++) Y[swz(t | ((uint32_t)b << 8))] = v[b];
+    TwSet w1;
+    tw_load<1>(w1, sub1_base(t), p, job.tw, 3);
     // X has been read by every thread: the next tile's copy may land in it
     if (__syncthreads_or(!ok)) {
       // the copy that did not complete may still land: wait for it once more
@@ -364,7 +416,7 @@ __global__ void __launch_bounds__(kThreads, 5) fft_m31_low_tma_kernel(const FftJ
       fence_proxy_async_smem();
       fetch_low_tile(jobs, work[next], X, &bar);
     }
-    finish_tile(Y, job, p, true);
+    finish_tile(Y, job, p, true, w1);
     __syncthreads();  // Y is rewritten by the next tile's first sub-pass
   }
 }

@@ -45,7 +45,6 @@ struct azk_qm31_fold_plan {
   cudaStream_t s = nullptr;
   uint64_t n_in = 0, n_out = 0;
   DevBuf ev, inv, out, ch;
-  StatusWord status;  // raised by the bulk-staged fold when a bounded wait runs out
   ~azk_qm31_fold_plan() {
     if (s) cudaStreamDestroy(s);
   }
@@ -54,11 +53,9 @@ struct azk_qm31_fold_plan {
 static double qm31_fold_run(azk_qm31_fold_plan* p, const uint4* ev, const uint4* inv, uint4* out, const uint32_t ch[4]) {
   AZK_CU(cudaMemcpyAsync(p->ch.p, ch, 16, cudaMemcpyHostToDevice, p->s));
   GpuTimer g(p->s);
-  AZK_CU(launch_fold_qm31_inv(ev, inv, p->ch.as<uint32_t>(), out, p->n_out, p->s, p->status.get(p->s)));
+  AZK_CU(launch_fold_qm31_inv(ev, inv, p->ch.as<uint32_t>(), out, p->n_out, p->s));
   g.stop();
-  const double sec = g.seconds();
-  p->status.check(p->s, "the QM31 fold");
-  return sec;
+  return g.seconds();
 }
 
 extern "C" {
@@ -165,7 +162,6 @@ struct azk_fold_chain_plan {
   std::vector<TreeJob> tree_jobs;
   std::vector<std::pair<uint64_t, uint64_t>> work_range;
   Sched sched;
-  StatusWord status;  // raised by the bulk-staged fold when a bounded wait runs out
   ~azk_fold_chain_plan() {
     if (s) cudaStreamDestroy(s);
   }
@@ -177,7 +173,7 @@ namespace {
 
 // Round r's fold from `prev` into `next` with challenge r (device limbs).
 void chain_fold(azk_fold_chain_plan* p, uint32_t r, const uint4* prev, const uint4* inv, uint4* next) {
-  AZK_CU(launch_fold_qm31_inv(prev, inv + p->inv_off[r], p->ch.as<uint32_t>() + 4 * r, next, p->count[r] / 2, p->s, p->status.get(p->s)));
+  AZK_CU(launch_fold_qm31_inv(prev, inv + p->inv_off[r], p->ch.as<uint32_t>() + 4 * r, next, p->count[r] / 2, p->s));
 }
 
 // Explicit or transcript mode (challenges already in p->ch): folds through the
@@ -349,7 +345,6 @@ azk_status azk_fold_chain_plan_execute(azk_fold_chain_plan* p, const uint32_t* e
     g.stop();
     AZK_CU(cudaMemcpyAsync(final_out, p->out.p, kQ * p->n_out, cudaMemcpyDeviceToHost, p->s));
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -369,7 +364,6 @@ azk_status azk_fold_chain_plan_execute_resident(azk_fold_chain_plan* p, const vo
     chain_fold_all(p, dev_q(dev_evaluations, evaluations_offset), dev_q(dev_inverse_layers, inverse_offset), dev_qw(dev_final, final_offset));
     g.stop();
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -395,7 +389,6 @@ azk_status azk_fold_chain_plan_execute_transcript(azk_fold_chain_plan* p, const 
     AZK_CU(cudaMemcpyAsync(final_out, p->out.p, kQ * p->n_out, cudaMemcpyDeviceToHost, p->s));
     if (challenges_out) AZK_CU(cudaMemcpyAsync(challenges_out, p->ch.p, 16ull * p->rounds, cudaMemcpyDeviceToHost, p->s));
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -421,7 +414,6 @@ azk_status azk_fold_chain_plan_execute_transcript_resident(azk_fold_chain_plan* 
     chain_fold_all(p, dev_q(dev_evaluations, evaluations_offset), dev_q(dev_inverse_layers, inverse_offset), dev_qw(dev_final, final_offset));
     g.stop();
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -446,7 +438,6 @@ azk_status azk_fold_chain_plan_execute_merkle(azk_fold_chain_plan* p, const uint
     if (commitments_out) AZK_CU(cudaMemcpyAsync(commitments_out, p->cm.p, 32ull * p->rounds, cudaMemcpyDeviceToHost, p->s));
     if (challenges_out) AZK_CU(cudaMemcpyAsync(challenges_out, p->ch.p, 16ull * p->rounds, cudaMemcpyDeviceToHost, p->s));
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -469,7 +460,6 @@ azk_status azk_fold_chain_plan_execute_merkle_readback(azk_fold_chain_plan* p, c
     if (commitments_out) AZK_CU(cudaMemcpyAsync(commitments_out, p->cm.p, 32ull * p->rounds, cudaMemcpyDeviceToHost, p->s));
     if (challenges_out) AZK_CU(cudaMemcpyAsync(challenges_out, p->ch.p, 16ull * p->rounds, cudaMemcpyDeviceToHost, p->s));
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -525,7 +515,6 @@ azk_status azk_fold_chain_plan_execute_merkle_resident(azk_fold_chain_plan* p, c
                              cudaMemcpyDeviceToDevice, p->s));
     g.stop();
     sync_stream(p->s);
-    p->status.check(p->s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }

@@ -20,27 +20,6 @@
 #include "azk_runtime.h"
 #include "azk_tuned.h"
 
-namespace azk {
-// sumcheck_kernels.cu
-struct SumcheckOut {
-  uint32_t claimed_sum;
-  uint32_t final_eval;
-  uint64_t digest[4];
-  uint32_t* r0;
-  uint32_t* r1;
-  uint32_t* challenges;
-};
-struct SumcheckJob {
-  const uint32_t* evals;
-  uint32_t* scratch;
-  SumcheckOut* out;
-  uint32_t log_n;
-  uint32_t pad;
-};
-cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s);
-cudaError_t launch_sumcheck_batch(const SumcheckJob* d_jobs, uint32_t count, cudaStream_t s);
-}  // namespace azk
-
 using namespace azk;
 
 namespace {
@@ -968,13 +947,14 @@ struct Resident {
 struct Staging {
   uint8_t* p = nullptr;
   size_t n = 0;
+  unsigned flags = cudaHostAllocDefault;
   uint8_t* ensure(size_t bytes) {
     if (bytes > n) {
       if (p) cudaFreeHost(p);
       p = nullptr;
       n = 0;
       size_t want = std::max<size_t>(bytes, 1 << 20);
-      AZK_CU(cudaHostAlloc(reinterpret_cast<void**>(&p), want, cudaHostAllocDefault));
+      AZK_CU(cudaHostAlloc(reinterpret_cast<void**>(&p), want, flags));
       n = want;
     }
     return p;
@@ -985,24 +965,27 @@ struct Staging {
 };
 
 // One table slot of the sum-check lane: device buffers for a table of up to
-// 2^cap_log words and page-locked staging for its input and results.
+// 2^cap_log words and page-locked, device-mapped staging for its input and
+// results (the kernel writes the results straight into it).
 struct SumcheckSlot {
   SumcheckBufs bufs;
   Staging pin;
   uint32_t cap_log = 0;  // 0: not allocated
   bool grow = false;     // cap_log was raised: the buffers are reallocated before use
   std::shared_ptr<ServeJob> job;
+  SumcheckSlot() { pin.flags = cudaHostAllocMapped; }
 };
-// A lane stream and the batch it runs.
+// A lane stream and the batch it runs.  Nothing is queued on a lane stream after a
+// batch's kernel (no event, no copy back): the completer polls the stream, so a
+// worker stream that shares the lane stream's hardware queue never waits behind a
+// queued operation that waits for the digest.
 struct SumcheckStream {
   cudaStream_t s = nullptr;
-  cudaEvent_t done = nullptr;
-  DevBuf jobs;
   std::vector<int> slots;
 };
-constexpr int kLaneSlots = 96;    // tables in the lane at once
-constexpr int kLaneStreams = 32;  // batches in flight at once
-constexpr int kLaneBatch = 32;    // tables per launch
+constexpr int kLaneSlots = 96;                 // tables in the lane at once
+constexpr int kLaneStreams = 32;               // batches in flight at once
+constexpr int kLaneBatch = kSumcheckBatchMax;  // tables per launch
 
 }  // namespace
 
@@ -1395,20 +1378,26 @@ void lane_launcher(azk_server* sv) {
     st.slots = batch;
     std::string error;
     try {
-      std::vector<SumcheckJob> jobs;
-      for (int slot : batch) {
-        SumcheckSlot& sl = *sv->sc_slot[slot];
+      SumcheckBatch jobs{};
+      for (size_t k = 0; k < batch.size(); k++) {
+        SumcheckSlot& sl = *sv->sc_slot[batch[k]];
         const uint32_t logn = sl.job->logn;
         uint8_t* pin = sl.pin.p;
+        // results land in the slot's mapped staging, after the table words
         SumcheckOut* h = reinterpret_cast<SumcheckOut*>(pin + align_up(4ull << logn, 64));
-        *h = sumcheck_out_ptrs(sl.bufs, logn);
+        uint32_t* rounds_h = reinterpret_cast<uint32_t*>(h + 1);
+        SumcheckOut* dh = nullptr;
+        AZK_CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dh), h, 0));
+        uint32_t* drounds = reinterpret_cast<uint32_t*>(dh + 1);
+        *h = SumcheckOut{};
+        h->r0 = drounds;
+        h->r1 = drounds + logn;
+        h->challenges = drounds + 2 * logn;
+        std::memset(rounds_h, 0, 12ull * logn);
         AZK_CU(cudaMemcpyAsync(sl.bufs.ev.p, pin, 4ull << logn, cudaMemcpyHostToDevice, st.s));
-        AZK_CU(cudaMemcpyAsync(sl.bufs.out.p, h, sizeof(SumcheckOut), cudaMemcpyHostToDevice, st.s));
-        jobs.push_back(SumcheckJob{sl.bufs.ev.as<uint32_t>(), sl.bufs.scratch.as<uint32_t>(), sl.bufs.out.as<SumcheckOut>(), logn, 0});
+        jobs.job[k] = SumcheckJob{sl.bufs.ev.as<uint32_t>(), sl.bufs.scratch.as<uint32_t>(), dh, logn, 0};
       }
-      AZK_CU(cudaMemcpyAsync(st.jobs.p, jobs.data(), sizeof(SumcheckJob) * jobs.size(), cudaMemcpyHostToDevice, st.s));
-      AZK_CU(launch_sumcheck_batch(st.jobs.as<SumcheckJob>(), (uint32_t)jobs.size(), st.s));
-      AZK_CU(cudaEventRecord(st.done, st.s));
+      AZK_CU(launch_sumcheck_batch(jobs, (uint32_t)batch.size(), st.s));
     } catch (const Error& e) {
       error = e.msg.empty() ? "sum-check launch failed" : e.msg;
     } catch (const std::exception& e) {
@@ -1437,64 +1426,56 @@ void lane_launcher(azk_server* sv) {
   }
 }
 
-// Lane completer: waits for each launched batch in launch order (a blocking-sync
-// event, no spinning), reads its results back and publishes them.
+// Lane completer: polls the lane streams that run a batch (cudaStreamQuery every
+// 200 us, nothing queued behind the kernels), and publishes a finished batch's
+// results from its slots' mapped staging.
 void lane_completer(azk_server* sv) {
   cudaSetDevice(sv->ctx->device);
   for (;;) {
-    int sid = -1;
+    std::vector<int> inflight;
     {
       std::unique_lock<std::mutex> lk(sv->mu);
       sv->lane_cv.wait(lk, [&] { return !sv->sc_inflight.empty() || sv->launcher_done; });
       if (sv->sc_inflight.empty()) return;
-      sid = sv->sc_inflight.front();
-      sv->sc_inflight.pop_front();
+      inflight.assign(sv->sc_inflight.begin(), sv->sc_inflight.end());
     }
-    SumcheckStream& st = sv->sc_stream[sid];
-    std::string error;
-    std::vector<std::vector<uint32_t>> words(st.slots.size());
-    try {
-      AZK_CU(cudaEventSynchronize(st.done));
-      for (size_t k = 0; k < st.slots.size(); k++) {
-        SumcheckSlot& sl = *sv->sc_slot[st.slots[k]];
-        const uint32_t logn = sl.job->logn;
-        SumcheckOut* h = reinterpret_cast<SumcheckOut*>(sl.pin.p + align_up(4ull << logn, 64));
-        uint32_t* rounds_h = reinterpret_cast<uint32_t*>(h + 1);
-        AZK_CU(cudaMemcpyAsync(h, sl.bufs.out.p, sizeof(SumcheckOut), cudaMemcpyDeviceToHost, st.s));
-        AZK_CU(cudaMemcpyAsync(rounds_h, sl.bufs.rounds.p, 12ull * logn, cudaMemcpyDeviceToHost, st.s));
-      }
-      sync_stream(st.s);
-      for (size_t k = 0; k < st.slots.size(); k++) {
-        SumcheckSlot& sl = *sv->sc_slot[st.slots[k]];
-        const uint32_t logn = sl.job->logn;
-        SumcheckOut* h = reinterpret_cast<SumcheckOut*>(sl.pin.p + align_up(4ull << logn, 64));
-        words[k] = sumcheck_words(*h, reinterpret_cast<uint32_t*>(h + 1), logn);
-      }
-    } catch (const Error& e) {
-      error = e.msg;
-    } catch (const std::exception& e) {
-      error = e.what();
+    std::vector<std::pair<int, std::string>> finished;  // (stream, error)
+    for (int sid : inflight) {
+      const cudaError_t e = cudaStreamQuery(sv->sc_stream[sid].s);
+      if (e == cudaErrorNotReady) continue;
+      if (e != cudaSuccess) cudaGetLastError();
+      finished.emplace_back(sid, e == cudaSuccess ? std::string() : std::string("sum-check batch failed: ") + cudaGetErrorString(e));
+    }
+    if (finished.empty()) {
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+      continue;
     }
     std::lock_guard<std::mutex> lk(sv->mu);
-    for (size_t k = 0; k < st.slots.size(); k++) {
-      const int slot = st.slots[k];
-      auto job = sv->sc_slot[slot]->job;
-      sv->sc_slot[slot]->job = nullptr;
-      sv->sc_free.push_back(slot);
-      if (job->id == 0) {  // a warm-up table
-        job->state = error.empty() ? 2 : 3;
-        sv->running--;
-        sv->warm_pending--;
-        continue;
+    for (auto& [sid, error] : finished) {
+      SumcheckStream& st = sv->sc_stream[sid];
+      for (const int slot : st.slots) {
+        SumcheckSlot& sl = *sv->sc_slot[slot];
+        auto job = sl.job;
+        sl.job = nullptr;
+        sv->sc_free.push_back(slot);
+        if (job->id == 0) {  // a warm-up table
+          job->state = error.empty() ? 2 : 3;
+          sv->running--;
+          sv->warm_pending--;
+          continue;
+        }
+        if (error.empty()) {
+          const SumcheckOut* h = reinterpret_cast<const SumcheckOut*>(sl.pin.p + align_up(4ull << job->logn, 64));
+          const std::vector<uint32_t> words = sumcheck_words(*h, reinterpret_cast<const uint32_t*>(h + 1), job->logn);
+          job->result.resize(4 * words.size());
+          std::memcpy(job->result.data(), words.data(), job->result.size());
+        }
+        publish(sv, *job, error.empty() ? 2 : 3, error);
       }
-      if (error.empty()) {
-        job->result.resize(4 * words[k].size());
-        std::memcpy(job->result.data(), words[k].data(), job->result.size());
-      }
-      publish(sv, *job, error.empty() ? 2 : 3, error);
+      st.slots.clear();
+      sv->sc_inflight.erase(std::find(sv->sc_inflight.begin(), sv->sc_inflight.end(), sid));
+      sv->sc_idle.push_back(sid);
     }
-    st.slots.clear();
-    sv->sc_idle.push_back(sid);
     sv->cv.notify_all();
     sv->done_cv.notify_all();
     sv->lane_cv.notify_all();
@@ -1656,8 +1637,6 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
     sv->sc_stream.resize(kLaneStreams);
     for (int k = 0; k < kLaneStreams; k++) {
       AZK_CU(cudaStreamCreateWithPriority(&sv->sc_stream[k].s, cudaStreamNonBlocking, prio_hi));
-      AZK_CU(cudaEventCreateWithFlags(&sv->sc_stream[k].done, cudaEventBlockingSync | cudaEventDisableTiming));
-      sv->sc_stream[k].jobs.alloc(sizeof(SumcheckJob) * kLaneBatch, "Sumcheck.LaneJobs");
       sv->sc_idle.push_back(k);
     }
     for (int k = 0; k < kLaneSlots; k++) {
@@ -1857,10 +1836,8 @@ void azk_server_destroy(azk_server* sv) {
   sv->lane_cv.notify_all();
   if (sv->sc_launcher.joinable()) sv->sc_launcher.join();
   if (sv->sc_completer.joinable()) sv->sc_completer.join();
-  for (auto& st : sv->sc_stream) {
-    if (st.done) cudaEventDestroy(st.done);
+  for (auto& st : sv->sc_stream)
     if (st.s) cudaStreamDestroy(st.s);
-  }
   for (auto st : sv->streams)
     if (st) cudaStreamDestroy(st);
   delete sv;

@@ -172,16 +172,6 @@ void FftPlan::check_status(cudaStream_t s) {
     fail(AZK_ERR_DEVICE_TIMEOUT, "a Circle FFT pass gave up waiting for its bulk tile copies");
   }
 }
-void StatusWord::check(cudaStream_t s, const char* what) {
-  if (!d.p) return;
-  uint32_t f = 0;
-  AZK_CU(cudaMemcpyAsync(&f, d.p, 4, cudaMemcpyDeviceToHost, s));
-  sync_stream(s);
-  if (f) {
-    AZK_CU(cudaMemsetAsync(d.p, 0, 4, s));
-    fail(AZK_ERR_DEVICE_TIMEOUT, std::string(what) + " gave up waiting for its bulk copies");
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Monomial -> FFT basis (host preprocessing of CircleCodewordPlan.execute(polynomial:))
@@ -1014,14 +1004,11 @@ azk_status azk_qm31_fold(azk_ctx* ctx, const uint32_t* ev, uint64_t n, const uin
     AZK_CU(cudaMemcpyAsync(de.p, ev, 16 * n, cudaMemcpyHostToDevice, s));
     AZK_CU(cudaMemcpyAsync(di.p, inv, 8 * n, cudaMemcpyHostToDevice, s));
     AZK_CU(cudaMemcpyAsync(dc.p, ch, 16, cudaMemcpyHostToDevice, s));
-    StatusWord status;
-    uint32_t* dst = status.get(s);
     GpuTimer g(s);
-    AZK_CU(launch_fold_qm31_inv(de.as<uint4>(), di.as<uint4>(), dc.as<uint32_t>(), dout.as<uint4>(), n / 2, s, dst));
+    AZK_CU(launch_fold_qm31_inv(de.as<uint4>(), di.as<uint4>(), dc.as<uint32_t>(), dout.as<uint4>(), n / 2, s));
     g.stop();
     AZK_CU(cudaMemcpyAsync(out, dout.p, 8 * n, cudaMemcpyDeviceToHost, s));
     sync_stream(s);
-    status.check(s, "the QM31 fold");
     fill_stats(st, t, 0, g.seconds());
   });
 }
@@ -1115,8 +1102,6 @@ azk_status azk_qm31_merkle_fold_chain(azk_ctx* ctx, const uint32_t* ev, uint64_t
     DevBuf dwork(work.size() * sizeof(uint2), "QM31Chain.Work");
     AZK_CU(cudaMemcpyAsync(jobs.p, hj.data(), sizeof(TreeJob) * rounds, cudaMemcpyHostToDevice, s));
     AZK_CU(cudaMemcpyAsync(dwork.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
-    StatusWord status;
-    uint32_t* dst = status.get(s);
     GpuTimer g(s);
     AZK_CU(launch_qm31_transcript_prefix(tr.as<Transcript>(), n, rounds, s));
     uint64_t inv_off = 0;
@@ -1124,7 +1109,7 @@ azk_status azk_qm31_merkle_fold_chain(azk_ctx* ctx, const uint32_t* ev, uint64_t
       AZK_CU(launch_tree_jobs(jobs.as<TreeJob>(), dwork.as<uint2>() + ranges[r].first, (uint32_t)ranges[r].second, hj[r].tile_log, kLeafQM31, 256, s));
       uint64_t m = n >> (r + 1);
       AZK_CU(launch_fold_qm31_inv(layers.as<uint4>() + layer_offset(logn, r), dinv.as<uint4>() + inv_off, dch.as<uint32_t>() + 4 * r,
-                                  layers.as<uint4>() + layer_offset(logn, r + 1), m, s, dst));
+                                  layers.as<uint4>() + layer_offset(logn, r + 1), m, s));
       inv_off += m;
     }
     g.stop();
@@ -1132,7 +1117,6 @@ azk_status azk_qm31_merkle_fold_chain(azk_ctx* ctx, const uint32_t* ev, uint64_t
     if (commitments_out) AZK_CU(cudaMemcpyAsync(commitments_out, dcm.p, 32ull * rounds, cudaMemcpyDeviceToHost, s));
     if (ch_out) AZK_CU(cudaMemcpyAsync(ch_out, dch.p, 16ull * rounds, cudaMemcpyDeviceToHost, s));
     sync_stream(s);
-    status.check(s, "a QM31 fold-chain round");
     fill_stats(st, t, 0, g.seconds());
   });
 }

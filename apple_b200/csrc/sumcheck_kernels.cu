@@ -13,23 +13,6 @@
 
 namespace azk {
 
-struct SumcheckOut {
-  uint32_t claimed_sum;
-  uint32_t final_eval;
-  uint64_t digest[4];
-  uint32_t* r0;          // rounds
-  uint32_t* r1;          // rounds
-  uint32_t* challenges;  // rounds
-};
-// One table of a batched launch.
-struct SumcheckJob {
-  const uint32_t* evals;
-  uint32_t* scratch;  // 2^log_n words
-  SumcheckOut* out;
-  uint32_t log_n;
-  uint32_t pad;
-};
-
 __device__ __forceinline__ uint32_t block_sum_m31(uint32_t v, uint32_t* red) {
   // warp tree then one warp over the warp sums (values < 2^31, sums reduced each step)
   for (int o = 16; o > 0; o >>= 1) v = m31_add(v, __shfl_down_sync(0xffffffffu, v, o));
@@ -241,10 +224,7 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
   uint32_t z = 0, o = 0;
   if (t < 32) {
     const uint64_t d = digest_words_warp(evals, n);
-    if (t < 4) {
-      s_digest[t] = d;
-      out->digest[t] = d;
-    }
+    if (t < 4) s_digest[t] = d;
   } else if (n >= 4) {
     pair_sums(reinterpret_cast<const uint4*>(evals), n >> 2, t - 32, blockDim.x - 32, z, o);
   } else if (n == 2 && t == 32) {
@@ -258,6 +238,7 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
   Transcript tr;
   if (t == 0) {
     out->claimed_sum = total;
+    for (int i = 0; i < 4; i++) out->digest[i] = s_digest[i];
     tr_reset(tr);
     FrameBuf f;
     sc_frame(f, 0);
@@ -269,11 +250,19 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
   }
   const uint32_t* cur = evals;
   uint32_t* bufs[2] = {scratch, scratch + (n >> 1)};
+  // the result arrays' addresses, read once (`out` may be host memory mapped
+  // into the device's address space)
+  uint32_t *r0 = nullptr, *r1 = nullptr, *chs = nullptr;
+  if (t == 0) {
+    r0 = out->r0;
+    r1 = out->r1;
+    chs = out->challenges;
+  }
   for (uint32_t r = 0; r < log_n; r++) {
     const uint64_t half = (n >> r) >> 1;
     if (t == 0) {
-      out->r0[r] = zs;
-      out->r1[r] = os;
+      r0[r] = zs;
+      r1[r] = os;
       FrameBuf f;
       sc_frame(f, 1);
       fb_u32(f, r);
@@ -286,7 +275,7 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
       tr_absorb(tr, f.b, f.n);
       uint32_t c;
       tr_squeeze_u32(tr, 1, kP, &c);
-      out->challenges[r] = c;
+      chs[r] = c;
       s_ch = c;
     }
     __syncthreads();
@@ -336,8 +325,8 @@ __global__ void __launch_bounds__(kSumcheckThreads) sumcheck_kernel(const uint32
   sumcheck_prove_block(evals, log_n, scratch, out);
 }
 
-__global__ void __launch_bounds__(kSumcheckThreads) sumcheck_batch_kernel(const SumcheckJob* __restrict__ jobs) {
-  const SumcheckJob j = jobs[blockIdx.x];
+__global__ void __launch_bounds__(kSumcheckThreads) sumcheck_batch_kernel(const __grid_constant__ SumcheckBatch batch) {
+  const SumcheckJob& j = batch.job[blockIdx.x];
   sumcheck_prove_block(j.evals, j.log_n, j.scratch, j.out);
 }
 
@@ -346,9 +335,10 @@ cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scr
   return cudaGetLastError();
 }
 
-cudaError_t launch_sumcheck_batch(const SumcheckJob* d_jobs, uint32_t count, cudaStream_t s) {
+cudaError_t launch_sumcheck_batch(const SumcheckBatch& batch, uint32_t count, cudaStream_t s) {
   if (!count) return cudaSuccess;
-  sumcheck_batch_kernel<<<count, kSumcheckThreads, 0, s>>>(d_jobs);
+  if (count > kSumcheckBatchMax) return cudaErrorInvalidValue;
+  sumcheck_batch_kernel<<<count, kSumcheckThreads, 0, s>>>(batch);
   return cudaGetLastError();
 }
 
