@@ -28,6 +28,10 @@ from ._capi import (  # noqa: E402,F401
 from .plans import (  # noqa: E402,F401
     BatchProver,
     CircleCodewordPlan,
+    CircleDomainMaterializationPlan,
+    CircleFRIFoldChainPlan,
+    CircleFRIFoldPlan,
+    CircleFRIMerkleTranscriptFoldChainPlan,
     CircleFRIResidentQueryExtractor,
     CirclePCSFRIProver,
     CircleWitnessToFFTBasisPlan,

@@ -134,6 +134,33 @@ PROTOTYPES = {
     "azk_query_extractor_query_bytes": (U64, [U32, U32]),
     "azk_query_extractor_extract": (I32, [P, P, U64, P, P, U64, P, U64P, STATS]),
     "azk_query_extractor_destroy": (None, [P]),
+    "azk_domain_plan_create": (I32, [P, U32, U32, U32, U32, PP]),
+    "azk_domain_plan_info": (I32, [P, U64P, U64P, U64P, STATS]),
+    "azk_domain_plan_buffers": (I32, [P, PP, PP, PP]),
+    "azk_domain_plan_read_points": (I32, [P, P]),
+    "azk_domain_plan_read_twiddles": (I32, [P, P]),
+    "azk_domain_plan_read_inverse_layers": (I32, [P, P]),
+    "azk_domain_plan_destroy": (None, [P]),
+    "azk_circle_fold_plan_create": (I32, [P, U32, PP]),
+    "azk_circle_fold_plan_execute": (I32, [P, P, P, P, STATS]),
+    "azk_circle_fold_plan_execute_resident": (I32, [P, P, U64, P, U64, P, STATS]),
+    "azk_circle_fold_plan_read_inverse": (I32, [P, P]),
+    "azk_circle_fold_plan_clear": (I32, [P]),
+    "azk_circle_fold_plan_destroy": (None, [P]),
+    "azk_circle_fold_chain_plan_create": (I32, [P, U32, U32, PP]),
+    "azk_circle_fold_chain_plan_execute": (I32, [P, P, P, P, STATS]),
+    "azk_circle_fold_chain_plan_execute_resident": (I32, [P, P, U64, P, U64, P, STATS]),
+    "azk_circle_fold_chain_plan_read_inverse_layers": (I32, [P, P]),
+    "azk_circle_fold_chain_plan_clear": (I32, [P]),
+    "azk_circle_fold_chain_plan_destroy": (None, [P]),
+    "azk_circle_merkle_chain_plan_create": (I32, [P, U32, U32, U32, U32, P, U32, PP]),
+    "azk_circle_merkle_chain_plan_info": (I32, [P, U64P, U64P]),
+    "azk_circle_merkle_chain_plan_execute": (I32, [P, P, P, P, P, STATS]),
+    "azk_circle_merkle_chain_plan_execute_resident": (I32, [P, P, U64, P, U64, P, U64, U64, P, U64, P, U64, STATS]),
+    "azk_circle_merkle_chain_plan_challenges": (I32, [P, P]),
+    "azk_circle_merkle_chain_plan_read_inverse_layers": (I32, [P, P]),
+    "azk_circle_merkle_chain_plan_clear": (I32, [P]),
+    "azk_circle_merkle_chain_plan_destroy": (None, [P]),
     "azk_pcs_prover_create": (I32, [P, U32, U32, U32, U32, U32, SCHED, PP]),
     "azk_pcs_proof_size": (U64, [U32, U32, U32, U32, U32]),
     "azk_pcs_prover_prove_evaluations": (I32, [P, P, P, P, U64, P, U64P, STATS]),

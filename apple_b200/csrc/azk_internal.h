@@ -205,6 +205,7 @@ cudaError_t launch_tree_jobs(const TreeJob* d_jobs, const uint2* d_work, uint32_
 cudaError_t launch_gather_openings(const TreeJob* d_job, const uint64_t* d_idx, uint32_t nidx, uint64_t* d_out, cudaStream_t s);
 cudaError_t launch_domain_tables(uint32_t logn, uint32_t* d_tw, uint32_t* d_inv, cudaStream_t s);
 cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s);
+cudaError_t launch_widen_m31(const uint32_t* d_in, uint4* d_out, uint64_t n, cudaStream_t s);
 // Witness columns -> FFT basis (witness_kernels.cu): factorial tables of n
 // entries (seg: ceil(n/1024) words of scratch), then the transform of two columns
 // of count_x / count_y monomial coefficients into 2n interleaved QM31.

@@ -64,6 +64,21 @@ cudaError_t launch_domain_points(uint32_t logn, uint32_t* d_xy, cudaStream_t s) 
   return cudaGetLastError();
 }
 
+// M31 values as QM31 values (a, 0, 0, 0): the inverse-domain layers in the
+// 16-byte layout the QM31 fold plans take.
+__global__ void widen_m31_kernel(const uint32_t* __restrict__ in, uint4* __restrict__ out, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = make_uint4(__ldg(in + i), 0u, 0u, 0u);
+}
+
+cudaError_t launch_widen_m31(const uint32_t* d_in, uint4* d_out, uint64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  uint64_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  widen_m31_kernel<<<(unsigned)blocks, 256, 0, s>>>(d_in, d_out, n);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Circle FFT.  Stages run logn-1 ... 0; stage s pairs (i, i + 2^s) inside blocks
 // of 2^(s+1) with the block's twiddle t: (l + r t, l - r t).  A pass runs a range

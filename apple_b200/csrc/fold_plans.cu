@@ -162,6 +162,11 @@ struct azk_fold_chain_plan {
   std::vector<TreeJob> tree_jobs;
   std::vector<std::pair<uint64_t, uint64_t>> work_range;
   Sched sched;
+  // Merkle-mode transcript: the QM31 fold chain's own frames, or (a Circle FRI
+  // Merkle-transcript chain) the Circle PCS V1 frames, whose prefix comes from the
+  // PCS instance fields in `pcs` (log size, security parameters, public digest)
+  uint32_t root_kind = kRootQM31Round;
+  DevBuf pcs;
   ~azk_fold_chain_plan() {
     if (s) cudaStreamDestroy(s);
   }
@@ -191,7 +196,10 @@ void chain_fold_all(azk_fold_chain_plan* p, const uint4* ev, const uint4* inv, u
 // 0 is read from `ev` (copied into log[0] first when `copy_first`).  With
 // `first_root` (device), round 0's commitment is that root instead of a tree.
 void chain_merkle(azk_fold_chain_plan* p, const uint4* ev, const uint4* inv, uint4* log, bool copy_first, uint4* out, const uint64_t* first_root) {
-  AZK_CU(launch_qm31_transcript_prefix(p->tr.as<Transcript>(), p->n_in, p->rounds, p->s));
+  if (p->root_kind == kRootCircleRound)
+    AZK_CU(launch_pcs_prefix(p->pcs.as<PcsInstance>(), 1, p->s));
+  else
+    AZK_CU(launch_qm31_transcript_prefix(p->tr.as<Transcript>(), p->n_in, p->rounds, p->s));
   if (copy_first) AZK_CU(cudaMemcpyAsync(log, ev, kQ * p->n_in, cudaMemcpyDeviceToDevice, p->s));
   const uint4* cur = copy_first ? log : ev;
   // per-round layer pointers in the tree jobs: rewritten for this call
@@ -200,7 +208,7 @@ void chain_merkle(azk_fold_chain_plan* p, const uint4* ev, const uint4* inv, uin
   for (uint32_t r = 0; r < p->rounds; r++) {
     if (r == 0 && first_root) {
       AZK_CU(cudaMemcpyAsync(p->cm.p, first_root, 32, cudaMemcpyDeviceToDevice, p->s));
-      AZK_CU(launch_transcript_rounds_given(p->tr.as<Transcript>(), kRootQM31Round, p->cm.as<uint64_t>(), 1, p->n_in, p->ch.as<uint32_t>(), p->s));
+      AZK_CU(launch_transcript_rounds_given(p->tr.as<Transcript>(), p->root_kind, p->cm.as<uint64_t>(), 1, p->n_in, p->ch.as<uint32_t>(), p->s));
     } else {
       AZK_CU(launch_tree_jobs(p->jobs.as<TreeJob>(), p->work.as<uint2>() + p->work_range[r].first, (uint32_t)p->work_range[r].second,
                               p->tree_jobs[r].tile_log, kLeafQM31, tree_threads(p->sched, p->tree_jobs[r].logn), p->s));
@@ -672,5 +680,377 @@ azk_status azk_query_extractor_extract(azk_query_extractor* x, const void* dev_l
 }
 
 void azk_query_extractor_destroy(azk_query_extractor* x) { delete x; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CircleDomainMaterializationPlan (CircleDomainMaterializationPlan.swift:52-219)
+// and the Circle FRI fold plans built on it (CircleFRIFoldPlan.swift:5-518): the
+// canonical domain's inverse-domain layers are materialised once per plan as QM31
+// values (a, 0, 0, 0) and the folds run through the QM31 fold plans above.
+// ---------------------------------------------------------------------------
+struct azk_domain_plan {
+  azk_ctx* ctx = nullptr;
+  std::mutex mu;
+  cudaStream_t s = nullptr;
+  uint32_t logn = 0, rounds = 0;
+  bool points = false, twiddles = false;
+  uint64_t inv_total = 0;
+  DevBuf pts, tw, inv;
+  double gpu_s = 0, wall_s = 0;
+  ~azk_domain_plan() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+struct azk_circle_fold_plan {
+  azk_ctx* ctx = nullptr;
+  std::mutex mu;
+  azk_domain_plan* dom = nullptr;
+  azk_qm31_fold_plan* fold = nullptr;
+  ~azk_circle_fold_plan();
+};
+
+struct azk_circle_fold_chain_plan {
+  azk_ctx* ctx = nullptr;
+  std::mutex mu;
+  azk_domain_plan* dom = nullptr;
+  azk_fold_chain_plan* chain = nullptr;
+  ~azk_circle_fold_chain_plan();
+};
+
+struct azk_circle_merkle_chain_plan {
+  azk_ctx* ctx = nullptr;
+  std::mutex mu;
+  azk_domain_plan* dom = nullptr;
+  azk_fold_chain_plan* chain = nullptr;
+  ~azk_circle_merkle_chain_plan();
+};
+
+extern "C" {
+
+azk_status azk_domain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t materialize_points, uint32_t materialize_twiddles, uint32_t inverse_rounds,
+                                  azk_domain_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out);
+    // CircleDomainMaterializationPlan.init preconditions (:59-66)
+    layout(log_size >= 1 && log_size <= 26);
+    layout(materialize_points || materialize_twiddles || inverse_rounds > 0);
+    layout(inverse_rounds <= log_size);
+    AZK_CU(cudaSetDevice(ctx->device));
+    Timer t;
+    auto p = std::make_unique<azk_domain_plan>();
+    p->ctx = ctx;
+    p->logn = log_size;
+    p->rounds = inverse_rounds;
+    p->points = materialize_points != 0;
+    p->twiddles = materialize_twiddles != 0;
+    const uint64_t n = 1ull << log_size;
+    p->inv_total = n - (n >> inverse_rounds);
+    p->s = plan_stream();
+    const auto& d = domain_tables(ctx, log_size);
+    if (p->points) p->pts.alloc(8 * n, "CircleDomain.DomainPoints");
+    if (p->twiddles) p->tw.alloc(4 * (n - 1), "CircleDomain.CodewordFFTTwiddles");
+    if (inverse_rounds) p->inv.alloc(kQ * p->inv_total, "CircleDomain.InverseDomain");
+    GpuTimer g(p->s);
+    if (p->points) AZK_CU(launch_domain_points(log_size, p->pts.as<uint32_t>(), p->s));
+    if (p->twiddles) AZK_CU(cudaMemcpyAsync(p->tw.p, d.tw, 4 * (n - 1), cudaMemcpyDeviceToDevice, p->s));
+    // inverse layer k (n >> (k+1) values) sits at n - (n >> k) in the context's
+    // table, the same offset the concatenated layers have here
+    if (inverse_rounds) AZK_CU(launch_widen_m31(d.inv, p->inv.as<uint4>(), p->inv_total, p->s));
+    g.stop();
+    p->gpu_s = g.seconds();
+    sync_stream(p->s);
+    p->wall_s = t.seconds();
+    *out = p.release();
+  });
+}
+
+azk_status azk_domain_plan_info(azk_domain_plan* p, uint64_t* twiddle_count, uint64_t* inverse_count, uint64_t* output_count, azk_stats* materialization) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    const uint64_t n = 1ull << p->logn;
+    if (twiddle_count) *twiddle_count = n - 1;
+    if (inverse_count) *inverse_count = p->inv_total;
+    if (output_count) *output_count = n >> p->rounds;
+    if (materialization) {
+      materialization->cpu_wall_s = p->wall_s;
+      materialization->gpu_s = p->gpu_s;
+      materialization->cpu_submit_ns = 0;
+    }
+  });
+}
+
+azk_status azk_domain_plan_buffers(azk_domain_plan* p, const void** points, const void** twiddles, const void** inverse_layers) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    if (points) *points = p->pts.p;
+    if (twiddles) *twiddles = p->tw.p;
+    if (inverse_layers) *inverse_layers = p->inv.p;
+  });
+}
+
+static void domain_read(azk_domain_plan* p, const DevBuf& b, bool present, void* out, uint64_t bytes) {
+  layout(out != nullptr);
+  // requireDomainPointBuffer / requireCodewordTwiddleBuffer / requireInverseDomainBuffer (:135-154)
+  require(present, AZK_ERR_INVALID_INPUT_LAYOUT, "the plan did not materialise this table");
+  std::lock_guard<std::mutex> lk(p->mu);
+  AZK_CU(cudaSetDevice(p->ctx->device));
+  AZK_CU(cudaMemcpyAsync(out, b.p, bytes, cudaMemcpyDeviceToHost, p->s));
+  sync_stream(p->s);
+}
+
+azk_status azk_domain_plan_read_points(azk_domain_plan* p, uint32_t* xy_out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    domain_read(p, p->pts, p->points, xy_out, 8ull << p->logn);
+  });
+}
+
+azk_status azk_domain_plan_read_twiddles(azk_domain_plan* p, uint32_t* out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    domain_read(p, p->tw, p->twiddles, out, 4 * ((1ull << p->logn) - 1));
+  });
+}
+
+azk_status azk_domain_plan_read_inverse_layers(azk_domain_plan* p, uint32_t* out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    domain_read(p, p->inv, p->rounds > 0, out, kQ * p->inv_total);
+  });
+}
+
+void azk_domain_plan_destroy(azk_domain_plan* p) { delete p; }
+
+}  // extern "C"
+
+azk_circle_fold_plan::~azk_circle_fold_plan() {
+  azk_qm31_fold_plan_destroy(fold);
+  azk_domain_plan_destroy(dom);
+}
+azk_circle_fold_chain_plan::~azk_circle_fold_chain_plan() {
+  azk_fold_chain_plan_destroy(chain);
+  azk_domain_plan_destroy(dom);
+}
+azk_circle_merkle_chain_plan::~azk_circle_merkle_chain_plan() {
+  azk_fold_chain_plan_destroy(chain);
+  azk_domain_plan_destroy(dom);
+}
+
+namespace {
+// A C-ABI call made inside another one: its failure becomes this call's.
+void forward(azk_ctx* ctx, azk_status st) {
+  if (st != AZK_OK) fail(st, azk_last_error_message(ctx));
+}
+}  // namespace
+
+extern "C" {
+
+// ---- CircleFRIFoldPlan (:5-130): circle -> line fold of the whole domain ----
+azk_status azk_circle_fold_plan_create(azk_ctx* ctx, uint32_t log_size, azk_circle_fold_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && log_size >= 1 && log_size <= 26);
+    auto p = std::make_unique<azk_circle_fold_plan>();
+    p->ctx = ctx;
+    forward(ctx, azk_domain_plan_create(ctx, log_size, 0, 0, 1, &p->dom));
+    forward(ctx, azk_qm31_fold_plan_create(ctx, 1ull << log_size, &p->fold));
+    *out = p.release();
+  });
+}
+
+azk_status azk_circle_fold_plan_execute(azk_circle_fold_plan* p, const uint32_t* evaluations, const uint32_t challenge[4], uint32_t* out,
+                                        azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && evaluations && challenge && out);
+    const uint64_t n = 1ull << p->dom->logn;
+    check_canonical_host(evaluations, 4 * n);
+    check_canonical_host(challenge, 4);
+    std::lock_guard<std::mutex> lk(p->mu);
+    azk_qm31_fold_plan* f = p->fold;
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    AZK_CU(cudaMemcpyAsync(f->ev.p, evaluations, kQ * n, cudaMemcpyHostToDevice, f->s));
+    azk_stats inner{};
+    forward(p->ctx, azk_qm31_fold_plan_execute_resident(f, f->ev.p, 0, p->dom->inv.p, 0, f->out.p, 0, challenge, &inner));
+    AZK_CU(cudaMemcpyAsync(out, f->out.p, kQ * (n / 2), cudaMemcpyDeviceToHost, f->s));
+    sync_stream(f->s);
+    fill_stats(st, t, 0, inner.gpu_s);
+  });
+}
+
+azk_status azk_circle_fold_plan_execute_resident(azk_circle_fold_plan* p, const void* dev_evaluations, uint64_t evaluations_offset, void* dev_out,
+                                                 uint64_t out_offset, const uint32_t challenge[4], azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    std::lock_guard<std::mutex> lk(p->mu);
+    forward(p->ctx, azk_qm31_fold_plan_execute_resident(p->fold, dev_evaluations, evaluations_offset, p->dom->inv.p, 0, dev_out, out_offset, challenge, st));
+  });
+}
+
+azk_status azk_circle_fold_plan_read_inverse(azk_circle_fold_plan* p, uint32_t* out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_domain_plan_read_inverse_layers(p->dom, out));
+  });
+}
+
+azk_status azk_circle_fold_plan_clear(azk_circle_fold_plan* p) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_qm31_fold_plan_clear(p->fold));
+  });
+}
+
+void azk_circle_fold_plan_destroy(azk_circle_fold_plan* p) { delete p; }
+
+// ---- CircleFRIFoldChainPlan (:132-280): explicit challenges ----
+azk_status azk_circle_fold_chain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t rounds, azk_circle_fold_chain_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && log_size >= 1 && log_size <= 26 && rounds >= 1 && rounds <= log_size);
+    auto p = std::make_unique<azk_circle_fold_chain_plan>();
+    p->ctx = ctx;
+    forward(ctx, azk_domain_plan_create(ctx, log_size, 0, 0, rounds, &p->dom));
+    forward(ctx, azk_fold_chain_plan_create(ctx, 1ull << log_size, rounds, &p->chain));
+    *out = p.release();
+  });
+}
+
+azk_status azk_circle_fold_chain_plan_execute(azk_circle_fold_chain_plan* p, const uint32_t* evaluations, const uint32_t* challenges, uint32_t* final_out,
+                                              azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && evaluations && challenges && final_out);
+    azk_fold_chain_plan* c = p->chain;
+    check_canonical_host(evaluations, 4 * c->n_in);
+    check_canonical_host(challenges, 4ull * c->rounds);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    AZK_CU(cudaMemcpyAsync(c->ev.p, evaluations, kQ * c->n_in, cudaMemcpyHostToDevice, c->s));
+    azk_stats inner{};
+    forward(p->ctx, azk_fold_chain_plan_execute_resident(c, c->ev.p, 0, p->dom->inv.p, 0, c->out.p, 0, challenges, &inner));
+    AZK_CU(cudaMemcpyAsync(final_out, c->out.p, kQ * c->n_out, cudaMemcpyDeviceToHost, c->s));
+    sync_stream(c->s);
+    fill_stats(st, t, 0, inner.gpu_s);
+  });
+}
+
+azk_status azk_circle_fold_chain_plan_execute_resident(azk_circle_fold_chain_plan* p, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                       void* dev_final, uint64_t final_offset, const uint32_t* challenges, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    std::lock_guard<std::mutex> lk(p->mu);
+    forward(p->ctx, azk_fold_chain_plan_execute_resident(p->chain, dev_evaluations, evaluations_offset, p->dom->inv.p, 0, dev_final, final_offset,
+                                                         challenges, st));
+  });
+}
+
+azk_status azk_circle_fold_chain_plan_read_inverse_layers(azk_circle_fold_chain_plan* p, uint32_t* out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_domain_plan_read_inverse_layers(p->dom, out));
+  });
+}
+
+azk_status azk_circle_fold_chain_plan_clear(azk_circle_fold_chain_plan* p) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_fold_chain_plan_clear(p->chain));
+  });
+}
+
+void azk_circle_fold_chain_plan_destroy(azk_circle_fold_chain_plan* p) { delete p; }
+
+// ---- CircleFRIMerkleTranscriptFoldChainPlan (:301-518): Circle PCS V1 frames ----
+azk_status azk_circle_merkle_chain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,
+                                               const uint8_t public_digest[32], uint32_t rounds, azk_circle_merkle_chain_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out && public_digest);
+    // init preconditions (:344-350) and CircleFRISecurityParametersV1 (CircleProofFormat.swift:136-151)
+    layout(log_size >= 1 && log_size <= 26 && rounds >= 1 && rounds <= log_size);
+    layout(log_blowup > 0 && queries > 0 && grinding_bits <= 20 && (uint64_t)log_blowup * queries + grinding_bits <= 0xFFFFFFFFull);
+    auto p = std::make_unique<azk_circle_merkle_chain_plan>();
+    p->ctx = ctx;
+    forward(ctx, azk_domain_plan_create(ctx, log_size, 0, 0, rounds, &p->dom));
+    forward(ctx, azk_fold_chain_plan_create(ctx, 1ull << log_size, rounds, &p->chain));
+    azk_fold_chain_plan* c = p->chain;
+    // the prefix frames come from a PCS instance record: log size, security
+    // parameters, public digest and the transcript they are absorbed into
+    PcsInstance I{};
+    I.logn = log_size;
+    I.rounds = rounds;
+    I.queries = queries;
+    I.log_blowup = log_blowup;
+    I.grinding_bits = grinding_bits;
+    std::memcpy(I.pub, public_digest, 32);
+    I.transcript = c->tr.as<Transcript>();
+    c->pcs.alloc(sizeof(PcsInstance), "CircleFRIMerkleChain.Instance");
+    AZK_CU(cudaMemcpyAsync(c->pcs.p, &I, sizeof(PcsInstance), cudaMemcpyHostToDevice, c->s));
+    sync_stream(c->s);
+    c->root_kind = kRootCircleRound;
+    for (auto& j : c->tree_jobs) j.root_action = kRootCircleRound;
+    *out = p.release();
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_info(azk_circle_merkle_chain_plan* p, uint64_t* output_count, uint64_t* committed_layer_count) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    if (output_count) *output_count = p->chain->n_out;
+    if (committed_layer_count) *committed_layer_count = p->chain->layer_log;
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_execute(azk_circle_merkle_chain_plan* p, const uint32_t* evaluations, uint32_t* final_out,
+                                                uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && evaluations && final_out);
+    azk_fold_chain_plan* c = p->chain;
+    check_canonical_host(evaluations, 4 * c->n_in);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    AZK_CU(cudaMemcpyAsync(c->ev.p, evaluations, kQ * c->n_in, cudaMemcpyHostToDevice, c->s));
+    azk_stats inner{};
+    forward(p->ctx, azk_fold_chain_plan_execute_merkle_readback(c, c->ev.p, 0, p->dom->inv.p, 0, final_out, commitments_out, challenges_out, &inner));
+    fill_stats(st, t, 0, inner.gpu_s);
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_execute_resident(azk_circle_merkle_chain_plan* p, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                         void* dev_committed_layers, uint64_t committed_layers_offset, void* dev_commitments,
+                                                         uint64_t commitments_offset, uint64_t commitment_stride, const void* dev_first_commitment,
+                                                         uint64_t first_commitment_offset, void* dev_final, uint64_t final_offset, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    std::lock_guard<std::mutex> lk(p->mu);
+    forward(p->ctx, azk_fold_chain_plan_execute_merkle_resident(p->chain, dev_evaluations, evaluations_offset, p->dom->inv.p, 0, dev_commitments,
+                                                                commitments_offset, commitment_stride, dev_committed_layers, committed_layers_offset,
+                                                                dev_first_commitment, first_commitment_offset, dev_final, final_offset, st));
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_challenges(azk_circle_merkle_chain_plan* p, uint32_t* challenges_out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_fold_chain_plan_challenges(p->chain, challenges_out));
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_read_inverse_layers(azk_circle_merkle_chain_plan* p, uint32_t* out) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_domain_plan_read_inverse_layers(p->dom, out));
+  });
+}
+
+azk_status azk_circle_merkle_chain_plan_clear(azk_circle_merkle_chain_plan* p) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p != nullptr);
+    forward(p->ctx, azk_fold_chain_plan_clear(p->chain));
+  });
+}
+
+void azk_circle_merkle_chain_plan_destroy(azk_circle_merkle_chain_plan* p) { delete p; }
 
 }  // extern "C"

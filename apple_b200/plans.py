@@ -500,6 +500,188 @@ class QM31FRIFoldChainPlan(_Plan):
         self._check(lib().azk_fold_chain_plan_clear(self._h))
 
 
+class CircleDomainMaterializationPlan(_Plan):
+    """CircleDomainMaterializationPlan (CircleDomainMaterializationPlan.swift:52-219):
+    domain points, FFT twiddles and QM31 inverse-domain layers built once on the
+    device, with their device addresses and read-back accessors."""
+
+    _destroy = "azk_domain_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int, materialize_points: bool = False, materialize_twiddles: bool = False,
+                 inverse_round_count: int = 0):
+        super().__init__(ctx)
+        self.log_size, self.inverse_round_count = log_size, inverse_round_count
+        self._check(lib().azk_domain_plan_create(ctx.handle, log_size, int(materialize_points), int(materialize_twiddles), inverse_round_count,
+                                                 ctypes.byref(self._h)))
+        tw, inv, out = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.materialization_stats = Stats()
+        self._check(lib().azk_domain_plan_info(self._h, ctypes.byref(tw), ctypes.byref(inv), ctypes.byref(out), ctypes.byref(self.materialization_stats)))
+        self.codeword_twiddle_count, self.total_inverse_domain_count, self.output_count = tw.value, inv.value, out.value
+        self.inverse_domain_layer_counts = [(1 << log_size) >> (k + 1) for k in range(inverse_round_count)]
+
+    def buffers(self):
+        """(points, twiddles, inverse layers) device addresses; None where not built."""
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        self._check(lib().azk_domain_plan_buffers(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def read_domain_points(self) -> np.ndarray:
+        out = np.empty((1 << self.log_size, 2), np.uint32)
+        self._check(lib().azk_domain_plan_read_points(self._h, _ptr(out)))
+        return out
+
+    def read_codeword_twiddles(self) -> np.ndarray:
+        out = np.empty(self.codeword_twiddle_count, np.uint32)
+        self._check(lib().azk_domain_plan_read_twiddles(self._h, _ptr(out)))
+        return out
+
+    def read_inverse_domain_layers(self):
+        flat = np.empty((max(1, self.total_inverse_domain_count), 4), np.uint32)
+        self._check(lib().azk_domain_plan_read_inverse_layers(self._h, _ptr(flat)))
+        out, off = [], 0
+        for c in self.inverse_domain_layer_counts:
+            out.append(flat[off:off + c])
+            off += c
+        return out
+
+
+class CircleFRIFoldPlan(_Plan):
+    """CircleFRIFoldPlan (CircleFRIFoldPlan.swift:5-130): the circle -> line fold of
+    a canonical domain's evaluations, inverse y twiddles materialised by the plan."""
+
+    _destroy = "azk_circle_fold_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int):
+        super().__init__(ctx)
+        self.log_size, self.input_count, self.output_count = log_size, 1 << log_size, 1 << (log_size - 1)
+        self._check(lib().azk_circle_fold_plan_create(ctx.handle, log_size, ctypes.byref(self._h)))
+
+    def execute(self, evaluations, challenge) -> np.ndarray:
+        ev, ch = _q(evaluations), _q(challenge)
+        if len(ev) != self.input_count or len(ch) != 1:
+            raise AZKError(1, "evaluations must cover the domain; one challenge")
+        out = np.empty((self.output_count, 4), np.uint32)
+        self._check(lib().azk_circle_fold_plan_execute(self._h, _ptr(ev), _ptr(ch), _ptr(out), ctypes.byref(self.last_stats)))
+        return out
+
+    def execute_resident(self, dev_evaluations, dev_out, challenge, evaluations_offset=0, out_offset=0) -> Stats:
+        ch = _q(challenge)
+        st = Stats()
+        self._check(lib().azk_circle_fold_plan_execute_resident(self._h, dev_evaluations, evaluations_offset, dev_out, out_offset, _ptr(ch),
+                                                                ctypes.byref(st)))
+        return st
+
+    def read_inverse_y_twiddles(self) -> np.ndarray:
+        out = np.empty((self.output_count, 4), np.uint32)
+        self._check(lib().azk_circle_fold_plan_read_inverse(self._h, _ptr(out)))
+        return out
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_circle_fold_plan_clear(self._h))
+
+
+class CircleFRIFoldChainPlan(_Plan):
+    """CircleFRIFoldChainPlan (CircleFRIFoldPlan.swift:132-280): `round_count` folds of
+    a canonical domain's evaluations with explicit challenges."""
+
+    _destroy = "azk_circle_fold_chain_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int, round_count: int):
+        super().__init__(ctx)
+        self.log_size, self.round_count = log_size, round_count
+        self.input_count, self.output_count = 1 << log_size, (1 << log_size) >> round_count
+        self._check(lib().azk_circle_fold_chain_plan_create(ctx.handle, log_size, round_count, ctypes.byref(self._h)))
+
+    def execute(self, evaluations, challenges) -> np.ndarray:
+        ev, ch = _q(evaluations), _q(challenges)
+        if len(ev) != self.input_count or len(ch) != self.round_count:
+            raise AZKError(1, "evaluations must cover the domain; one challenge per round")
+        out = np.empty((self.output_count, 4), np.uint32)
+        self._check(lib().azk_circle_fold_chain_plan_execute(self._h, _ptr(ev), _ptr(ch), _ptr(out), ctypes.byref(self.last_stats)))
+        return out
+
+    def execute_resident(self, dev_evaluations, dev_final, challenges, evaluations_offset=0, final_offset=0) -> Stats:
+        ch = _q(challenges)
+        st = Stats()
+        self._check(lib().azk_circle_fold_chain_plan_execute_resident(self._h, dev_evaluations, evaluations_offset, dev_final, final_offset, _ptr(ch),
+                                                                      ctypes.byref(st)))
+        return st
+
+    def read_inverse_domain_layers(self):
+        flat = np.empty(((1 << self.log_size) - self.output_count, 4), np.uint32)
+        self._check(lib().azk_circle_fold_chain_plan_read_inverse_layers(self._h, _ptr(flat)))
+        out, off = [], 0
+        for k in range(self.round_count):
+            c = (1 << self.log_size) >> (k + 1)
+            out.append(flat[off:off + c])
+            off += c
+        return out
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_circle_fold_chain_plan_clear(self._h))
+
+
+class CircleFRIMerkleTranscriptFoldChainPlan(_Plan):
+    """CircleFRIMerkleTranscriptFoldChainPlan (CircleFRIFoldPlan.swift:301-518): every
+    round's layer committed as a SHA3 Merkle tree and its challenge drawn from the
+    Circle PCS V1 transcript (domain, security parameters, public digest)."""
+
+    _destroy = "azk_circle_merkle_chain_plan_destroy"
+
+    def __init__(self, ctx: Context, log_size: int, log_blowup: int, queries: int, public_digest: bytes, round_count: int, grinding_bits: int = 0):
+        super().__init__(ctx)
+        if len(public_digest) != 32:
+            raise AZKError(1, "the public-input digest is 32 bytes")
+        self.log_size, self.round_count, self.input_count = log_size, round_count, 1 << log_size
+        pub = _u8(public_digest)
+        self._check(lib().azk_circle_merkle_chain_plan_create(ctx.handle, log_size, log_blowup, queries, grinding_bits, _ptr(pub), round_count,
+                                                              ctypes.byref(self._h)))
+        o, l = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().azk_circle_merkle_chain_plan_info(self._h, ctypes.byref(o), ctypes.byref(l)))
+        self.output_count, self.total_committed_layer_count = o.value, l.value
+        self.committed_layer_counts = [(1 << log_size) >> k for k in range(round_count)]
+
+    def execute(self, evaluations):
+        """Returns (final layer, commitments, challenges)."""
+        ev = _q(evaluations)
+        if len(ev) != self.input_count:
+            raise AZKError(1, "evaluations must cover the domain")
+        out = np.empty((self.output_count, 4), np.uint32)
+        cm = np.empty(32 * self.round_count, np.uint8)
+        ch = np.empty((self.round_count, 4), np.uint32)
+        self._check(lib().azk_circle_merkle_chain_plan_execute(self._h, _ptr(ev), _ptr(out), _ptr(cm), _ptr(ch), ctypes.byref(self.last_stats)))
+        return out, [cm[32 * k:32 * k + 32].tobytes() for k in range(self.round_count)], ch
+
+    def execute_resident(self, dev_evaluations, dev_commitments, dev_final, dev_committed_layers=None, dev_first_commitment=None, commitment_stride=32,
+                         evaluations_offset=0, committed_layers_offset=0, commitments_offset=0, first_commitment_offset=0, final_offset=0) -> Stats:
+        """executeResident, executeMaterializedResident (with `dev_committed_layers`) and
+        ...WithPrecomputedFirstCommitment (with `dev_first_commitment` as well)."""
+        st = Stats()
+        self._check(lib().azk_circle_merkle_chain_plan_execute_resident(self._h, dev_evaluations, evaluations_offset, dev_committed_layers,
+                                                                        committed_layers_offset, dev_commitments, commitments_offset, commitment_stride,
+                                                                        dev_first_commitment, first_commitment_offset, dev_final, final_offset,
+                                                                        ctypes.byref(st)))
+        return st
+
+    def challenges(self) -> np.ndarray:
+        ch = np.empty((self.round_count, 4), np.uint32)
+        self._check(lib().azk_circle_merkle_chain_plan_challenges(self._h, _ptr(ch)))
+        return ch
+
+    def read_inverse_domain_layers(self):
+        flat = np.empty(((1 << self.log_size) - self.output_count, 4), np.uint32)
+        self._check(lib().azk_circle_merkle_chain_plan_read_inverse_layers(self._h, _ptr(flat)))
+        out, off = [], 0
+        for k in range(self.round_count):
+            c = (1 << self.log_size) >> (k + 1)
+            out.append(flat[off:off + c])
+            off += c
+        return out
+
+    def clear_reusable_buffers(self):
+        self._check(lib().azk_circle_merkle_chain_plan_clear(self._h))
+
+
 class CircleFRIResidentQueryExtractor(_Plan):
     """CircleFRIResidentQueryExtractorV1 (CircleFRIFoldPlan.swift:1027-1231): query
     openings from committed layers on the device, in the proof codec's encoding."""

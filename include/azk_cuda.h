@@ -144,6 +144,27 @@ azk_status azk_merkle_root_noalloc(const void* dev_leaves, uint64_t leaf_count, 
 azk_status azk_circle_domain_points(azk_ctx* ctx, uint32_t log_size, uint32_t* xy_out);
 azk_status azk_circle_fft_twiddles(azk_ctx* ctx, uint32_t log_size, uint32_t* out);
 azk_status azk_circle_inverse_layers(azk_ctx* ctx, uint32_t log_size, uint32_t rounds, uint32_t* out);
+/* Plan form (CircleDomainMaterializationPlan.init, :52-133): the tables are built
+ * once on the device and stay there.  At least one of points, twiddles or
+ * inverse_rounds (<= log_size) is asked for.  Inverse layers are QM31 values
+ * (a, 0, 0, 0), 16 bytes each, layer k (N >> (k+1) values) after layers 0..k-1. */
+typedef struct azk_domain_plan azk_domain_plan;
+azk_status azk_domain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t materialize_points, uint32_t materialize_twiddles,
+                                  uint32_t inverse_rounds, azk_domain_plan** out);
+/* Counts (N - 1 twiddles, inverse values, values left after the rounds) and the
+ * materialisation's timing (materializationStats). */
+azk_status azk_domain_plan_info(azk_domain_plan* plan, uint64_t* twiddle_count, uint64_t* inverse_count, uint64_t* output_count,
+                                azk_stats* materialization);
+/* Device addresses of the tables, NULL for one not materialised
+ * (requireDomainPointBuffer / ...TwiddleBuffer / ...InverseDomainBuffer, :135-154). */
+azk_status azk_domain_plan_buffers(azk_domain_plan* plan, const void** points, const void** twiddles, const void** inverse_layers);
+/* readDomainPoints (2N words, (x, y) per point in storage order), readCodewordTwiddles,
+ * readInverseDomainLayers (:156-219); a table the plan did not build is
+ * AZK_ERR_INVALID_INPUT_LAYOUT. */
+azk_status azk_domain_plan_read_points(azk_domain_plan* plan, uint32_t* xy_out);
+azk_status azk_domain_plan_read_twiddles(azk_domain_plan* plan, uint32_t* out);
+azk_status azk_domain_plan_read_inverse_layers(azk_domain_plan* plan, uint32_t* out);
+void azk_domain_plan_destroy(azk_domain_plan* plan);
 
 /* ---- Circle FFT codeword (CircleCodeword.swift:411-887) ----
  * Input: N interleaved FFT-basis coefficients [x0, y0, x1, y1, ...] (QM31),
@@ -263,6 +284,62 @@ uint64_t azk_query_extractor_query_bytes(uint32_t log_size, uint32_t rounds);
 azk_status azk_query_extractor_extract(azk_query_extractor* extractor, const void* dev_layers, uint64_t layers_offset, const uint8_t* commitments,
                                        const uint64_t* pair_indices, uint64_t count, uint8_t* queries_out, uint64_t* out_len, azk_stats* stats);
 void azk_query_extractor_destroy(azk_query_extractor* extractor);
+
+/* ---- Circle FRI fold plans (CircleFRIFoldPlan.swift:5-518) ----
+ * The canonical domain of size 2^log_size supplies the inverse-domain layers
+ * (materialised once per plan); folds run through the QM31 fold plans above, with
+ * the same resident range and aliasing rules.  Evaluations are N QM31 values. */
+
+/* CircleFRIFoldPlan (:5-130): one circle -> line fold (N -> N/2). */
+typedef struct azk_circle_fold_plan azk_circle_fold_plan;
+azk_status azk_circle_fold_plan_create(azk_ctx* ctx, uint32_t log_size, azk_circle_fold_plan** out);
+azk_status azk_circle_fold_plan_execute(azk_circle_fold_plan* plan, const uint32_t* evaluations, const uint32_t challenge[4], uint32_t* out,
+                                        azk_stats* stats);
+azk_status azk_circle_fold_plan_execute_resident(azk_circle_fold_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset, void* dev_out,
+                                                 uint64_t out_offset, const uint32_t challenge[4], azk_stats* stats);
+/* readInverseYTwiddles (:108-110): N/2 QM31 values. */
+azk_status azk_circle_fold_plan_read_inverse(azk_circle_fold_plan* plan, uint32_t* out);
+azk_status azk_circle_fold_plan_clear(azk_circle_fold_plan* plan);
+void azk_circle_fold_plan_destroy(azk_circle_fold_plan* plan);
+
+/* CircleFRIFoldChainPlan (:132-280): `rounds` folds with explicit challenges
+ * (round 0 circle -> line, then line -> line). */
+typedef struct azk_circle_fold_chain_plan azk_circle_fold_chain_plan;
+azk_status azk_circle_fold_chain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t rounds, azk_circle_fold_chain_plan** out);
+azk_status azk_circle_fold_chain_plan_execute(azk_circle_fold_chain_plan* plan, const uint32_t* evaluations, const uint32_t* challenges,
+                                              uint32_t* final_out, azk_stats* stats);
+azk_status azk_circle_fold_chain_plan_execute_resident(azk_circle_fold_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                       void* dev_final, uint64_t final_offset, const uint32_t* challenges, azk_stats* stats);
+azk_status azk_circle_fold_chain_plan_read_inverse_layers(azk_circle_fold_chain_plan* plan, uint32_t* out);
+azk_status azk_circle_fold_chain_plan_clear(azk_circle_fold_chain_plan* plan);
+void azk_circle_fold_chain_plan_destroy(azk_circle_fold_chain_plan* plan);
+
+/* CircleFRIMerkleTranscriptFoldChainPlan (:301-518): each round's layer is
+ * committed as a SHA3 Merkle tree of 16-byte leaves and its challenge drawn from
+ * the Circle PCS V1 transcript (header, domain, security parameters, public digest,
+ * then commitment and challenge frames per round). */
+typedef struct azk_circle_merkle_chain_plan azk_circle_merkle_chain_plan;
+azk_status azk_circle_merkle_chain_plan_create(azk_ctx* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t grinding_bits,
+                                               const uint8_t public_digest[32], uint32_t rounds, azk_circle_merkle_chain_plan** out);
+/* outputCount and totalCommittedLayerCount (the committed-layer log: the input
+ * layers of rounds 0..R-1, concatenated). */
+azk_status azk_circle_merkle_chain_plan_info(azk_circle_merkle_chain_plan* plan, uint64_t* output_count, uint64_t* committed_layer_count);
+/* execute (:391-409): final layer, 32-byte commitments and challenges read back. */
+azk_status azk_circle_merkle_chain_plan_execute(azk_circle_merkle_chain_plan* plan, const uint32_t* evaluations, uint32_t* final_out,
+                                                uint8_t* commitments_out, uint32_t* challenges_out, azk_stats* stats);
+/* executeResident (dev_committed_layers NULL), executeMaterializedResident
+ * (committed layers written there) and ...WithPrecomputedFirstCommitment
+ * (dev_first_commitment: round 0's 32-byte root, which then needs the committed
+ * layer buffer) (:434-510). */
+azk_status azk_circle_merkle_chain_plan_execute_resident(azk_circle_merkle_chain_plan* plan, const void* dev_evaluations, uint64_t evaluations_offset,
+                                                         void* dev_committed_layers, uint64_t committed_layers_offset, void* dev_commitments,
+                                                         uint64_t commitments_offset, uint64_t commitment_stride, const void* dev_first_commitment,
+                                                         uint64_t first_commitment_offset, void* dev_final, uint64_t final_offset, azk_stats* stats);
+/* Challenges of the last execution (4 limbs per round). */
+azk_status azk_circle_merkle_chain_plan_challenges(azk_circle_merkle_chain_plan* plan, uint32_t* challenges_out);
+azk_status azk_circle_merkle_chain_plan_read_inverse_layers(azk_circle_merkle_chain_plan* plan, uint32_t* out);
+azk_status azk_circle_merkle_chain_plan_clear(azk_circle_merkle_chain_plan* plan);
+void azk_circle_merkle_chain_plan_destroy(azk_circle_merkle_chain_plan* plan);
 
 /* Sustained LOP3 + SHF (funnel shift) issue rate of the device, 32-bit ops per
  * second, from a probe kernel of independent chains: the integer roofline of
