@@ -41,6 +41,7 @@ from .plans import (  # noqa: E402,F401
     QM31FRIFoldChainPlan,
     QM31FRIFoldPlan,
     SHA3FixedOneBlockHashPlan,
+    SHA3PrehashedLeavesMerkleCommitPlan,
     SHA3RawLeavesMerkleCommitPlan,
     circle_domain_points,
     circle_fft_twiddles,

@@ -134,6 +134,10 @@ PROTOTYPES = {
     "azk_query_extractor_query_bytes": (U64, [U32, U32]),
     "azk_query_extractor_extract": (I32, [P, P, U64, P, P, U64, P, U64P, STATS]),
     "azk_query_extractor_destroy": (None, [P]),
+    "azk_merkle_prehashed_plan_create": (I32, [P, U64, PP]),
+    "azk_merkle_prehashed_plan_commit": (I32, [P, P, P, STATS]),
+    "azk_merkle_prehashed_plan_commit_resident": (I32, [P, P, U64, P, STATS]),
+    "azk_merkle_prehashed_plan_destroy": (None, [P]),
     "azk_domain_plan_create": (I32, [P, U32, U32, U32, U32, PP]),
     "azk_domain_plan_info": (I32, [P, U64P, U64P, U64P, STATS]),
     "azk_domain_plan_buffers": (I32, [P, PP, PP, PP]),

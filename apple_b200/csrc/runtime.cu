@@ -395,6 +395,19 @@ struct azk_merkle_plan {
   }
 };
 
+struct azk_merkle_prehashed_plan {
+  azk_ctx* ctx;
+  std::mutex mu;
+  cudaStream_t s = nullptr;
+  uint64_t count;
+  uint32_t logn, tile_log;
+  DevBuf staging, inner, counters, job, work, root;
+  TreeJob h_job{};
+  ~azk_merkle_prehashed_plan() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
 struct azk_codeword_plan {
   azk_ctx* ctx;
   std::mutex mu;
@@ -738,6 +751,83 @@ azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* digests, uint64
     fill_stats(st, t, 0, g.seconds());
   });
 }
+
+// ---- SHA3PrehashedLeavesMerkleCommitPlan (MerkleCommitter.swift:314-524) ----
+azk_status azk_merkle_prehashed_plan_create(azk_ctx* ctx, uint64_t leaf_count, azk_merkle_prehashed_plan** out) {
+  return guarded(ctx, [&] {
+    layout(ctx && out);
+    // init (:330-334): a non-zero power of two that fits 32 bits
+    require(is_pow2(leaf_count), AZK_ERR_INVALID_LEAF_COUNT, "Leaf count must be a non-zero power of two, got " + std::to_string(leaf_count) + ".");
+    layout(leaf_count <= 0xFFFFFFFFull);
+    AZK_CU(cudaSetDevice(ctx->device));
+    auto p = std::make_unique<azk_merkle_prehashed_plan>();
+    p->ctx = ctx;
+    p->count = leaf_count;
+    p->logn = ilog2(leaf_count);
+    p->tile_log = std::min<uint32_t>(10, p->logn);
+    if (p->tile_log == 0 && p->logn) p->tile_log = 1;
+    p->s = new_stream();
+    p->staging.alloc(32 * leaf_count, "Merkle.PrehashedPlanLeaves");
+    p->inner.alloc((leaf_count > 1 ? leaf_count - 1 : 1) * 32, "Merkle.PrehashedPlanInner");
+    p->counters.alloc(tree_counter_count(p->logn, p->tile_log) * 4, "Merkle.PrehashedPlanCounters");
+    p->root.alloc(32, "Merkle.PrehashedPlanRoot");
+    p->job.alloc(sizeof(TreeJob), "Merkle.PrehashedPlanJob");
+    const uint64_t tiles = 1ull << (p->logn - p->tile_log);
+    std::vector<uint2> w(tiles);
+    for (uint64_t i = 0; i < tiles; i++) w[i] = make_uint2(0, (uint32_t)i);
+    p->work.alloc(tiles * sizeof(uint2), "Merkle.PrehashedPlanWork");
+    TreeJob& j = p->h_job;
+    j.logn = p->logn;
+    j.kind = kLeafDigest;
+    j.tile_log = p->tile_log;
+    j.group_log = p->tile_log ? p->tile_log : 1;
+    j.inner = p->inner.as<uint64_t>();
+    j.counters = p->counters.as<uint32_t>();
+    j.root_out = p->root.as<uint64_t>();
+    AZK_CU(cudaMemsetAsync(p->counters.p, 0, p->counters.bytes, p->s));
+    AZK_CU(cudaMemcpyAsync(p->work.p, w.data(), tiles * sizeof(uint2), cudaMemcpyHostToDevice, p->s));
+    sync_stream(p->s);
+    *out = p.release();
+  });
+}
+
+static void prehashed_commit(azk_merkle_prehashed_plan* p, const uint8_t* leaves, uint8_t root[32], azk_stats* st, const Timer& t) {
+  p->h_job.raw = leaves;
+  AZK_CU(cudaMemcpyAsync(p->job.p, &p->h_job, sizeof(TreeJob), cudaMemcpyHostToDevice, p->s));
+  GpuTimer g(p->s);
+  AZK_CU(launch_tree_jobs(p->job.as<TreeJob>(), p->work.as<uint2>(), (uint32_t)(1ull << (p->logn - p->tile_log)), p->tile_log, kLeafDigest, 256, p->s));
+  g.stop();
+  AZK_CU(cudaMemcpyAsync(root, p->root.p, 32, cudaMemcpyDeviceToHost, p->s));
+  sync_stream(p->s);
+  fill_stats(st, t, 0, g.seconds());
+}
+
+azk_status azk_merkle_prehashed_plan_commit(azk_merkle_prehashed_plan* p, const void* host_digests, uint8_t root_out[32], azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && host_digests && root_out);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    AZK_CU(cudaMemcpyAsync(p->staging.p, host_digests, 32 * p->count, cudaMemcpyHostToDevice, p->s));
+    prehashed_commit(p, p->staging.as<uint8_t>(), root_out, st, t);
+  });
+}
+
+azk_status azk_merkle_prehashed_plan_commit_resident(azk_merkle_prehashed_plan* p, const void* dev_digests, uint64_t offset, uint8_t root_out[32],
+                                                     azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && root_out);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    require_device_range(dev_digests, offset, 32 * p->count);
+    // the digests are read as 16-byte vectors
+    layout((reinterpret_cast<uintptr_t>(dev_digests) + offset) % 16 == 0, "resident digests must start on a 16-byte boundary");
+    Timer t;
+    prehashed_commit(p, static_cast<const uint8_t*>(dev_digests) + offset, root_out, st, t);
+  });
+}
+
+void azk_merkle_prehashed_plan_destroy(azk_merkle_prehashed_plan* p) { delete p; }
 
 // ---- circle domain ----
 azk_status azk_circle_domain_points(azk_ctx* ctx, uint32_t logn, uint32_t* xy) {

@@ -500,6 +500,31 @@ class QM31FRIFoldChainPlan(_Plan):
         self._check(lib().azk_fold_chain_plan_clear(self._h))
 
 
+class SHA3PrehashedLeavesMerkleCommitPlan(_Plan):
+    """SHA3PrehashedLeavesMerkleCommitPlan (MerkleCommitter.swift:314-524): the Merkle
+    root over `leaf_count` 32-byte leaf digests."""
+
+    _destroy = "azk_merkle_prehashed_plan_destroy"
+
+    def __init__(self, ctx: Context, leaf_count: int):
+        super().__init__(ctx)
+        self.leaf_count = leaf_count
+        self._check(lib().azk_merkle_prehashed_plan_create(ctx.handle, leaf_count, ctypes.byref(self._h)))
+
+    def commit(self, digests) -> bytes:
+        d = _u8(digests)
+        if d.nbytes != 32 * self.leaf_count:
+            raise AZKError(1, "32 bytes per leaf digest")
+        root = np.empty(32, np.uint8)
+        self._check(lib().azk_merkle_prehashed_plan_commit(self._h, _ptr(d), _ptr(root), ctypes.byref(self.last_stats)))
+        return root.tobytes()
+
+    def commit_resident(self, dev_digests, offset: int = 0) -> bytes:
+        root = np.empty(32, np.uint8)
+        self._check(lib().azk_merkle_prehashed_plan_commit_resident(self._h, dev_digests, offset, _ptr(root), ctypes.byref(self.last_stats)))
+        return root.tobytes()
+
+
 class CircleDomainMaterializationPlan(_Plan):
     """CircleDomainMaterializationPlan (CircleDomainMaterializationPlan.swift:52-219):
     domain points, FFT twiddles and QM31 inverse-domain layers built once on the

@@ -118,6 +118,16 @@ void azk_merkle_plan_destroy(azk_merkle_plan* plan);
 /* Root over 32-byte prehashed leaves (SHA3MerkleCommitter.commitPrehashedLeaves, :225-304;
  * SHA3PrehashedLeavesMerkleCommitPlan, :314-524). */
 azk_status azk_merkle_commit_prehashed(azk_ctx* ctx, const void* host_digests, uint64_t digest_bytes, uint8_t root_out[32], azk_stats* stats);
+/* SHA3PrehashedLeavesMerkleCommitPlan (MerkleCommitter.swift:314-524): the root over
+ * `leaf_count` (a power of two) 32-byte digests, from host memory or resident at a
+ * byte offset in device memory (commit(leafHashBuffer:leafHashOffset:), :358-398);
+ * resident digests start on a 16-byte boundary. */
+typedef struct azk_merkle_prehashed_plan azk_merkle_prehashed_plan;
+azk_status azk_merkle_prehashed_plan_create(azk_ctx* ctx, uint64_t leaf_count, azk_merkle_prehashed_plan** out);
+azk_status azk_merkle_prehashed_plan_commit(azk_merkle_prehashed_plan* plan, const void* host_digests, uint8_t root_out[32], azk_stats* stats);
+azk_status azk_merkle_prehashed_plan_commit_resident(azk_merkle_prehashed_plan* plan, const void* dev_digests, uint64_t offset, uint8_t root_out[32],
+                                                     azk_stats* stats);
+void azk_merkle_prehashed_plan_destroy(azk_merkle_prehashed_plan* plan);
 
 /* Merkle root of raw leaves with no device allocation: no counterpart in the
  * reference.  For callers that may not call cudaMalloc (a host that gives the

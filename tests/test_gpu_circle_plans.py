@@ -132,3 +132,27 @@ def test_circle_merkle_chain_plan(ctx, oracle, log_size, rounds, queries):
     plan.execute_resident(d_ev.ptr, d_cm.ptr, d_fin3.ptr, dev_committed_layers=d_log.ptr, dev_first_commitment=d_first.ptr, commitment_stride=stride)
     assert np.array_equal(_q_from(d_fin3, plan.output_count), fin)
     assert np.array_equal(plan.challenges(), ch)
+
+
+@pytest.mark.parametrize("log_count", [0, 1, 5, 12, 17])
+def test_prehashed_merkle_plan(ctx, oracle, log_count):
+    """SHA3PrehashedLeavesMerkleCommitPlan: host and resident commits equal the
+    oracle's prehashed root; a misaligned or out-of-range resident buffer and a
+    count that is not a power of two are rejected."""
+    rng = np.random.default_rng(300 + log_count)
+    n = 1 << log_count
+    dig = rng.integers(0, 256, 32 * n, dtype=np.uint8).tobytes()
+    want = oracle.merkle_root_prehashed(dig)
+    plan = azk.SHA3PrehashedLeavesMerkleCommitPlan(ctx, n)
+    assert plan.commit(dig) == want
+    buf = ctx.alloc(32 * n + 64)
+    buf.upload(np.frombuffer(dig, np.uint8), 64)
+    assert plan.commit_resident(buf.ptr, 64) == want
+    assert plan.commit_resident(buf.ptr, 64) == want  # counters reset themselves
+    for off in (8, 96):
+        with pytest.raises(azk.AZKError) as e:
+            plan.commit_resident(buf.ptr, off)
+        assert e.value.name == "invalidInputLayout"
+    with pytest.raises(azk.AZKError) as e:
+        azk.SHA3PrehashedLeavesMerkleCommitPlan(ctx, 3)
+    assert e.value.name == "invalidLeafCount"
