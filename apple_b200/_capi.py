@@ -170,6 +170,8 @@ PROTOTYPES = {
     "azk_pcs_prover_prove_evaluations": (I32, [P, P, P, P, U64, P, U64P, STATS]),
     "azk_pcs_prover_prove_coefficients": (I32, [P, P, U64, P, P, U64P, STATS]),
     "azk_pcs_prover_prove_resident": (I32, [P, P, U64, I32, P, P, U64P, STATS]),
+    "azk_pcs_prover_prove_polynomial": (I32, [P, P, U64, P, U64, P, P, U64P, STATS]),
+    "azk_pcs_prover_prove_resident_witness": (I32, [P, P, U64, U64, P, U64, U64, P, P, U64P, STATS]),
     "azk_pcs_prover_trace": (I32, [P, P, P, P, P]),
     "azk_pcs_prover_destroy": (None, [P]),
     "azk_batch_create": (I32, [P, U32, P, P, U32, U32, SCHED, PP]),

@@ -573,6 +573,12 @@ struct azk_pcs_prover {
   std::mutex mu;
   Engine eng;
   uint32_t logn, rounds, queries, log_blowup, grinding;
+  // monomial columns -> FFT basis on the device (made on first use)
+  azk_witness_plan* wit = nullptr;
+  DevBuf wx, wy;  // staging for host columns
+  ~azk_pcs_prover() {
+    if (wit) azk_witness_plan_destroy(wit);
+  }
 };
 
 struct azk_batch {
@@ -678,8 +684,11 @@ azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* din, uin
     layout(p && din && pub && dproof && proof_len && in_off % 16 == 0);
     std::lock_guard<std::mutex> lk(p->mu);
     uint64_t N = 1ull << p->logn;
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    require_device_range(din, in_off, 16 * N);
     Timer t;
     pcs_ensure_claimed(p, {});
+    require_device_range(dproof, 0, std::min<uint64_t>(*proof_len, p->eng.proof_len[0]));
     Engine& e = p->eng;
     const uint8_t* src = static_cast<const uint8_t*>(din) + in_off;
     void* dst = is_coeffs ? (void*)e.arena.at<uint4>(e.off_input[0]) : (void*)e.h_inst[0].layers;
@@ -691,6 +700,66 @@ azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* din, uin
       e.check_input_canonical(dst, 4 * N);
     }
     pcs_prove_common(p, is_coeffs != 0, pub, static_cast<uint8_t*>(dproof), true, proof_len, st, t);
+  });
+}
+
+}  // extern "C"
+
+// Monomial coefficient columns (device) -> interleaved FFT-basis coefficients in
+// the engine's input, through the witness plan's kernels (the conversion the
+// reference's prove(polynomial:) runs on the CPU, CircleCodeword.swift:983-1005,
+// and proveResidentWitnessCoefficients on the GPU, :1061-1080, 1235-1280); then the
+// input scan over all N values (the line-basis step can spread nonzeros over the
+// whole coefficient range).
+static void pcs_witness_input(azk_pcs_prover* p, const void* dx, uint64_t x_off, uint64_t nx, const void* dy, uint64_t y_off, uint64_t ny) {
+  if (!p->wit) {
+    const azk_status s = azk_witness_plan_create(p->ctx, p->logn, &p->wit);
+    if (s != AZK_OK) fail(s, azk_last_error_message(p->ctx));
+  }
+  Engine& e = p->eng;
+  azk_stats ws{};
+  const azk_status s = azk_witness_plan_execute_resident(p->wit, dx, x_off, nx, dy, y_off, ny, e.arena.buf.p, e.off_input[0], &ws);
+  if (s != AZK_OK) fail(s, azk_last_error_message(p->ctx));
+  e.scan_inputs({1ull << p->logn});
+}
+
+extern "C" {
+
+azk_status azk_pcs_prover_prove_polynomial(azk_pcs_prover* p, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny, const uint8_t pub[32],
+                                           uint8_t* proof_out, uint64_t* proof_len, azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && pub && proof_out && proof_len && (x || !nx) && (y || !ny));
+    const uint64_t half = (1ull << p->logn) / 2;
+    layout(nx <= half && ny <= half, "each coefficient column holds at most half the domain size");
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    pcs_ensure_claimed(p, {});
+    if (!p->wx.p) {
+      p->wx.alloc(16 * std::max<uint64_t>(half, 1), "CirclePCSProver.WitnessX");
+      p->wy.alloc(16 * std::max<uint64_t>(half, 1), "CirclePCSProver.WitnessY");
+    }
+    Engine& e = p->eng;
+    if (nx) AZK_CU(cudaMemcpyAsync(p->wx.p, x, 16 * nx, cudaMemcpyHostToDevice, e.s));
+    if (ny) AZK_CU(cudaMemcpyAsync(p->wy.p, y, 16 * ny, cudaMemcpyHostToDevice, e.s));
+    sync_stream(e.s);
+    pcs_witness_input(p, p->wx.p, 0, nx, p->wy.p, 0, ny);
+    pcs_prove_common(p, true, pub, proof_out, false, proof_len, st, t);
+  });
+}
+
+azk_status azk_pcs_prover_prove_resident_witness(azk_pcs_prover* p, const void* dev_x, uint64_t x_offset, uint64_t nx, const void* dev_y,
+                                                 uint64_t y_offset, uint64_t ny, const uint8_t pub[32], void* dproof, uint64_t* proof_len,
+                                                 azk_stats* st) {
+  return guarded(p ? p->ctx : nullptr, [&] {
+    layout(p && pub && dproof && proof_len);
+    std::lock_guard<std::mutex> lk(p->mu);
+    AZK_CU(cudaSetDevice(p->ctx->device));
+    Timer t;
+    pcs_ensure_claimed(p, {});
+    require_device_range(dproof, 0, std::min<uint64_t>(*proof_len, p->eng.proof_len[0]));
+    pcs_witness_input(p, dev_x, x_offset, nx, dev_y, y_offset, ny);
+    pcs_prove_common(p, true, pub, static_cast<uint8_t*>(dproof), true, proof_len, st, t);
   });
 }
 

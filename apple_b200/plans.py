@@ -798,6 +798,22 @@ class CirclePCSFRIProver(_Plan):
                                                         ctypes.byref(n), ctypes.byref(self.last_stats)))
         return n.value
 
+    def prove_polynomial(self, x_coefficients, y_coefficients, public_digest: bytes) -> bytes:
+        """prove(polynomial:): monomial columns, converted to the FFT basis on the device."""
+        x, y, pub = _q(x_coefficients), _q(y_coefficients), _u8(public_digest)
+        out, n = self._buf()
+        self._check(lib().azk_pcs_prover_prove_polynomial(self._h, _ptr(x) if len(x) else None, len(x), _ptr(y) if len(y) else None, len(y),
+                                                          _ptr(pub), _ptr(out), ctypes.byref(n), ctypes.byref(self.last_stats)))
+        return out[: n.value].tobytes()
+
+    def prove_resident_witness(self, dev_x, x_count, dev_y, y_count, public_digest: bytes, dev_proof, x_offset=0, y_offset=0) -> int:
+        """proveResidentWitnessCoefficients: monomial columns already on the device."""
+        pub = _u8(public_digest)
+        n = ctypes.c_uint64(pcs_proof_size(self.log_size, self.rounds, self.queries, 0, self.grinding_bits))
+        self._check(lib().azk_pcs_prover_prove_resident_witness(self._h, dev_x, x_offset, x_count, dev_y, y_offset, y_count, _ptr(pub), dev_proof,
+                                                                ctypes.byref(n), ctypes.byref(self.last_stats)))
+        return n.value
+
     def trace(self):
         """(commitments, challenges, final layer, query pairs) of the last proof."""
         cm = np.empty(32 * self.rounds, np.uint8)

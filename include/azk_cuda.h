@@ -394,6 +394,17 @@ azk_status azk_pcs_prover_prove_coefficients(azk_pcs_prover* p, const uint32_t* 
  * input_is_coefficients, else evaluations); proof bytes written to dev_proof. */
 azk_status azk_pcs_prover_prove_resident(azk_pcs_prover* p, const void* dev_input, uint64_t in_offset, int input_is_coefficients,
                                          const uint8_t public_digest[32], void* dev_proof, uint64_t* proof_len, azk_stats* stats);
+/* From monomial coefficient columns (x: x_count QM31, y: y_count QM31, each at most
+ * N/2): converted to the FFT basis on the device by the witness kernels, then
+ * proved as above (prove(polynomial:), CircleCodeword.swift:983-1005). */
+azk_status azk_pcs_prover_prove_polynomial(azk_pcs_prover* p, const uint32_t* x_coefficients, uint64_t x_count, const uint32_t* y_coefficients,
+                                           uint64_t y_count, const uint8_t public_digest[32], uint8_t* proof_out, uint64_t* proof_len,
+                                           azk_stats* stats);
+/* The same from columns resident in device memory; proof bytes written to dev_proof
+ * (proveResidentCoefficients / proveResidentWitnessCoefficients, :1020-1080). */
+azk_status azk_pcs_prover_prove_resident_witness(azk_pcs_prover* p, const void* dev_x, uint64_t x_offset, uint64_t x_count, const void* dev_y,
+                                                 uint64_t y_offset, uint64_t y_count, const uint8_t public_digest[32], void* dev_proof,
+                                                 uint64_t* proof_len, azk_stats* stats);
 /* Public readbacks of the last proof: commitments (32 bytes each), challenges,
  * final layer and query pair indices (any pointer may be NULL). */
 azk_status azk_pcs_prover_trace(azk_pcs_prover* p, uint8_t* commitments, uint32_t* challenges, uint32_t* final_layer, uint32_t* query_pairs);

@@ -57,3 +57,28 @@ def test_witness_resident_and_rejections(ctx, oracle):
     bad[3, 2] = G.P
     with pytest.raises(azk.AZKError):
         plan.execute(bad, y)
+
+
+def test_prover_from_polynomial_golden_and_resident(ctx, oracle, golden):
+    """prove(polynomial:) and proveResidentWitnessCoefficients: the monomial columns of
+    the log-14 golden proof go through the prover's own device conversion and give
+    the reference's proof digest, from host and from resident columns."""
+    v = golden["bench_codeword_prover_log14"]
+    x, y = G.bench_codeword_polynomial(1 << 14)
+    pub = bytes(0xA0 + i for i in range(32))
+    prover = azk.CirclePCSFRIProver(ctx, 14, 2, 4, 3)
+    proof = prover.prove_polynomial(x, y, pub)
+    assert oracle.sha3_256(proof).hex() == v["proof_hex"]
+    x, y = np.asarray(x, np.uint32).reshape(-1, 4), np.asarray(y, np.uint32).reshape(-1, 4)
+    dx, dy = ctx.alloc(max(16, x.nbytes)), ctx.alloc(max(16, y.nbytes))
+    dx.upload(x)
+    dy.upload(y)
+    dproof = ctx.alloc(len(proof))
+    n = prover.prove_resident_witness(dx.ptr, len(x), dy.ptr, len(y), pub, dproof.ptr)
+    assert n == len(proof) and dproof.download(n) == proof
+    # random columns: the same proof as from the oracle's FFT-basis coefficients
+    rng = np.random.default_rng(77)
+    xs, ys = _cols(rng, 300, 211)
+    p2 = azk.CirclePCSFRIProver(ctx, 11, 1, 8, 5)
+    want = p2.prove_coefficients(oracle.fft_basis_coefficients(11, xs, ys), pub)
+    assert p2.prove_polynomial(xs, ys, pub) == want
