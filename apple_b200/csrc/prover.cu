@@ -8,12 +8,14 @@
 // still active in that round, so small instances share the GPU with large ones
 // and the whole superstep is a fixed launch sequence captured in a CUDA graph.
 // Plain form: the same kernels, launched instance after instance.
+#include <map>
 #include <memory>
 #include <algorithm>
 #include <condition_variable>
 #include <deque>
 #include <set>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 
 #include "azk_field.cuh"
@@ -70,8 +72,18 @@ struct Engine {
   std::vector<uint32_t> ids;
   DevBuf d_tree_jobs, d_tree_work, d_fold_jobs, d_fold_work, d_ids;
 
-  cudaGraphExec_t graph = nullptr;
-  bool graph_from_coeffs = false;
+  // Captured launch sequences, keyed by the FFT work-list set in use (its narrow
+  // flags), the input kind and the active-instance count (0: all).  Every FFT
+  // work-list set keeps its own device lists (`fft` in use, `fft_saved` the
+  // others), so a graph stays valid while other sets run.
+  using GraphKey = std::tuple<std::vector<uint8_t>, bool, uint32_t>;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  std::map<std::vector<uint8_t>, FftPlan> fft_saved;
+  static constexpr size_t kMaxGraphs = 64, kMaxFftSets = 16;
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+  }
 
   // Per-stage CUDA events (profiling): stage kind 0 = FFT, 1 = tree (fold +
   // hash + transcript), 2 = final fold, 3 = transcript/queries/emission.
@@ -84,7 +96,7 @@ struct Engine {
   uint32_t launches = 0;
 
   ~Engine() {
-    if (graph) cudaGraphExecDestroy(graph);
+    drop_graphs();
     for (auto e : ev_a) cudaEventDestroy(e);
     for (auto e : ev_b) cudaEventDestroy(e);
     if (owns_streams && s) cudaStreamDestroy(s);
@@ -166,17 +178,34 @@ struct Engine {
     set_fft_narrow(narrow);
   }
   // Which instances run the one-limb FFT kernel; `narrow` covers the transforms of
-  // the first narrow.size() instances (the FFT runs over those).  A change rebuilds
-  // the FFT work lists and drops the captured graph (captured again on the next run).
+  // the first narrow.size() instances (the FFT runs over those).  A set of flags
+  // seen before gets its saved work lists back (and its graphs stay valid); a new
+  // one builds lists of its own.  Past kMaxFftSets saved sets, the saved sets and
+  // every graph are dropped.
   void set_fft_narrow(const std::vector<uint8_t>& narrow) {
     if (narrow == fft_narrow) return;
     sync_stream(s);
+    auto it = fft_saved.find(narrow);
+    FftPlan next;
+    const bool saved = it != fft_saved.end();
+    if (saved) {
+      next = std::move(it->second);
+      fft_saved.erase(it);
+    }
+    fft_saved[fft_narrow] = std::move(fft);
+    if (saved) {
+      fft = std::move(next);
+    } else {
+      fft = FftPlan();
+      fft.build(std::vector<FftJob>(fft_transforms.begin(), fft_transforms.begin() + narrow.size()), narrow);
+      fft.upload(s);
+      sync_stream(s);
+    }
     fft_narrow = narrow;
-    fft.build(std::vector<FftJob>(fft_transforms.begin(), fft_transforms.begin() + narrow.size()), fft_narrow);
-    fft.upload(s);
-    sync_stream(s);
-    if (graph) cudaGraphExecDestroy(graph);
-    graph = nullptr;
+    if (fft_saved.size() > kMaxFftSets) {
+      drop_graphs();
+      fft_saved.clear();
+    }
   }
 
   // `run_stream` / `upload_stream`: streams owned by the caller (a server worker,
@@ -509,22 +538,25 @@ struct Engine {
     if (plain) {
       ev_used = 0;
       for (uint32_t i = 0; i < active(); i++) enqueue_instance(i, from_coeffs);
-    } else if (!any_grinding && sched.graph && !prof && !n_act) {
+    } else if (!any_grinding && sched.graph && !prof) {
       // (profiled runs take the eager path below: the same launch sequence, with
       // event pairs around each stage)
-      if (!graph || graph_from_coeffs != from_coeffs) {
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
+      GraphKey key{fft_narrow, from_coeffs, n_act};
+      auto it = graphs.find(key);
+      if (it == graphs.end()) {
+        if (graphs.size() >= kMaxGraphs) drop_graphs();
         cudaGraph_t gr;
+        cudaGraphExec_t exec = nullptr;
         AZK_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         enqueue_rounds_batched(from_coeffs);
         enqueue_tail_batched();
         AZK_CU(cudaStreamEndCapture(s, &gr));
-        AZK_CU(cudaGraphInstantiate(&graph, gr, 0));
+        const cudaError_t e = cudaGraphInstantiate(&exec, gr, 0);
         cudaGraphDestroy(gr);
-        graph_from_coeffs = from_coeffs;
+        AZK_CU(e);
+        it = graphs.emplace(std::move(key), exec).first;
       }
-      AZK_CU(cudaGraphLaunch(graph, s));
+      AZK_CU(cudaGraphLaunch(it->second, s));
     } else {
       enqueue_rounds_batched(from_coeffs);
       for (uint32_t i = 0; i < active(); i++) grind_instance(i);
@@ -1107,15 +1139,14 @@ uint32_t shape_capacity(const azk_server* sv, const ServeJob& j) {
 
 // Proves a group of same-shape PCS jobs on the worker's engine for the shape (made
 // on first use with room for the shape's capacity): inputs staged and copied, one
-// scan launch, one batched superstep over the group's instances, proofs read back.
+// scan launch, one batched superstep over the group's instances (one CUDA graph
+// launch: the engine captures the sequence once per group size), proofs read back.
 void run_pcs_group(azk_server* sv, Resident& r, std::vector<std::shared_ptr<ServeJob>>& g, Staging& st, cudaStream_t s) {
   const ServeJob& j0 = *g[0];
   if (!r.eng) {
     r.eng = std::make_unique<Engine>();
-    Sched sc = sv->sched;
-    sc.graph = false;
     std::vector<InstanceCfg> cf(r.cap, InstanceCfg{j0.logn, j0.rounds, j0.queries, j0.log_blowup, 0, {}});
-    r.eng->init(sv->ctx, cf, sc, s, s);
+    r.eng->init(sv->ctx, cf, sv->sched, s, s);
   }
   Engine* e = r.eng.get();
   const size_t m = g.size();
