@@ -355,7 +355,7 @@ def run_serving(azk, ctx, args, batched_jobs_per_s, batched_elems_per_s=None):
     sc_tables = [uniform_m31(SEED ^ (0x5C0 + i), 1 << 20) for i in range(2)]
     pubs = public_digests(4096, SEED ^ 0x5E)
     server = azk.ProofServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), slots=args.serve_slots,
-                             schedule=dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=0))
+                             schedule=dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1))
 
     def submit(job, i):
         kind, k = job
