@@ -120,10 +120,10 @@ __device__ __forceinline__ Pass low_pass(const FftJob& job, uint64_t tile) {
 // values v[b] (bit k of b = L bit 4Q + k; Lbase = the thread's L with those bits
 // zero): 8 butterflies with the 2^(3-K) twiddles of the stage's blocks above it.
 __device__ __forceinline__ void bfly(qm31& l, qm31& r, uint32_t t) {
-  const qm31 rt = q_mul_m31(r, t);
-  const qm31 a = q_add(l, rt);
-  r = q_sub(l, rt);
-  l = a;
+  bfly(l.a, r.a, t);
+  bfly(l.b, r.b, t);
+  bfly(l.c, r.c, t);
+  bfly(l.d, r.d, t);
 }
 
 // Twiddles of one sub-pass, loaded ahead of the butterflies that use them (before
@@ -220,11 +220,21 @@ __device__ __forceinline__ void finish_tile(uint32_t* Y, const FftJob& job, cons
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
-  __shared__ __align__(16) uint32_t Y[kTile];
-  const uint2 w = work[blockIdx.x];
-  const FftJob& job = jobs[w.x];
-  const Pass p = make_pass(job, w.y);
+// make_pass with the pass's stage count M (> 0) known at compile time: the same
+// values, so the sub-pass conditions and index arithmetic fold to constants.
+template <int M>
+__device__ __forceinline__ Pass make_pass_m(const FftJob& job, uint64_t tile) {
+  Pass p = make_pass(job, tile);
+  if constexpr (M > 0) {
+    p.m = M;
+    p.c = kFftLowBits - M;
+  }
+  return p;
+}
+
+template <int M>
+__device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y) {
+  const Pass p = make_pass_m<M>(job, w.y);
   const uint64_t N = 1ull << p.logn;
   const bool first = job.pass == 0;
   const bool last = job.pass == fft_high_chunks(p.logn);
@@ -273,6 +283,24 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob*
   tw_load<1>(w1, sub1_base(t), p, job.tw, 3);
   __syncthreads();
   finish_tile(Y, job, p, last, w1);
+}
+
+// One CTA per tile; the passes that hold most of the values of large transforms
+// (6 to 10 high stages, and the single pass of a 2^12 transform) run code
+// specialised for their stage count, the others the general form.
+__global__ void __launch_bounds__(kThreads, 4) fft_m31_tile_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work) {
+  __shared__ __align__(16) uint32_t Y[kTile];
+  const uint2 w = work[blockIdx.x];
+  const FftJob& job = jobs[w.x];
+  switch (fft_pass_geom(job.logn, job.pass).m) {
+    case 10: m31_tile<10>(job, w, Y); break;
+    case 9: m31_tile<9>(job, w, Y); break;
+    case 8: m31_tile<8>(job, w, Y); break;
+    case 7: m31_tile<7>(job, w, Y); break;
+    case 6: m31_tile<6>(job, w, Y); break;
+    case 12: m31_tile<12>(job, w, Y); break;
+    default: m31_tile<0>(job, w, Y); break;
+  }
 }
 
 // ---------------------------------------------------------------------------
