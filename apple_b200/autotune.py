@@ -414,14 +414,26 @@ TABLE_SHAPES = {
     "pcs_batch": dict(concurrent=64, leaf_bytes=16, fold=1),   # batched supersteps: many trees per launch
     "merkle_raw64": dict(concurrent=1, leaf_bytes=64, fold=0),  # raw-leaf Merkle plan
 }
+# Shapes whose threads per CTA stay fixed: a batched commit launch holds layers of
+# many sizes, the measured gain of another thread count at 64 concurrent trees is
+# at most 1 % (log 6-18), and the largest layers (2^19-2^22 leaves x 64) are
+# outside the measured grid, so the depth is chosen at the default 256 threads.
+FIXED_THREADS = {"pcs_batch": 256}
 
 
 def export(tuner: Tuner, report: dict, json_path: str, header_path: str):
     """Write the tables (and the evidence behind them) as JSON and as the C++ header
     the library compiles in (`csrc/azk_tuned.h`): per layer size the treelet depth
     and the threads per CTA the model picks."""
-    both = {name: tuner.layer_tables(**kw) for name, kw in TABLE_SHAPES.items()}
-    doc = {"device": _device_name(tuner.ctx), "report": report, "shapes": TABLE_SHAPES,
+    both = {}
+    for name, kw in TABLE_SHAPES.items():
+        if name in FIXED_THREADS:
+            th = FIXED_THREADS[name]
+            tiles = tuner.layer_table(threads=th, **kw)
+            both[name] = (tiles, {lg: th for lg in tiles})
+        else:
+            both[name] = tuner.layer_tables(**kw)
+    doc = {"device": _device_name(tuner.ctx), "report": report, "shapes": TABLE_SHAPES, "fixed_threads": FIXED_THREADS,
            "tables": {k: {str(lg): t for lg, t in v[0].items()} for k, v in both.items()},
            "thread_tables": {k: {str(lg): t for lg, t in v[1].items()} for k, v in both.items()}}
     with open(json_path, "w") as f:

@@ -14,31 +14,10 @@ namespace azk {
 static constexpr uint32_t kP = 2147483647u;
 static constexpr uint32_t kInv2 = 1073741824u;
 
-// On the device, part of the integer adds below are issued as multiply-adds
-// (x * 1 + y), which run on the FMA pipe: field-arithmetic kernels (FFT
-// butterflies, folds, and the folds inside the commit kernel next to its Keccak
-// rounds) otherwise queue on the integer ALU pipe while the FMA pipe idles.  The
-// factor 1 is read from constant memory at run time, so the compiler cannot turn
-// a multiply-add back into an add.  The values computed are the same.
-#ifdef __CUDACC__
-static __constant__ uint32_t kFmaOne = 1;
-#endif
-#ifdef __CUDA_ARCH__
-__device__ __forceinline__ uint32_t add_fma(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(kFmaOne), "r"(b));
-  return r;
-}
-#define AZK_ADD(a, b) add_fma((a), (b))
-#else
-#define AZK_ADD(a, b) ((a) + (b))
-#endif
-
-// s < 2p -> s mod p.  s - p = s + (2^32 - p) is below s exactly when s >= p
-// (otherwise it wraps above it), so the reduction is an unsigned minimum: one
-// subtract, one min.
+// s < 2p -> s mod p.  s - p is below s exactly when s >= p (otherwise it wraps
+// above it), so the reduction is an unsigned minimum: one subtract, one min.
 __host__ __device__ __forceinline__ uint32_t m31_reduce_once(uint32_t s) {
-  const uint32_t t = AZK_ADD(s, 0x80000001u);
+  const uint32_t t = s - kP;
   return t < s ? t : s;
 }
 __host__ __device__ __forceinline__ uint32_t m31_fold64(uint64_t v) {
@@ -48,7 +27,7 @@ __host__ __device__ __forceinline__ uint32_t m31_fold64(uint64_t v) {
   return s >= kP ? s - kP : s;
 }
 // Inputs are at most p (canonical values, or p itself as a redundant zero).
-__host__ __device__ __forceinline__ uint32_t m31_add(uint32_t a, uint32_t b) { return m31_reduce_once(AZK_ADD(a, b)); }
+__host__ __device__ __forceinline__ uint32_t m31_add(uint32_t a, uint32_t b) { return m31_reduce_once(a + b); }
 // a + (p - b) lies in [0, 2p): one reduction, no branch on a >= b.
 __host__ __device__ __forceinline__ uint32_t m31_sub(uint32_t a, uint32_t b) { return m31_reduce_once(a + (kP - b)); }
 __host__ __device__ __forceinline__ uint32_t m31_neg(uint32_t a) { return a == 0 ? 0 : kP - a; }
@@ -57,7 +36,7 @@ __host__ __device__ __forceinline__ uint32_t m31_neg(uint32_t a) { return a == 0
 // finishes it.
 __host__ __device__ __forceinline__ uint32_t m31_mul(uint32_t a, uint32_t b) {
   const uint64_t v = (uint64_t)a * (uint64_t)b;
-  return m31_reduce_once(AZK_ADD((uint32_t)v & kP, (uint32_t)(v >> 31)));
+  return m31_reduce_once(((uint32_t)v & kP) + (uint32_t)(v >> 31));
 }
 // x * 2^-1 mod p: halve an even value, or (x + p) / 2 = (x >> 1) + 2^30 for an odd one.
 __host__ __device__ __forceinline__ uint32_t m31_half(uint32_t a) { return (a >> 1) + ((a & 1u) << 30); }
@@ -72,7 +51,6 @@ __host__ __device__ __forceinline__ uint32_t m31_pow(uint32_t b, uint32_t e) {
 }
 // Fermat inverse a^(p-2); returns 0 for a == 0 (callers validate).
 __host__ __device__ __forceinline__ uint32_t m31_inv(uint32_t a) { return m31_pow(a, kP - 2); }
-
 
 struct qm31 {
   uint32_t a, b, c, d;

@@ -659,9 +659,9 @@ def config_block(args, logs):
                     f"16-B QM31 leaves, fold to log {args.final_log}, 64 queries, proof bytes on device",
         "instances": len(logs),
         "total_codeword_elems": int(sum(1 << lg for lg in logs)),
-        "schedule": ({"treelet_log": args.treelet_log, "group_log": args.group_log, "threads": args.threads, "graph": True} if args.treelet_log else
+        "schedule": ({"treelet_log": args.treelet_log, "group_log": args.group_log, "threads": args.threads or 256, "graph": True} if args.treelet_log else
                      {"treelet": "tuned per-layer table (cost model over measured timings, csrc/azk_tuned.h pcs_batch)", "group_log": args.group_log,
-                      "threads": args.threads, "graph": True}),
+                      "threads": args.threads or "tuned per-layer table (pcs_batch: 256)", "graph": True}),
         "l2": "inputs larger than L2 (codewords and trees of one superstep are several GB)",
         "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))} (no data-path collective)",
     }
@@ -681,7 +681,7 @@ def main():
     ap.add_argument("--compare-schedules", type=int, default=1)
     ap.add_argument("--leaf64", type=int, default=1)
     ap.add_argument("--group-log", type=int, default=12)
-    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA of the commit kernel (0: the tuned per-layer tables)")
     ap.add_argument("--plain-steps", type=int, default=5)
     ap.add_argument("--plain-warmup", type=int, default=1)
     ap.add_argument("--cpu-max-log", type=int, default=64, help="largest log size in the CPU oracle's sample")
@@ -715,7 +715,7 @@ def main():
     # schedule: the library's tuned per-layer table for batched supersteps unless a
     # fixed treelet depth is asked for
     if args.treelet_log:
-        sched = dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1)
+        sched = dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads or 256, use_graph=1)
     else:
         sched = dict(group_log=args.group_log, threads=args.threads, use_graph=1)
     batch = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=sched)
@@ -848,8 +848,11 @@ def main():
     plain_mismatch = False
     if args.plain_steps:
         tables = tuned_tables()
+        thr = tuned_thread_tables() or {}
         psched = dict(layer_treelet=tables["pcs_single"], group_log=args.group_log, threads=args.threads, use_graph=0) if tables and not args.treelet_log \
             else sched
+        if psched is not sched and not args.threads and "pcs_single" in thr:
+            psched["layer_threads"] = thr["pcs_single"]
         if batch is not None:
             del batch
             batch = None
@@ -873,7 +876,7 @@ def main():
         from apple_b200 import autotune as T
 
         tables = tuned_tables() or {}
-        bq = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=dict(treelet_log=12, group_log=args.group_log, threads=args.threads, use_graph=0))
+        bq = azk.BatchProver(ctx, logs, rounds, 2, 64, schedule=dict(treelet_log=12, group_log=args.group_log, threads=256, use_graph=0))
         bq.upload(host_rows, offsets, counts)
         bq.prove(pubs, plain=True)
         pt = [bq.prove(pubs, plain=True).gpu_s for _ in range(3)]
