@@ -38,6 +38,13 @@ __host__ __device__ __forceinline__ uint32_t m31_mul(uint32_t a, uint32_t b) {
   const uint64_t v = (uint64_t)a * (uint64_t)b;
   return m31_reduce_once(((uint32_t)v & kP) + (uint32_t)(v >> 31));
 }
+// a * t for a <= p and t2 = 2t (t < p): the 64-bit product a t2 = 2 a t has a t >> 31
+// in its high word and (a t mod 2^31) << 1 in its low word, so the Mersenne fold is
+// hi + (lo >> 1) (below 2p), without masking the low word.
+__host__ __device__ __forceinline__ uint32_t m31_mul_dbl(uint32_t a, uint32_t t2) {
+  const uint64_t v = (uint64_t)a * (uint64_t)t2;
+  return m31_reduce_once((uint32_t)(v >> 32) + ((uint32_t)v >> 1));
+}
 // x * 2^-1 mod p: halve an even value, or (x + p) / 2 = (x >> 1) + 2^30 for an odd one.
 __host__ __device__ __forceinline__ uint32_t m31_half(uint32_t a) { return (a >> 1) + ((a & 1u) << 30); }
 __host__ __device__ __forceinline__ uint32_t m31_pow(uint32_t b, uint32_t e) {

@@ -90,7 +90,7 @@ struct FftJob {
   uint32_t pass;             // this job's pass index (0 reads `in`; the last pass is the low stages)
   const uint4* in;           // FFT-basis coefficients (read by the first pass)
   uint4* out;                // codeword (bit-reversed order)
-  const uint32_t* tw;        // stage twiddles of the domain (N - 1 values)
+  const uint32_t* tw;        // stage twiddles of the domain (N - 1 values; tw + N: the same doubled)
   uint32_t* narrow;          // N words of scratch between passes of the one-limb kernel
   const InputInfo* info;     // nonzero prefix of the input (null: all N coefficients read)
 };

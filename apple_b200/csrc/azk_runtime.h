@@ -25,7 +25,7 @@ struct azk_ctx {
   std::mutex mu;
   std::string last_error;
   struct Domain {
-    uint32_t* tw = nullptr;
+    uint32_t* tw = nullptr;  // N - 1 stage twiddles, then (at tw + N) the same doubled
     uint32_t* inv = nullptr;
   };
   std::map<uint32_t, Domain> domains;

@@ -11,7 +11,8 @@
 namespace azk {
 
 // ---------------------------------------------------------------------------
-// Domain tables.  tw[off(s) + h] = stage-s FFT twiddle of block h, with
+// Domain tables.  tw[off(s) + h] = stage-s FFT twiddle of block h (and tw[N + g]
+// = 2 tw[g], the doubled copy the register-blocked FFT multiplies by), with
 // off(0) = 0 and off(s) = N - (N >> s): the y coordinate of the point at storage
 // index h << 1 for stage 0, else its x coordinate doubled s - 1 times.  The FRI
 // inverse-domain layer k is the elementwise inverse of stage k (inv(y) for the
@@ -39,6 +40,7 @@ __global__ void domain_tables_kernel(uint32_t logn, uint32_t* __restrict__ tw, u
     for (uint32_t k = 1; k < s; k++) v = double_x(v);
   }
   tw[g] = v;
+  tw[n + g] = v << 1;  // doubled copy for the register-blocked FFT's multiply
   if (inv) inv[g] = m31_inv(v);
 }
 

@@ -55,8 +55,12 @@ __device__ __forceinline__ uint64_t twoff(uint32_t logn, uint32_t s) {
 // values stay one aligned 16-byte vector.
 __device__ __forceinline__ uint32_t swz(uint32_t L) { return L ^ (((L >> 3) & 12u) | ((L >> 4) & 16u)); }
 
-__device__ __forceinline__ void bfly(uint32_t& l, uint32_t& r, uint32_t t) {
-  const uint32_t rt = m31_mul(r, t);
+// The doubled twiddle table (2 t at tw + N): the butterflies multiply by 2t.
+__device__ __forceinline__ const uint32_t* tw2(const FftJob& job) { return job.tw + (1ull << job.logn); }
+
+// (l, r) -> (l + r t, l - r t), given t2 = 2t
+__device__ __forceinline__ void bfly(uint32_t& l, uint32_t& r, uint32_t t2) {
+  const uint32_t rt = m31_mul_dbl(r, t2);
   const uint32_t a = m31_add(l, rt);
   r = m31_sub(l, rt);
   l = a;
@@ -195,7 +199,7 @@ __device__ __forceinline__ void finish_tile(uint32_t* Y, const FftJob& job, cons
   for (int b = 0; b < 16; b++) Y[swz(LB | ((uint32_t)b << 4))] = v[b];
   const uint32_t LC = t << 4;
   TwSet w0;
-  tw_load<0>(w0, LC, p, job.tw, 3);
+  tw_load<0>(w0, LC, p, tw2(job), 3);
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < 4; r++) {
@@ -247,7 +251,7 @@ __device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y
   const uint32_t t = threadIdx.x;
   const uint32_t LA = t;
   TwSet w2;
-  tw_load<2>(w2, LA, p, job.tw, top_zero ? 1 : 3);
+  tw_load<2>(w2, LA, p, tw2(job), top_zero ? 1 : 3);
   uint32_t v[16];
   if (first) {
     const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
@@ -280,7 +284,7 @@ __device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y
 #pragma unroll
   for (int b = 0; b < 16; b++) Y[swz(LA | ((uint32_t)b << 8))] = v[b];
   TwSet w1;
-  tw_load<1>(w1, sub1_base(t), p, job.tw, 3);
+  tw_load<1>(w1, sub1_base(t), p, tw2(job), 3);
   __syncthreads();
   finish_tile(Y, job, p, last, w1);
 }
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   const uint32_t t = threadIdx.x;
   const uint32_t LA = t;
   TwSet tws;
-  tw_load<2>(tws, LA, p, job.tw, top_zero ? 1 : 3);
+  tw_load<2>(tws, LA, p, tw2(job), top_zero ? 1 : 3);
   qm31 v[16];
   if (first) {
     const int loads = top_zero ? 4 : 16;
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
 #pragma unroll
   for (int b = 0; b < 16; b++) Yq[swq(LA | ((uint32_t)b << 8))] = from_q(v[b]);
   const uint32_t LB = sub1_base(t);
-  tw_load<1>(tws, LB, p, job.tw, 3);
+  tw_load<1>(tws, LB, p, tw2(job), 3);
   __syncthreads();
 #pragma unroll
   for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LB | ((uint32_t)b << 4))]);
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
 #pragma unroll
   for (int b = 0; b < 16; b++) Yq[swq(LB | ((uint32_t)b << 4))] = from_q(v[b]);
   const uint32_t LC = t << 4;
-  tw_load<0>(tws, LC, p, job.tw, 3);
+  tw_load<0>(tws, LC, p, tw2(job), 3);
   __syncthreads();
 #pragma unroll
   for (int b = 0; b < 16; b++) v[b] = to_q(Yq[swq(LC | (uint32_t)b)]);
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_low_tma_kernel(const FftJ
     const FftJob& job = jobs[w.x];
     const Pass p = low_pass(job, w.y);
     TwSet w2;
-    tw_load<2>(w2, t, p, job.tw, 3);
+    tw_load<2>(w2, t, p, tw2(job), 3);
     const bool ok = mbar_wait(&bar, phase);
     phase ^= 1u;
     uint32_t v[16];
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_low_tma_kernel(const FftJ
 #pragma unroll
     for (int b = 0; b < 16; b++) Y[swz(t | ((uint32_t)b << 8))] = v[b];
     TwSet w1;
-    tw_load<1>(w1, sub1_base(t), p, job.tw, 3);
+    tw_load<1>(w1, sub1_base(t), p, tw2(job), 3);
     // X has been read by every thread: the next tile's copy may land in it
     if (__syncthreads_or(!ok)) {
       // the copy that did not complete may still land: wait for it once more

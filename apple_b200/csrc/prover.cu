@@ -1025,8 +1025,9 @@ uint64_t pcs_instance_bytes(uint32_t logn, uint32_t rounds, uint32_t queries) {
 uint64_t pcs_engine_bytes(uint32_t logn, uint32_t rounds, uint32_t queries, uint32_t cap) {
   return cap * pcs_instance_bytes(logn, rounds, queries) + (64ull << 10);
 }
-// Domain tables of a log size (FFT twiddles and their inverses, N - 1 words each).
-uint64_t domain_bytes(uint32_t logn) { return 8ull << logn; }
+// Domain tables of a log size (FFT twiddles, their doubled copy and their
+// inverses, N words each).
+uint64_t domain_bytes(uint32_t logn) { return 12ull << logn; }
 
 struct SumcheckBufs {
   DevBuf ev, scratch, rounds, out;

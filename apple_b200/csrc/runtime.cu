@@ -28,7 +28,7 @@ const azk_ctx::Domain& azk::domain_tables(azk_ctx* ctx, uint32_t logn) {
   if (it != ctx->domains.end()) return it->second;
   uint64_t n = 1ull << logn;
   azk_ctx::Domain d;
-  AZK_CU(cudaMalloc(&d.tw, 4 * (n - 1 + 1)));
+  AZK_CU(cudaMalloc(&d.tw, 4 * 2 * n));  // twiddles, then their doubled copy at tw + N
   AZK_CU(cudaMalloc(&d.inv, 4 * (n - 1 + 1)));
   AZK_CU(launch_domain_tables(logn, d.tw, d.inv, ctx->stream));
   sync_stream(ctx->stream);

@@ -52,6 +52,8 @@ int main() {
     uint32_t x = U(rng), y = U(rng);
     if (t < 8) { x = (t & 1) ? 0 : O::m31::P - 1; y = (t & 2) ? 0 : O::m31::P - 1; }
     CHECK(azk::m31_mul(x, y) == O::m31::mul(x, y), "m31 mul");
+    CHECK(azk::m31_mul_dbl(x, y << 1) == O::m31::mul(x, y), "m31 mul by a doubled operand");
+    CHECK(azk::m31_mul_dbl(O::m31::P, y << 1) == 0, "m31 mul by a doubled operand, redundant zero");
     CHECK(azk::m31_add(x, y) == O::m31::add(x, y), "m31 add");
     CHECK(azk::m31_sub(x, y) == O::m31::sub(x, y), "m31 sub");
     CHECK(azk::m31_half(x) == O::m31::mul(x, 1073741824u), "m31 half");
