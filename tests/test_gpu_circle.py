@@ -146,3 +146,26 @@ def test_canonical_gate(ctx):
     buf.upload(words)
     _capi.check(_capi.lib().azk_check_canonical(ctx.handle, buf.ptr, 1024, ctypes.byref(flag)))
     assert flag.value == 1
+
+
+@pytest.mark.parametrize("log_size", [5, 13])
+def test_codeword_plan_resident_ranges(ctx, oracle, log_size):
+    """executeResident (CircleCodeword.swift:517-545): coefficients and codeword in
+    device buffers at byte offsets equal the host form; a range past its allocation
+    or an output over the coefficients is rejected."""
+    rng = np.random.default_rng(log_size)
+    n = 1 << log_size
+    coeffs = rng.integers(0, G.P, size=(n, 4), dtype=np.uint32)
+    plan = azk.CircleCodewordPlan(ctx, log_size)
+    want = plan.execute_coefficients(coeffs)
+    din, dout = ctx.alloc(16 * n + 32), ctx.alloc(16 * n + 64)
+    din.upload(coeffs, 32)
+    plan.execute_resident(din.ptr, dout.ptr, in_offset=32, out_offset=64)
+    assert np.array_equal(np.frombuffer(dout.download(16 * n, 64), np.uint32).reshape(-1, 4), want)
+    for args in [dict(in_offset=48), dict(out_offset=80)]:
+        with pytest.raises(azk.AZKError) as e:
+            plan.execute_resident(din.ptr, dout.ptr, **args)
+        assert e.value.name == "invalidInputLayout"
+    with pytest.raises(azk.AZKError) as e:
+        plan.execute_resident(din.ptr, din.ptr, in_offset=32, out_offset=16)
+    assert e.value.name == "invalidInputLayout"
