@@ -93,7 +93,6 @@ struct FftJob {
   const uint32_t* tw;        // stage twiddles of the domain (N - 1 values; tw + N: the same doubled)
   uint32_t* narrow;          // N words of scratch between passes of the one-limb kernel
   const InputInfo* info;     // nonzero prefix of the input (null: all N coefficients read)
-  const void* tmap;          // first pass: tensor map over `in` for the staged row copies (or null)
 };
 
 // Circle FFT pass geometry: the stages above bit 12 run first in chunks of at
@@ -226,42 +225,21 @@ uint64_t witness_partial_values(uint64_t n);
 // a bounded wait on its copies runs out.
 // kFftQ4Tile: four-limb tiles of transforms of 2^12 values or more that are not
 // lifted M31 polynomials (fft_q_tile_kernel); kFftQM31 then serves the smaller ones.
-// kFftM31First6 ... kFftM31First10: first passes of 6 ... 10 stages whose
-// coefficient prefix is at most N/4, rows staged by tensor copies.
-enum FftKind : uint32_t {
-  kFftQM31 = 0,
-  kFftM31Small = 1,
-  kFftM31Tile = 2,
-  kFftM31Low = 3,
-  kFftQ4Tile = 4,
-  kFftM31First6 = 5,
-  kFftM31First10 = 9,
-  kFftKinds = 10
-};
-// Input form of a transform: QM31 coefficients, a lifted M31 polynomial, or a
-// lifted M31 polynomial whose nonzero prefix is at most N/4.
-enum FftInput : uint8_t { kFftInQM31 = 0, kFftInM31 = 1, kFftInM31Quarter = 2 };
+enum FftKind : uint32_t { kFftQM31 = 0, kFftM31Small = 1, kFftM31Tile = 2, kFftM31Low = 3, kFftQ4Tile = 4, kFftKinds = 5 };
 cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t kind, uint32_t* d_status, cudaStream_t s);
 cudaError_t prepare_fft_m31_kernels();
 cudaError_t launch_fft_m31_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 cudaError_t launch_fft_m31_low(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t* d_status, cudaStream_t s);
-cudaError_t launch_fft_m31_first(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t m, uint32_t* d_status, cudaStream_t s);
 cudaError_t launch_fft_q_tiles(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, cudaStream_t s);
 // Which kernel runs pass `pass` of a transform of 2^logn values, and how many
 // work items (tiles) it has.
-inline uint32_t fft_pass_kind(uint32_t logn, uint32_t pass, uint32_t input) {
-  if (input == kFftInQM31) return logn < kFftLowBits ? kFftQM31 : kFftQ4Tile;
+inline uint32_t fft_pass_kind(uint32_t logn, uint32_t pass, bool narrow) {
+  if (!narrow) return logn < kFftLowBits ? kFftQM31 : kFftQ4Tile;
   if (logn < kFftLowBits) return kFftM31Small;
-  if (pass == 0 && logn > kFftLowBits && input == kFftInM31Quarter) {
-    const uint32_t m = fft_pass_geom(logn, 0).m;
-    if (m >= 6 && m <= 10) return kFftM31First6 + (m - 6);
-  }
   return (pass == fft_high_chunks(logn) && pass > 0) ? kFftM31Low : kFftM31Tile;
 }
-inline bool fft_kind_first(uint32_t kind) { return kind >= kFftM31First6 && kind <= kFftM31First10; }
 inline uint64_t fft_kind_tiles(uint32_t logn, uint32_t pass, uint32_t kind) {
-  return (kind == kFftM31Tile || kind == kFftM31Low || kind == kFftQ4Tile || fft_kind_first(kind)) ? (1ull << (logn - kFftLowBits))
-                                                                                                   : fft_pass_tiles(logn, pass);
+  return (kind == kFftM31Tile || kind == kFftM31Low || kind == kFftQ4Tile) ? (1ull << (logn - kFftLowBits)) : fft_pass_tiles(logn, pass);
 }
 // Canonicality gate over `count` QM31 coefficients; with `info`, also clears
 // info->m31 when some coefficient has a nonzero b, c or d limb (the caller sets

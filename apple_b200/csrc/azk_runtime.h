@@ -1,7 +1,6 @@
 // Host-side runtime shared by the C-ABI translation units: context, error
 // handling, device buffers, domain-table cache and the work-list builders.
 #pragma once
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <array>
@@ -251,16 +250,11 @@ struct FftPlan {
   std::vector<FftJob> jobs;
   std::vector<uint2> work;  // all steps, step-major, kind-major, transform-contiguous
   std::vector<std::array<uint64_t, kFftKinds>> part_off, part_cnt;  // per step and kind
-  std::vector<uint8_t> narrow;                                      // per transform: FftInput
+  std::vector<uint8_t> narrow;                                      // per transform
   std::vector<std::vector<std::pair<uint64_t, uint64_t>>> inst_range;  // [step][transform] -> (offset, count)
   std::vector<std::vector<uint8_t>> inst_kind;                         // [step][transform] -> FftKind
   DevBuf d_jobs, d_work;
   DevBuf d_status;  // raised by a pass kernel whose bounded wait ran out
-  // first passes whose row copies go through a tensor map (job index, host map),
-  // and the maps in device memory (128 bytes each, 64-byte aligned)
-  std::vector<uint32_t> tmap_jobs;
-  std::vector<CUtensorMap> h_maps;
-  DevBuf d_tmaps;
   size_t steps() const { return part_off.size(); }
   void build(const std::vector<FftJob>& transforms, const std::vector<uint8_t>& narrow_flags = {});
   void upload(cudaStream_t s);

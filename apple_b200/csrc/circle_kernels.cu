@@ -471,12 +471,6 @@ cudaError_t launch_fft_pass(const FftJob* d_jobs, const uint2* d_work, uint32_t 
       return launch_fft_m31_tiles(d_jobs, d_work, nwork, s);
     case kFftM31Low:
       return launch_fft_m31_low(d_jobs, d_work, nwork, d_status, s);
-    case kFftM31First6:
-    case kFftM31First6 + 1:
-    case kFftM31First6 + 2:
-    case kFftM31First6 + 3:
-    case kFftM31First10:
-      return launch_fft_m31_first(d_jobs, d_work, nwork, kind - kFftM31First6 + 6, d_status, s);
     case kFftQ4Tile:
       return launch_fft_q_tiles(d_jobs, d_work, nwork, s);
     default:

@@ -31,8 +31,6 @@
 //    more bounded wait for the copy it was waiting on.
 //  - fft_q_tile_kernel: the same tiles over QM31 values (inputs that are not lifted
 //    M31 polynomials), in place in the codeword buffer between passes.
-#include <algorithm>
-
 #include "azk_bulk.cuh"
 #include "azk_field.cuh"
 #include "azk_internal.h"
@@ -238,10 +236,8 @@ __device__ __forceinline__ Pass make_pass_m(const FftJob& job, uint64_t tile) {
   return p;
 }
 
-// One tile of a one-limb pass.  STAGED: a first pass whose input rows are already
-// in shared memory (value L of the tile at staged[L], L < 1024; top_zero holds).
-template <int M, bool STAGED = false>
-__device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y, const uint4* staged = nullptr) {
+template <int M>
+__device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y) {
   const Pass p = make_pass_m<M>(job, w.y);
   const uint64_t N = 1ull << p.logn;
   const bool first = job.pass == 0;
@@ -251,7 +247,7 @@ __device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y
   // two top stages (m >= 2; they are L bits 11 and 10): every value with either of
   // those bits set is zero, so the two top stages only copy (l + 0 t, l - 0 t) and
   // only 4 of the thread's 16 values are read
-  const bool top_zero = STAGED || (first && p.m >= 2 && count <= (N >> 2));
+  const bool top_zero = first && p.m >= 2 && count <= (N >> 2);
   const uint32_t t = threadIdx.x;
   const uint32_t LA = t;
   TwSet w2;
@@ -259,16 +255,7 @@ __device__ __forceinline__ void m31_tile(const FftJob& job, uint2 w, uint32_t* Y
   uint32_t v[16];
   if (first) {
     const uint32_t* in_a = reinterpret_cast<const uint32_t*>(job.in);
-    if (STAGED) {
-      // the rows were copied whole (zeros past the prefix included): the a limbs of
-      // the thread's 4 values, read as single words
-      const uint32_t* sa = reinterpret_cast<const uint32_t*>(staged);
-      uint32_t x[4];
-#pragma unroll
-      for (int b = 0; b < 4; b++) x[b] = sa[4 * (LA | ((uint32_t)b << 8))];
-#pragma unroll
-      for (int b = 0; b < 16; b++) v[b] = x[b & 3];
-    } else if (top_zero) {
+    if (top_zero) {
       uint32_t x[4];
 #pragma unroll
       for (int b = 0; b < 4; b++) {
@@ -407,95 +394,6 @@ __global__ void __launch_bounds__(kThreads, 2) fft_q_tile_kernel(const FftJob* _
   }
 }
 
-// ---------------------------------------------------------------------------
-// First (high-stage) passes of M = 6 ... 10 stages of one-limb transforms whose
-// coefficient prefix is at most N/4 (so only a tile's lower quarter of rows is
-// read), persistent: a CTA walks the pass's tiles, and the rows come in by one
-// tensor copy per tile (cp.async.bulk.tensor.3d through the job's tensor map: box =
-// 2^(M-2) rows x 2^(12-M) coefficients x 16 bytes = 16 KB).  Two landing buffers:
-// the copy for a CTA's next tile is issued when the current tile starts, into the
-// buffer the tile before it used (finished at the previous iteration's closing
-// barrier), so it runs under the whole tile.  The host sends only such passes here
-// (a tensor map and the prefix bound are checked again: a tile without them raises
-// status bit 2 and is skipped).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool first_staged(const FftJob& job) {
-  if (!job.tmap) return false;
-  const uint64_t N = 1ull << job.logn;
-  const uint64_t count = (job.info != nullptr && job.info->count != 0) ? job.info->count : N;
-  return count <= (N >> 2);
-}
-
-// Tensor copy of tile `tile`'s lower-quarter rows: coordinates {0, mid, hi << m}.
-__device__ __forceinline__ void fetch_first_tile(const FftJob& job, uint64_t tile, uint4* X, uint64_t* bar) {
-  const FftPassGeom g = fft_pass_geom(job.logn, 0);
-  const uint32_t c = kFftLowBits - g.m, midbits = g.s_lo - c;
-  const uint32_t mid = (uint32_t)(tile & ((1ull << midbits) - 1)), row = (uint32_t)((tile >> midbits) << g.m);
-  // the map was written by a host copy before the launch: order the tensor-map
-  // proxy's read of it after that write
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(job.tmap) : "memory");
-  mbar_expect_tx(bar, 1024u * 16u);
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(X)),
-      "l"(job.tmap), "r"(0), "r"(mid), "r"(row), "r"(smem_u32(bar))
-      : "memory");
-}
-
-template <int M>
-__global__ void __launch_bounds__(kThreads, 4) fft_m31_first_kernel(const FftJob* __restrict__ jobs, const uint2* __restrict__ work, uint32_t nwork,
-                                                                    uint32_t* __restrict__ status) {
-  // dynamic shared memory: two landing buffers (16 KB each), the swizzled working
-  // buffer, the two mbarriers
-  extern __shared__ __align__(128) uint4 fsm[];
-  uint4 (*X)[1024] = reinterpret_cast<uint4 (*)[1024]>(fsm);
-  uint32_t* Y = reinterpret_cast<uint32_t*>(fsm + 2048);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(fsm + 2048 + kTile / 4);
-  const uint32_t t = threadIdx.x;
-  uint32_t item = blockIdx.x;
-  if (item >= nwork) return;
-  if (t == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    const uint2 w0 = work[item];
-    if (first_staged(jobs[w0.x])) fetch_first_tile(jobs[w0.x], w0.y, X[0], &bar[0]);
-  }
-  __syncthreads();
-  uint32_t sidx = 0;  // tiles copied so far: buffer sidx & 1, parity (sidx >> 1) & 1
-  for (; item < nwork; item += gridDim.x) {
-    const uint2 w = work[item];
-    const FftJob& job = jobs[w.x];
-    const bool staged = first_staged(job);
-    const uint32_t buf = sidx & 1u;
-    if (staged) {
-      const bool ok = mbar_wait(&bar[buf], (sidx >> 1) & 1u);
-      if (__syncthreads_or(!ok)) {
-        // the copy that did not complete may still land: wait once more (bounded)
-        if (t == 0) {
-          atomicOr(status, 1u);
-          mbar_wait(&bar[buf], (sidx >> 1) & 1u);
-        }
-        return;
-      }
-    }
-    const uint32_t next = item + gridDim.x;
-    if (t == 0 && next < nwork) {
-      const uint2 wn = work[next];
-      if (first_staged(jobs[wn.x])) {
-        const uint32_t nb = (sidx + (staged ? 1u : 0u)) & 1u;
-        fence_proxy_async_smem();
-        fetch_first_tile(jobs[wn.x], wn.y, X[nb], &bar[nb]);
-      }
-    }
-    if (staged) {
-      m31_tile<M, true>(job, w, Y, X[buf]);
-      sidx++;
-    } else if (t == 0) {
-      atomicOr(status, 2u);
-    }
-    __syncthreads();  // Y and this tile's landing buffer are rewritten later
-  }
-}
-
 // Queue the bulk copy of work item `item`'s input tile (4096 contiguous words of the
 // exchange buffer: the low pass has c = 0 and s_lo = 0, so tile w is words
 // [4096 w, 4096 w + 4096); 16 KB, 16-byte aligned) into X.
@@ -555,19 +453,7 @@ __global__ void __launch_bounds__(kThreads, 4) fft_m31_low_tma_kernel(const FftJ
   }
 }
 
-int g_low_grid[64] = {0};    // resident CTAs of the persistent kernels, per device
-int g_first_grid[64] = {0};  // (the first-pass kernels share one occupancy)
-constexpr size_t kFirstSmem = (2048 + kTile / 4) * sizeof(uint4) + 16;
-
-template <int M>
-cudaError_t prepare_first(int* per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(fft_m31_first_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFirstSmem);
-  if (e != cudaSuccess) return e;
-  int k = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, fft_m31_first_kernel<M>, kThreads, kFirstSmem)) != cudaSuccess) return e;
-  *per_sm = *per_sm ? std::min(*per_sm, k) : k;
-  return cudaSuccess;
-}
+int g_low_grid[64] = {0};  // resident CTAs of the persistent kernel, per device
 
 }  // namespace
 
@@ -579,12 +465,6 @@ cudaError_t prepare_fft_m31_kernels() {
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_m31_low_tma_kernel, kThreads, 0)) != cudaSuccess) return e;
   if (dev >= 0 && dev < 64) g_low_grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
-  per_sm = 0;
-  if ((e = prepare_first<6>(&per_sm)) != cudaSuccess || (e = prepare_first<7>(&per_sm)) != cudaSuccess ||
-      (e = prepare_first<8>(&per_sm)) != cudaSuccess || (e = prepare_first<9>(&per_sm)) != cudaSuccess ||
-      (e = prepare_first<10>(&per_sm)) != cudaSuccess)
-    return e;
-  if (dev >= 0 && dev < 64) g_first_grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
   return cudaSuccess;
 }
 
@@ -607,23 +487,6 @@ cudaError_t launch_fft_m31_low(const FftJob* d_jobs, const uint2* d_work, uint32
   const uint32_t resident = (uint32_t)g_low_grid[dev];
   const uint32_t grid = resident && resident < nwork ? resident : nwork;
   fft_m31_low_tma_kernel<<<grid, kThreads, 0, s>>>(d_jobs, d_work, nwork, d_status);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_fft_m31_first(const FftJob* d_jobs, const uint2* d_work, uint32_t nwork, uint32_t m, uint32_t* d_status, cudaStream_t s) {
-  if (nwork == 0) return cudaSuccess;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
-  const uint32_t resident = (uint32_t)g_first_grid[dev];
-  const uint32_t grid = resident && resident < nwork ? resident : nwork;
-  switch (m) {
-    case 6: fft_m31_first_kernel<6><<<grid, kThreads, kFirstSmem, s>>>(d_jobs, d_work, nwork, d_status); break;
-    case 7: fft_m31_first_kernel<7><<<grid, kThreads, kFirstSmem, s>>>(d_jobs, d_work, nwork, d_status); break;
-    case 8: fft_m31_first_kernel<8><<<grid, kThreads, kFirstSmem, s>>>(d_jobs, d_work, nwork, d_status); break;
-    case 9: fft_m31_first_kernel<9><<<grid, kThreads, kFirstSmem, s>>>(d_jobs, d_work, nwork, d_status); break;
-    case 10: fft_m31_first_kernel<10><<<grid, kThreads, kFirstSmem, s>>>(d_jobs, d_work, nwork, d_status); break;
-    default: return cudaErrorInvalidValue;
-  }
   return cudaGetLastError();
 }
 

@@ -166,11 +166,8 @@ struct Engine {
     AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s_up));
     sync_stream(s_up);
     layout(f == 0, "input contains a non-canonical field element");
-    // lifted M31 inputs take the one-limb kernels; a prefix of at most N/4 also
-    // lets the first pass copy only the lower quarter of its rows
     std::vector<uint8_t> narrow(m);
-    for (size_t i = 0; i < m; i++)
-      narrow[i] = h[i].m31 ? ((h[i].count <= ((1ull << cfg[i].logn) >> 2)) ? kFftInM31Quarter : kFftInM31) : kFftInQM31;
+    for (size_t i = 0; i < m; i++) narrow[i] = h[i].m31 ? 1 : 0;
     set_fft_narrow(narrow);
   }
   // Inputs written by the caller through a device pointer: nothing known.

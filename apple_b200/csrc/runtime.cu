@@ -4,8 +4,6 @@
 #include <algorithm>
 #include <cstdlib>
 
-#include <cuda.h>
-
 #include "azk_field.cuh"
 #include "azk_runtime.h"
 #include "azk_tuned.h"
@@ -89,45 +87,6 @@ MemRangeFn mem_range_fn() {
 }
 }  // namespace
 
-namespace {
-// cuTensorMapEncodeTiled through the runtime's driver entry point.
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled_fn() {
-  static EncodeTiledFn fn = [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess) {
-      cudaGetLastError();
-      f = nullptr;
-    }
-    return reinterpret_cast<EncodeTiledFn>(f);
-  }();
-  return fn;
-}
-
-// Tensor map of a first FFT pass's coefficient rows: the interleaved QM31
-// coefficients (16 bytes each) as a 3-D array of 32-bit words,
-//   dim 0: the 4 * 2^c words of a tile row (2^c consecutive coefficients),
-//   dim 1: the 2^(s_lo - c) tiles that share a row set (stride 16 * 2^c bytes),
-//   dim 2: the N >> s_lo rows (stride 16 * 2^s_lo bytes),
-// copied in boxes of one tile's lower-quarter rows: {4 * 2^c, 1, 2^(m-2)}, 16 KB.
-// Element (k, mid, R) is word k of coefficient (R << s_lo) | (mid << c) | (k / 4).
-bool encode_first_pass_map(const FftJob& j, CUtensorMap* out) {
-  EncodeTiledFn fn = encode_tiled_fn();
-  if (!fn) return false;
-  const FftPassGeom g = fft_pass_geom(j.logn, 0);
-  const uint32_t c = kFftLowBits - g.m;
-  const cuuint64_t dims[3] = {4ull << c, 1ull << (g.s_lo - c), (1ull << j.logn) >> g.s_lo};
-  const cuuint64_t strides[2] = {16ull << c, 16ull << g.s_lo};
-  const cuuint32_t box[3] = {4u << c, 1u, 1u << (g.m - 2)};
-  const cuuint32_t estr[3] = {1u, 1u, 1u};
-  return fn(out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<uint4*>(j.in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-}  // namespace
-
 void azk::require_device_range(const void* p, uint64_t off, uint64_t bytes) {
   layout(p != nullptr, "null device pointer");
   const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -145,7 +104,7 @@ void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uin
   jobs.clear();
   work.clear();
   narrow.assign(transforms.size(), 0);
-  for (size_t i = 0; i < transforms.size() && i < narrow_flags.size(); i++) narrow[i] = narrow_flags[i] <= kFftInM31Quarter ? narrow_flags[i] : kFftInM31;
+  for (size_t i = 0; i < transforms.size() && i < narrow_flags.size(); i++) narrow[i] = narrow_flags[i] ? 1 : 0;
   uint32_t max_passes = 0;
   for (auto& t : transforms) max_passes = std::max(max_passes, fft_high_chunks(t.logn) + 1);
   std::array<uint64_t, kFftKinds> zero{};
@@ -154,30 +113,13 @@ void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uin
   inst_range.assign(max_passes, std::vector<std::pair<uint64_t, uint64_t>>(transforms.size(), {0, 0}));
   inst_kind.assign(max_passes, std::vector<uint8_t>(transforms.size(), 0));
   std::vector<std::vector<uint32_t>> job_at(max_passes, std::vector<uint32_t>(transforms.size(), UINT32_MAX));
-  tmap_jobs.clear();
-  h_maps.clear();
-  std::vector<uint32_t> job_kind;
   for (size_t i = 0; i < transforms.size(); i++) {
     uint32_t passes = fft_high_chunks(transforms[i].logn) + 1;
     for (uint32_t p = 0; p < passes; p++) {
       FftJob j = transforms[i];
       j.pass = p;
-      j.tmap = nullptr;
-      uint32_t kind = fft_pass_kind(j.logn, p, narrow[i]);
-      // a staged first pass needs its tensor map (over the whole N-coefficient
-      // buffer); without the driver's encoder it reads its coefficients directly
-      if (fft_kind_first(kind)) {
-        CUtensorMap map;
-        if (encode_first_pass_map(j, &map)) {
-          tmap_jobs.push_back((uint32_t)jobs.size());
-          h_maps.push_back(map);
-        } else {
-          kind = kFftM31Tile;
-        }
-      }
       job_at[max_passes - passes + p][i] = (uint32_t)jobs.size();
       jobs.push_back(j);
-      job_kind.push_back(kind);
     }
   }
   for (uint32_t step = 0; step < max_passes; step++) {
@@ -187,7 +129,7 @@ void FftPlan::build(const std::vector<FftJob>& transforms, const std::vector<uin
         uint32_t jid = job_at[step][i];
         if (jid == UINT32_MAX) continue;
         const FftJob& j = jobs[jid];
-        if (job_kind[jid] != kind) continue;
+        if (fft_pass_kind(j.logn, j.pass, narrow[i] != 0) != kind) continue;
         uint64_t tiles = fft_kind_tiles(j.logn, j.pass, kind);
         inst_range[step][i] = {work.size(), tiles};
         inst_kind[step][i] = (uint8_t)kind;
@@ -208,12 +150,6 @@ void FftPlan::upload(cudaStream_t s) {
     d_status.alloc(16, "fft status");
     AZK_CU(cudaMemsetAsync(d_status.p, 0, 16, s));
   }
-  if (!tmap_jobs.empty()) {
-    const uint64_t mb = sizeof(CUtensorMap) * tmap_jobs.size();
-    if (d_tmaps.bytes < mb) d_tmaps.alloc(mb, "fft tensor maps");
-    for (size_t k = 0; k < tmap_jobs.size(); k++) jobs[tmap_jobs[k]].tmap = d_tmaps.as<uint8_t>() + sizeof(CUtensorMap) * k;
-    AZK_CU(cudaMemcpyAsync(d_tmaps.p, h_maps.data(), mb, cudaMemcpyHostToDevice, s));
-  }
   if (!jobs.empty()) AZK_CU(cudaMemcpyAsync(d_jobs.p, jobs.data(), jobs.size() * sizeof(FftJob), cudaMemcpyHostToDevice, s));
   if (!work.empty()) AZK_CU(cudaMemcpyAsync(d_work.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
 }
@@ -233,8 +169,7 @@ void FftPlan::check_status(cudaStream_t s) {
   sync_stream(s);
   if (f) {
     AZK_CU(cudaMemsetAsync(d_status.p, 0, 4, s));
-    if (f & 1u) fail(AZK_ERR_DEVICE_TIMEOUT, "a Circle FFT pass gave up waiting for its bulk tile copies");
-    fail(AZK_ERR_COMMAND_EXECUTION_FAILED, "a staged Circle FFT first pass met a tile without its tensor map or prefix bound");
+    fail(AZK_ERR_DEVICE_TIMEOUT, "a Circle FFT pass gave up waiting for its bulk tile copies");
   }
 }
 

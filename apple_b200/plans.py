@@ -903,10 +903,11 @@ def sumcheck_prove(ctx: Context, evaluations) -> dict:
     r0, r1, ch = (np.zeros(max(1, rounds), np.uint32) for _ in range(3))
     cs, fe = ctypes.c_uint32(), ctypes.c_uint32()
     dg = np.zeros(32, np.uint8)
-    check(lib().azk_sumcheck_prove(ctx.handle, _ptr(ev), len(ev), _ptr(r0), _ptr(r1), _ptr(ch), ctypes.byref(cs), ctypes.byref(fe), _ptr(dg), None),
-          ctx.handle)
+    st = Stats()
+    check(lib().azk_sumcheck_prove(ctx.handle, _ptr(ev), len(ev), _ptr(r0), _ptr(r1), _ptr(ch), ctypes.byref(cs), ctypes.byref(fe), _ptr(dg),
+                                   ctypes.byref(st)), ctx.handle)
     return {"r0": r0[:rounds], "r1": r1[:rounds], "challenges": ch[:rounds], "claimed_sum": cs.value, "final": fe.value,
-            "initial_digest": dg.tobytes()}
+            "initial_digest": dg.tobytes(), "gpu_s": st.gpu_s, "wall_s": st.cpu_wall_s}
 
 
 def _sumcheck_words(words: np.ndarray) -> dict:
