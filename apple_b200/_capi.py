@@ -195,6 +195,8 @@ PROTOTYPES = {
     "azk_server_create": (I32, [P, U64, U32, SCHED, PP]),
     "azk_server_submit_pcs": (I32, [P, U32, U32, U32, U32, P, U64, P, U64P]),
     "azk_server_submit_sumcheck": (I32, [P, P, U64, U64P]),
+    "azk_server_submit_pcs_nocopy": (I32, [P, U32, U32, U32, U32, P, U64, P, U64P]),
+    "azk_server_submit_sumcheck_nocopy": (I32, [P, P, U64, U64P]),
     "azk_server_warm": (I32, [P, P, P, U32, U32, U32, P, U32]),
     "azk_server_poll": (I32, [P, U64, IP, ctypes.POINTER(ctypes.c_double), P, U64P]),
     "azk_server_release": (I32, [P, U64]),

@@ -28,7 +28,7 @@ cudaStream_t plan_stream() {
 }
 
 void check_canonical_host(const uint32_t* v, uint64_t words) {
-  for (uint64_t i = 0; i < words; i++) layout(v[i] < kP, "input contains a non-canonical field element");
+  layout(all_canonical(v, words), "input contains a non-canonical field element");
 }
 void check_nonzero_host(const uint32_t* v, uint64_t count) {
   for (uint64_t i = 0; i < count; i++) layout(v[4 * i] | v[4 * i + 1] | v[4 * i + 2] | v[4 * i + 3], "inverse-domain point is zero");

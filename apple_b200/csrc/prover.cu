@@ -85,6 +85,18 @@ struct Engine {
     graphs.clear();
   }
 
+  // Kept for the engine's lifetime, so a run creates and destroys nothing: the
+  // run's timing events, and page-locked words for the input scan's readbacks
+  // (two status words at 0 and 16, then the per-instance input descriptions and
+  // the scan's job list).
+  cudaEvent_t tm_a = nullptr, tm_b = nullptr;
+  HostPinned hsmall;
+  uint32_t* hword(int k) const { return reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(hsmall.p) + 16 * k); }
+  InputInfo* hinfo() const { return reinterpret_cast<InputInfo*>(static_cast<uint8_t*>(hsmall.p) + 64); }
+  ScanJob* hscan() const {
+    return reinterpret_cast<ScanJob*>(static_cast<uint8_t*>(hsmall.p) + 64 + align_up(sizeof(InputInfo) * cfg.size(), 16));
+  }
+
   // Per-stage CUDA events (profiling): stage kind 0 = FFT, 1 = tree (fold +
   // hash + transcript), 2 = final fold, 3 = transcript/queries/emission.
   bool prof = false;
@@ -99,6 +111,8 @@ struct Engine {
     drop_graphs();
     for (auto e : ev_a) cudaEventDestroy(e);
     for (auto e : ev_b) cudaEventDestroy(e);
+    if (tm_a) cudaEventDestroy(tm_a);
+    if (tm_b) cudaEventDestroy(tm_b);
     if (owns_streams && s) cudaStreamDestroy(s);
     if (owns_streams && s_up) cudaStreamDestroy(s_up);
   }
@@ -147,11 +161,12 @@ struct Engine {
   // of its engine's instances).
   void scan_inputs(const std::vector<uint64_t>& counts) {
     const size_t m = counts.size();
-    std::vector<InputInfo> h(m);
+    InputInfo* h = hinfo();
+    ScanJob* jobs = hscan();
+    uint32_t* f = hword(0);
     for (size_t i = 0; i < m; i++) h[i] = InputInfo{1u, 0u, counts[i]};
-    AZK_CU(cudaMemcpyAsync(d_info(), h.data(), sizeof(InputInfo) * h.size(), cudaMemcpyHostToDevice, s_up));
+    AZK_CU(cudaMemcpyAsync(d_info(), h, sizeof(InputInfo) * m, cudaMemcpyHostToDevice, s_up));
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s_up));
-    std::vector<ScanJob> jobs(m);
     uint64_t max_n = 0;
     for (size_t i = 0; i < m; i++) {
       const uint64_t N = 1ull << cfg[i].logn;
@@ -159,13 +174,12 @@ struct Engine {
       max_n = std::max(max_n, N);
     }
     if (!d_scan.p) d_scan.alloc(sizeof(ScanJob) * cfg.size(), "PCS.ScanJobs");
-    AZK_CU(cudaMemcpyAsync(d_scan.p, jobs.data(), sizeof(ScanJob) * jobs.size(), cudaMemcpyHostToDevice, s_up));
-    AZK_CU(launch_scan_inputs(d_scan.as<ScanJob>(), (uint32_t)jobs.size(), max_n, d_flag(), s_up));
-    uint32_t f = 0;
-    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s_up));
-    AZK_CU(cudaMemcpyAsync(h.data(), d_info(), sizeof(InputInfo) * h.size(), cudaMemcpyDeviceToHost, s_up));
+    AZK_CU(cudaMemcpyAsync(d_scan.p, jobs, sizeof(ScanJob) * m, cudaMemcpyHostToDevice, s_up));
+    AZK_CU(launch_scan_inputs(d_scan.as<ScanJob>(), (uint32_t)m, max_n, d_flag(), s_up));
+    AZK_CU(cudaMemcpyAsync(f, d_flag(), 4, cudaMemcpyDeviceToHost, s_up));
+    AZK_CU(cudaMemcpyAsync(h, d_info(), sizeof(InputInfo) * m, cudaMemcpyDeviceToHost, s_up));
     sync_stream(s_up);
-    layout(f == 0, "input contains a non-canonical field element");
+    layout(*f == 0, "input contains a non-canonical field element");
     std::vector<uint8_t> narrow(m);
     for (size_t i = 0; i < m; i++) narrow[i] = h[i].m31 ? 1 : 0;
     set_fft_narrow(narrow);
@@ -227,6 +241,9 @@ struct Engine {
       AZK_CU(cudaStreamCreateWithPriority(&s_up, cudaStreamNonBlocking, prio_hi));
     }
     size_t n = cfg.size();
+    if (!tm_a) AZK_CU(cudaEventCreateWithFlags(&tm_a, cudaEventBlockingSync));
+    if (!tm_b) AZK_CU(cudaEventCreateWithFlags(&tm_b, cudaEventBlockingSync));
+    hsmall.ensure(64 + align_up(sizeof(InputInfo) * n, 16) + sizeof(ScanJob) * n);
     leaf_values = cfg.empty() ? 1 : cfg[0].leaf_values;
     for (auto& i : cfg) {
       layout(i.leaf_values == leaf_values && (leaf_values == 1 || leaf_values == 4), "all instances of a batch share one leaf size (16 or 64 bytes)");
@@ -534,7 +551,7 @@ struct Engine {
   // Run the whole superstep; returns device seconds.
   double run(bool from_coeffs, bool plain, uint64_t* submit_ns, const Timer& t) {
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
-    GpuTimer g(s);
+    GpuTimer g(s, tm_a, tm_b);
     if (plain) {
       ev_used = 0;
       for (uint32_t i = 0; i < active(); i++) enqueue_instance(i, from_coeffs);
@@ -572,10 +589,10 @@ struct Engine {
   void check_input_canonical(const void* dptr, uint64_t words) {
     AZK_CU(cudaMemsetAsync(d_flag(), 0, 4, s));
     AZK_CU(launch_check_canonical(static_cast<const uint32_t*>(dptr), words, d_flag(), s));
-    uint32_t f = 0;
-    AZK_CU(cudaMemcpyAsync(&f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
+    uint32_t* f = hword(1);
+    AZK_CU(cudaMemcpyAsync(f, d_flag(), 4, cudaMemcpyDeviceToHost, s));
     sync_stream(s);
-    layout(f == 0, "input contains a non-canonical field element");
+    layout(*f == 0, "input contains a non-canonical field element");
   }
 
   void trace(uint32_t i, uint8_t* cm, uint32_t* ch, uint32_t* fl, uint32_t* qp) {
@@ -997,9 +1014,11 @@ struct ServeJob {
   uint64_t id = 0;
   int kind = 0;  // 0 pcs, 1 sumcheck
   uint32_t logn = 0, rounds = 0, queries = 0, log_blowup = 0;
-  std::vector<uint32_t> input;  // pcs: coefficient words; sumcheck: evaluations
-  uint64_t count = 0;           // pcs: coefficient count
-  bool zeros = false;           // warm-up job: `count` zero coefficients, no `input`
+  std::vector<uint32_t> input;        // pcs: coefficient words; sumcheck: evaluations
+  const uint32_t* borrowed = nullptr;  // the caller's words instead of `input` (no-copy submission)
+  uint64_t count = 0;                 // pcs: coefficient count
+  bool zeros = false;                 // warm-up job: `count` zero coefficients, no `input`
+  uint32_t warm_group = 1;            // warm-up job: proved as a group of this many copies
   uint8_t pub[32] = {0};
   std::chrono::steady_clock::time_point submitted, started, finished;
   int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
@@ -1010,6 +1029,15 @@ struct ServeJob {
 using ShapeKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>;  // PCS: logn, rounds, queries, log_blowup
 
 ShapeKey shape_of(const ServeJob& j) { return std::make_tuple(j.logn, j.rounds, j.queries, j.log_blowup); }
+
+const uint32_t* job_words(const ServeJob& j) { return j.borrowed ? j.borrowed : j.input.data(); }
+// Once a job's words are in page-locked staging nothing reads them again: its copy
+// goes back to the allocator (so the next submission reuses warm pages) and a
+// borrowed pointer is forgotten.  Only the thread that holds the job calls this.
+void drop_input(ServeJob& j) {
+  std::vector<uint32_t>().swap(j.input);
+  j.borrowed = nullptr;
+}
 
 // Jobs of one shape proved together, at most: 8 up to 2^17 values, then halving
 // (4 at 2^18, 2 at 2^19), one from 2^20 on, where one job already fills the GPU's
@@ -1085,7 +1113,7 @@ struct SumcheckStream {
   cudaStream_t s = nullptr;
   std::vector<int> slots;
 };
-constexpr int kLaneSlots = 96;                 // tables in the lane at once
+constexpr int kLaneSlots = 256;  // tables in the lane at once (a packed CTA runs four, one per SM sub-partition)
 constexpr int kLaneStreams = 32;               // batches in flight at once
 constexpr int kLaneBatch = kSumcheckBatchMax;  // tables per launch
 
@@ -1099,6 +1127,7 @@ struct azk_server {
   std::mutex mu;
   std::condition_variable cv, done_cv, lane_cv;
   std::deque<std::shared_ptr<ServeJob>> queue;
+  uint64_t queued_sc = 0;  // sum-check jobs in `queue`
   std::unordered_map<uint64_t, std::shared_ptr<ServeJob>> jobs;
   uint64_t next_id = 1;
   uint64_t held = 0;  // device bytes held (engines, lane slots, domain tables)
@@ -1167,7 +1196,8 @@ void run_pcs_group(azk_server* sv, Resident& r, std::vector<std::shared_ptr<Serv
     if (g[i]->zeros)
       std::memset(pin + off[i], 0, 16 * counts[i]);
     else
-      std::memcpy(pin + off[i], g[i]->input.data(), 16 * counts[i]);
+      std::memcpy(pin + off[i], job_words(*g[i]), 16 * counts[i]);
+    drop_input(*g[i]);
     AZK_CU(cudaMemcpyAsync(e->arena.at<uint4>(e->off_input[i]), pin + off[i], 16 * counts[i], cudaMemcpyHostToDevice, e->s_up));
   }
   e->scan_inputs(counts);  // waits for the copies
@@ -1180,7 +1210,7 @@ void run_pcs_group(azk_server* sv, Resident& r, std::vector<std::shared_ptr<Serv
   for (size_t i = 0; i < m; i++)
     AZK_CU(cudaMemcpyAsync(pin + i * align_up(proof, 64), e->h_inst[i].proof, proof, cudaMemcpyDeviceToHost, e->s));
   sync_stream(e->s);
-  e->fft.check_status(e->s);
+  e->fft.check_status(e->s, e->hword(1));
   for (size_t i = 0; i < m; i++) g[i]->result.assign(pin + i * align_up(proof, 64), pin + i * align_up(proof, 64) + proof);
 }
 
@@ -1320,15 +1350,22 @@ bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
     sv->warm[w].pop_front();
     sv->busy[w] = 1;
     j->state = 1;
-    tk.group = {j};
+    tk.group.assign(std::max<uint32_t>(1, std::min(j->warm_group, cache[key].cap)), j);
     tk.warm = true;
     return true;
   }
   if (sv->queue.empty()) return false;
-  // the front job; when it is a sum-check and every lane slot holds a table, the
-  // first queued proof job instead (a full lane never holds proof jobs back)
+  // A sum-check costs its worker only a copy into a lane slot, then runs for tens
+  // of milliseconds on one warp beside the proofs: while the lane has a free slot,
+  // the first queued sum-check goes ahead of the proof jobs, so its digest overlaps
+  // them instead of starting after them.  Otherwise the front job; when that is a
+  // sum-check and every lane slot holds a table, the first queued proof job (a full
+  // lane never holds proof jobs back).
   auto pick = sv->queue.begin();
-  if ((*pick)->kind == 1 && sv->sc_free.empty()) {
+  if (!sv->sc_free.empty() && sv->queued_sc > 0) {
+    while (pick != sv->queue.end() && (*pick)->kind != 1) ++pick;
+    if (pick == sv->queue.end()) pick = sv->queue.begin();
+  } else if ((*pick)->kind == 1) {
     while (pick != sv->queue.end() && (*pick)->kind == 1) ++pick;
     if (pick == sv->queue.end()) return false;
   }
@@ -1352,6 +1389,7 @@ bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
     }
     sl.job = j;
     sv->queue.erase(pick);
+    sv->queued_sc--;
     sv->running++;
     sv->busy[w] = 1;
     j->state = 1;
@@ -1404,8 +1442,7 @@ void publish(azk_server* sv, ServeJob& j, int outcome, const std::string& error)
   j.error = error;
   j.state = outcome;
   j.finished = std::chrono::steady_clock::now();
-  j.input.clear();
-  j.input.shrink_to_fit();
+  drop_input(j);
   sv->running--;
   sv->completed++;
   if (j.kind == 0 && outcome == 2) sv->elems += 1ull << j.logn;
@@ -1425,7 +1462,8 @@ void lane_submit(azk_server* sv, int slot) {
     if (j.zeros)
       std::memset(pin, 0, 4ull << j.logn);
     else
-      std::memcpy(pin, j.input.data(), 4ull << j.logn);
+      std::memcpy(pin, job_words(j), 4ull << j.logn);
+    drop_input(j);
   } catch (const Error& e) {
     error = e.msg;
   } catch (const std::exception& e) {
@@ -1674,8 +1712,49 @@ uint64_t submit(azk_server* sv, std::shared_ptr<ServeJob> j, uint64_t bytes) {
   }
   sv->jobs[j->id] = j;
   sv->queue.push_back(j);
+  if (j->kind == 1) sv->queued_sc++;
   sv->cv.notify_all();
   return j->id;
+}
+
+// The submission entry points: arguments checked (a non-canonical word is refused
+// here, before the job is queued), then the words copied into the job or, with
+// `borrow`, only their address kept: the worker that takes the job reads them into
+// its page-locked staging.
+uint64_t submit_pcs(azk_server* sv, uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t rounds, const uint32_t* coeffs,
+                    uint64_t count, const uint8_t pub[32], const uint64_t* job_id, bool borrow) {
+  layout(sv && coeffs && pub && job_id);
+  validate_params(logn, log_blowup, queries, 0, rounds);
+  layout(count >= 1 && count <= (1ull << logn));
+  layout(all_canonical(coeffs, 4 * count), "input contains a non-canonical field element");
+  auto j = std::make_shared<ServeJob>();
+  j->kind = 0;
+  j->logn = logn;
+  j->rounds = rounds;
+  j->queries = queries;
+  j->log_blowup = log_blowup;
+  if (borrow)
+    j->borrowed = coeffs;
+  else
+    j->input.assign(coeffs, coeffs + 4 * count);
+  j->count = count;
+  std::memcpy(j->pub, pub, 32);
+  return submit(sv, j, pcs_engine_bytes(logn, rounds, queries, 1) + domain_bytes(logn));
+}
+
+uint64_t submit_sumcheck(azk_server* sv, const uint32_t* evals, uint64_t count, const uint64_t* job_id, bool borrow) {
+  layout(sv && evals && job_id);
+  // M31MultilinearSumcheckProofBuilderV1.prove preconditions (SumcheckOracle.swift:803-807)
+  layout(count > 1 && is_pow2(count) && count <= (1ull << 28));
+  layout(all_canonical(evals, count), "input contains a non-canonical field element");
+  auto j = std::make_shared<ServeJob>();
+  j->kind = 1;
+  j->logn = ilog2(count);
+  if (borrow)
+    j->borrowed = evals;
+  else
+    j->input.assign(evals, evals + count);
+  return submit(sv, j, sumcheck_table_bytes(j->logn));
 }
 
 }  // namespace
@@ -1688,7 +1767,7 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evals, uint64_t coun
     layout(ctx && evals && sums0 && sums1 && challenges && claimed_sum && final_eval && digest);
     // preconditions of M31MultilinearSumcheckProofBuilderV1.prove (SumcheckOracle.swift:803-807)
     layout(count > 1 && is_pow2(count) && count <= (1ull << 28), "evaluation count must be a power of two greater than one");
-    for (uint64_t i = 0; i < count; i++) layout(evals[i] < kP, "input contains a non-canonical field element");
+    layout(all_canonical(evals, count), "input contains a non-canonical field element");
     std::lock_guard<std::mutex> lk(ctx->mu);
     Timer t;
     uint32_t logn = ilog2(count);
@@ -1753,22 +1832,12 @@ azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t s
 
 azk_status azk_server_submit_pcs(azk_server* sv, uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t rounds, const uint32_t* coeffs,
                                  uint64_t count, const uint8_t pub[32], uint64_t* job_id) {
-  return guarded(sv ? sv->ctx : nullptr, [&] {
-    layout(sv && coeffs && pub && job_id);
-    validate_params(logn, log_blowup, queries, 0, rounds);
-    layout(count >= 1 && count <= (1ull << logn));
-    for (uint64_t i = 0; i < 4 * count; i++) layout(coeffs[i] < kP, "input contains a non-canonical field element");
-    auto j = std::make_shared<ServeJob>();
-    j->kind = 0;
-    j->logn = logn;
-    j->rounds = rounds;
-    j->queries = queries;
-    j->log_blowup = log_blowup;
-    j->input.assign(coeffs, coeffs + 4 * count);
-    j->count = count;
-    std::memcpy(j->pub, pub, 32);
-    *job_id = submit(sv, j, pcs_engine_bytes(logn, rounds, queries, 1) + domain_bytes(logn));
-  });
+  return guarded(sv ? sv->ctx : nullptr, [&] { *job_id = submit_pcs(sv, logn, log_blowup, queries, rounds, coeffs, count, pub, job_id, false); });
+}
+
+azk_status azk_server_submit_pcs_nocopy(azk_server* sv, uint32_t logn, uint32_t log_blowup, uint32_t queries, uint32_t rounds,
+                                        const uint32_t* coeffs, uint64_t count, const uint8_t pub[32], uint64_t* job_id) {
+  return guarded(sv ? sv->ctx : nullptr, [&] { *job_id = submit_pcs(sv, logn, log_blowup, queries, rounds, coeffs, count, pub, job_id, true); });
 }
 
 azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint32_t* pcs_rounds, uint32_t n_pcs, uint32_t log_blowup,
@@ -1819,19 +1888,32 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
     std::unique_lock<std::mutex> lk(sv->mu);
     for (uint32_t w = 0; w < sv->slots; w++) {
       for (uint32_t i = 0; i < n_pcs; i++) {
-        auto j = std::make_shared<ServeJob>();  // id 0: a warm-up job
-        j->kind = 0;
-        j->logn = pcs_logn[i];
-        j->rounds = pcs_rounds[i];
-        j->queries = queries;
-        j->log_blowup = log_blowup;
-        // all 2^logn coefficients (zeros): the worker's pinned staging grows to a
-        // full group of the shape's largest inputs now, not in the middle of
-        // serving, where freeing the smaller buffer would wait for the whole device
-        j->zeros = true;
-        j->count = 1ull << j->logn;
-        sv->warm[w].push_back(j);
-        sv->warm_pending++;
+        ServeJob shape;
+        shape.logn = pcs_logn[i];
+        shape.rounds = pcs_rounds[i];
+        shape.queries = queries;
+        shape.log_blowup = log_blowup;
+        // one group of each size the shape can take: a group size's first run
+        // builds the engine's FFT work lists for it (device allocations) and
+        // captures its graph, and either, in the middle of serving, waits for the
+        // whole device, long sum-check kernels included
+        const uint32_t cap = shape_capacity(sv, shape);
+        for (uint32_t m = cap; m >= 1; m--) {
+          auto j = std::make_shared<ServeJob>();  // id 0: a warm-up job
+          j->kind = 0;
+          j->logn = shape.logn;
+          j->rounds = shape.rounds;
+          j->queries = queries;
+          j->log_blowup = log_blowup;
+          j->warm_group = m;
+          // all 2^logn coefficients (zeros): the worker's pinned staging grows to a
+          // full group of the shape's largest inputs now, not in the middle of
+          // serving, where freeing the smaller buffer would wait for the whole device
+          j->zeros = true;
+          j->count = 1ull << j->logn;
+          sv->warm[w].push_back(j);
+          sv->warm_pending++;
+        }
       }
     }
     // one table of zeros per listed size through the lane (kernels loaded before serving)
@@ -1841,6 +1923,7 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
       j->logn = lg;
       j->zeros = true;
       sv->queue.push_front(j);
+      sv->queued_sc++;
       sv->warm_pending++;
     }
     sv->cv.notify_all();
@@ -1849,17 +1932,11 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
 }
 
 azk_status azk_server_submit_sumcheck(azk_server* sv, const uint32_t* evals, uint64_t count, uint64_t* job_id) {
-  return guarded(sv ? sv->ctx : nullptr, [&] {
-    layout(sv && evals && job_id);
-    // M31MultilinearSumcheckProofBuilderV1.prove preconditions (SumcheckOracle.swift:803-807)
-    layout(count > 1 && is_pow2(count) && count <= (1ull << 28));
-    for (uint64_t i = 0; i < count; i++) layout(evals[i] < kP, "input contains a non-canonical field element");
-    auto j = std::make_shared<ServeJob>();
-    j->kind = 1;
-    j->logn = ilog2(count);
-    j->input.assign(evals, evals + count);
-    *job_id = submit(sv, j, sumcheck_table_bytes(j->logn));
-  });
+  return guarded(sv ? sv->ctx : nullptr, [&] { *job_id = submit_sumcheck(sv, evals, count, job_id, false); });
+}
+
+azk_status azk_server_submit_sumcheck_nocopy(azk_server* sv, const uint32_t* evals, uint64_t count, uint64_t* job_id) {
+  return guarded(sv ? sv->ctx : nullptr, [&] { *job_id = submit_sumcheck(sv, evals, count, job_id, true); });
 }
 
 azk_status azk_server_poll(azk_server* sv, uint64_t id, int* state, double* latency_s, uint8_t* out, uint64_t* out_len) {

@@ -162,12 +162,13 @@ void FftPlan::launch_step_for(size_t step, size_t t, cudaStream_t s) const {
   auto r = inst_range[step][t];
   AZK_CU(launch_fft_pass(d_jobs.as<FftJob>(), d_work.as<uint2>() + r.first, (uint32_t)r.second, inst_kind[step][t], d_status.as<uint32_t>(), s));
 }
-void FftPlan::check_status(cudaStream_t s) {
+void FftPlan::check_status(cudaStream_t s, uint32_t* host_word) {
   if (!d_status.p) return;
-  uint32_t f = 0;
-  AZK_CU(cudaMemcpyAsync(&f, d_status.p, 4, cudaMemcpyDeviceToHost, s));
+  uint32_t local = 0;
+  uint32_t* f = host_word ? host_word : &local;
+  AZK_CU(cudaMemcpyAsync(f, d_status.p, 4, cudaMemcpyDeviceToHost, s));
   sync_stream(s);
-  if (f) {
+  if (*f) {
     AZK_CU(cudaMemsetAsync(d_status.p, 0, 4, s));
     fail(AZK_ERR_DEVICE_TIMEOUT, "a Circle FFT pass gave up waiting for its bulk tile copies");
   }
@@ -230,8 +231,8 @@ std::vector<Q> line_basis(const uint32_t* m, uint64_t count, uint64_t capacity) 
 std::vector<uint32_t> azk::fft_basis_from_monomials(uint32_t logn, const uint32_t* x, uint64_t nx, const uint32_t* y, uint64_t ny) {
   uint64_t half = 1ull << (logn - 1);
   layout(nx <= half && ny <= half && (nx || ny));
-  for (uint64_t i = 0; i < 4 * nx; i++) layout(x[i] < kP);
-  for (uint64_t i = 0; i < 4 * ny; i++) layout(y[i] < kP);
+  layout(all_canonical(x, 4 * nx));
+  layout(all_canonical(y, 4 * ny));
   auto xl = line_basis(x, nx, half), yl = line_basis(y, ny, half);
   std::vector<uint32_t> out(8 * half);
   for (uint64_t i = 0; i < half; i++) {
@@ -909,7 +910,7 @@ azk_status azk_codeword_plan_execute(azk_codeword_plan* p, const uint32_t* coeff
     layout(p && codeword && (coeffs || !count));
     uint64_t n = 1ull << p->logn;
     layout(count <= n);
-    for (uint64_t i = 0; i < 4 * count; i++) layout(coeffs[i] < kP);
+    layout(all_canonical(coeffs, 4 * count));
     std::lock_guard<std::mutex> lk(p->mu);
     Timer t;
     if (count) AZK_CU(cudaMemcpyAsync(p->coeff.p, coeffs, 16 * count, cudaMemcpyHostToDevice, p->s));
@@ -937,8 +938,8 @@ azk_status azk_codeword_plan_execute_polynomial(azk_codeword_plan* p, const uint
     }
     const uint64_t half = (1ull << p->logn) / 2;
     layout(nx <= half && ny <= half, "each coefficient column holds at most half the domain size");
-    for (uint64_t i = 0; i < 4 * nx; i++) layout(x[i] < kP, "input contains a non-canonical field element");
-    for (uint64_t i = 0; i < 4 * ny; i++) layout(y[i] < kP, "input contains a non-canonical field element");
+    layout(all_canonical(x, 4 * nx), "input contains a non-canonical field element");
+    layout(all_canonical(y, 4 * ny), "input contains a non-canonical field element");
     std::lock_guard<std::mutex> lk(p->mu);
     AZK_CU(cudaSetDevice(p->ctx->device));
     Timer t;
@@ -1082,7 +1083,7 @@ void azk_witness_plan_destroy(azk_witness_plan* p) { delete p; }
 
 // ---- folds ----
 static void check_qm31(const uint32_t* v, uint64_t words) {
-  for (uint64_t i = 0; i < words; i++) layout(v[i] < kP);
+  layout(all_canonical(v, words));
 }
 
 azk_status azk_qm31_fold(azk_ctx* ctx, const uint32_t* ev, uint64_t n, const uint32_t* inv, const uint32_t ch[4], uint32_t* out, azk_stats* st) {

@@ -2,30 +2,17 @@
 // SumcheckOracle.swift:797-868; statement digest :743-754; word digest :1288-1299;
 // transcript frames :1066-1106).
 //
-// One CTA of 256 threads per table.  The statement's word digest is one
-// sequential sponge over the table, so it runs on one warp (the state spread over
-// the warp's lanes) while the CTA's other warps wait; then the block proves the
-// rounds.  A table of 2^20 words is 4 MiB, so each round is a few microseconds of
-// one SM; keeping the rounds in one CTA needs no grid-wide wait and lets many jobs
-// share the GPU.
+// A table is proved by one group of warps: one warp computes the statement's word
+// digest, a sequential sponge over the whole table (about 30,000 dependent
+// permutations for 2^20 words), while the group's other warps sum the table for
+// round 0; then the group proves the rounds.  A table of 2^20 words is 4 MiB, so
+// each round is a few microseconds of one SM, and keeping a table in one group
+// needs no grid-wide wait.  The single-table kernel is one CTA of 8 warps; the
+// batched kernel packs four tables into one CTA (sumcheck_packed_kernel).
 #include "azk_field.cuh"
 #include "azk_internal.h"
 
 namespace azk {
-
-__device__ __forceinline__ uint32_t block_sum_m31(uint32_t v, uint32_t* red) {
-  // warp tree then one warp over the warp sums (values < 2^31, sums reduced each step)
-  for (int o = 16; o > 0; o >>= 1) v = m31_add(v, __shfl_down_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  uint32_t w = 0;
-  if (threadIdx.x < 32) {
-    w = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0u;
-    for (int o = 16; o > 0; o >>= 1) w = m31_add(w, __shfl_down_sync(0xffffffffu, w, o));
-  }
-  __syncthreads();
-  return w;  // valid in thread 0
-}
 
 __device__ void sc_frame(FrameBuf& f, uint8_t type) {
   const char dom[] = "AppleZKProver.M31MultilinearSumcheck";
@@ -142,10 +129,10 @@ struct BlockWords {
   __device__ __forceinline__ uint64_t word() const { return ((uint64_t)w0 >> 16) | ((uint64_t)w1 << 16) | ((uint64_t)w2 << 48); }
 };
 
-// SHA3-256 of the framed table, by the whole warp; lanes 0..3 return the digest lanes.
-__device__ uint64_t digest_words_warp(const uint32_t* words, uint64_t count) {
+// SHA3-256 of the framed table, by the whole warp (`col`: its 64-word shared
+// exchange array, 16-byte aligned); lanes 0..3 return the digest lanes.
+__device__ uint64_t digest_words_warp(const uint32_t* words, uint64_t count, uint64_t* col) {
   const uint32_t lane = threadIdx.x & 31;
-  __shared__ __align__(16) uint64_t col[64];
   const WarpKeccak kf(lane, col);
   const uint64_t total = 50 + 4 * count;
   uint64_t a = 0;
@@ -205,47 +192,92 @@ __device__ __forceinline__ void pair_sums(const uint4* __restrict__ q, uint64_t 
   }
 }
 
-// One table on one CTA.  Warp 0 computes the statement's word digest while the
-// other warps sum the table's even and odd entries (round 0's two sums; together
-// the claimed sum), which need no challenge.  Then each round is a transcript
-// round by thread 0 (round frame, challenge frame, squeeze one word mod p) and
-// one pass over the table that folds it, t'[i] = (1 - r) t[2i] + r t[2i+1], and
-// sums the folded table's even and odd entries for the next round, so after the
-// digest the table is read once per round.  One launch per table (or per batch of
-// tables, one CTA each) leaves no launch in the stream waiting behind the digest,
-// so a stream that shares a hardware work queue with others never holds that
-// queue for the digest's duration.
-__device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch, SumcheckOut* __restrict__ out) {
-  __shared__ uint32_t red[32];
-  __shared__ uint32_t s_ch;
-  __shared__ uint64_t s_digest[4];
+// The threads that prove one table.  CtaGroup: a whole CTA (the single-table
+// kernel).  PackedGroup: warps g, g + 4, g + 8, g + 12 of a 16-warp CTA, which
+// the SM places on one sub-partition, with named barrier g + 1.
+struct CtaGroup {
+  __device__ uint32_t tid() const { return threadIdx.x; }
+  __device__ uint32_t size() const { return blockDim.x; }
+  __device__ void sync() const { __syncthreads(); }
+};
+constexpr uint32_t kPackedTables = 4;  // tables per packed CTA, one per sub-partition
+constexpr uint32_t kPackedWarps = 4;   // warps per packed table
+struct PackedGroup {
+  uint32_t g;
+  __device__ uint32_t tid() const { return (threadIdx.x >> 7) * 32 + (threadIdx.x & 31); }
+  __device__ uint32_t size() const { return 32 * kPackedWarps; }
+  __device__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(32 * kPackedWarps) : "memory"); }
+};
+
+// A group's shared scratch: the digest warp's exchange arrays, per-warp partial
+// sums, the broadcast challenge and the digest.
+struct SumcheckShared {
+  __align__(16) uint64_t col[64];
+  uint32_t red[2][32];
+  uint32_t ch;
+  uint64_t digest[4];
+};
+
+// Sum of v over the group, valid in the group's thread 0 (values < 2^31, reduced
+// at every step).  Two arrays alternate, so one barrier per call suffices: thread
+// 0 reads a call's array before it reaches the next call's barrier, which every
+// writer of the call after that must pass first.
+template <class G>
+__device__ __forceinline__ uint32_t group_sum_m31(const G& grp, uint32_t v, uint32_t (&red)[2][32], uint32_t& parity) {
+  for (int o = 16; o > 0; o >>= 1) v = m31_add(v, __shfl_down_sync(0xffffffffu, v, o));
+  const uint32_t t = grp.tid();
+  uint32_t* r = red[parity];
+  parity ^= 1u;
+  if ((t & 31) == 0) r[t >> 5] = v;
+  grp.sync();
+  uint32_t w = 0;
+  if (t == 0)
+    for (uint32_t k = 0; k < (grp.size() >> 5); k++) w = m31_add(w, r[k]);
+  return w;
+}
+
+// One table on one group.  The group's first warp computes the statement's word
+// digest while its other warps sum the table's even and odd entries (round 0's
+// two sums; together the claimed sum), which need no challenge.  Then each round
+// is a transcript round by the group's thread 0 (round frame, challenge frame,
+// squeeze one word mod p) and one pass over the table that folds it,
+// t'[i] = (1 - r) t[2i] + r t[2i+1], and sums the folded table's even and odd
+// entries for the next round, so after the digest the table is read once per
+// round.  One launch per table (or per batch of tables) leaves no launch in the
+// stream waiting behind the digest, so a stream that shares a hardware work queue
+// with others never holds that queue for the digest's duration.
+template <class G>
+__device__ void sumcheck_prove_group(const G& grp, SumcheckShared& sh, const uint32_t* __restrict__ evals, uint32_t log_n,
+                                     uint32_t* __restrict__ scratch, SumcheckOut* __restrict__ out) {
   const uint64_t n = 1ull << log_n;
-  const uint32_t t = threadIdx.x;
+  const uint32_t t = grp.tid(), nt = grp.size();
+  uint32_t parity = 0;
   uint32_t z = 0, o = 0;
   if (t < 32) {
-    const uint64_t d = digest_words_warp(evals, n);
-    if (t < 4) s_digest[t] = d;
+    const uint64_t d = digest_words_warp(evals, n, sh.col);
+    if (t < 4) sh.digest[t] = d;
   } else if (n >= 4) {
-    pair_sums(reinterpret_cast<const uint4*>(evals), n >> 2, t - 32, blockDim.x - 32, z, o);
+    pair_sums(reinterpret_cast<const uint4*>(evals), n >> 2, t - 32, nt - 32, z, o);
   } else if (n == 2 && t == 32) {
     z = evals[0];
     o = evals[1];
   }
-  uint32_t zs = block_sum_m31(z, red);
-  uint32_t os = block_sum_m31(o, red);
-  // block_sum_m31's value is valid in thread 0, which alone runs the transcript
-  const uint32_t total = n == 1 ? evals[0] : m31_add(zs, os);
+  uint32_t zs = group_sum_m31(grp, z, sh.red, parity);
+  uint32_t os = group_sum_m31(grp, o, sh.red, parity);
+  // group_sum_m31's value is valid in thread 0, which alone runs the transcript
+  // (the digest lanes are visible to it after the first sum's barrier)
+  const uint32_t total = m31_add(zs, os);
   Transcript tr;
   if (t == 0) {
     out->claimed_sum = total;
-    for (int i = 0; i < 4; i++) out->digest[i] = s_digest[i];
+    for (int i = 0; i < 4; i++) out->digest[i] = sh.digest[i];
     tr_reset(tr);
     FrameBuf f;
     sc_frame(f, 0);
     fb_u64(f, n);
     fb_u32(f, log_n);
     fb_u32(f, total);
-    for (int i = 0; i < 4; i++) fb_u64(f, s_digest[i]);
+    for (int i = 0; i < 4; i++) fb_u64(f, sh.digest[i]);
     tr_absorb(tr, f.b, f.n);
   }
   const uint32_t* cur = evals;
@@ -276,10 +308,10 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
       uint32_t c;
       tr_squeeze_u32(tr, 1, kP, &c);
       chs[r] = c;
-      s_ch = c;
+      sh.ch = c;
     }
-    __syncthreads();
-    const uint32_t c = s_ch;
+    grp.sync();
+    const uint32_t c = sh.ch;
     const uint32_t omc = m31_sub(1, c);
     uint32_t* nxt = bufs[r & 1];
     z = 0;
@@ -289,16 +321,16 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
       const uint4* q = reinterpret_cast<const uint4*>(cur);
       uint2* w = reinterpret_cast<uint2*>(nxt);
       const uint64_t quarter = half >> 1;
-      for (uint64_t j = t; j < quarter; j += 8 * (uint64_t)blockDim.x) {
+      for (uint64_t j = t; j < quarter; j += 8 * (uint64_t)nt) {
         uint4 v[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-          const uint64_t jj = j + (uint64_t)k * blockDim.x;
+          const uint64_t jj = j + (uint64_t)k * nt;
           v[k] = jj < quarter ? q[jj] : make_uint4(0u, 0u, 0u, 0u);
         }
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-          const uint64_t jj = j + (uint64_t)k * blockDim.x;
+          const uint64_t jj = j + (uint64_t)k * nt;
           const uint32_t e = m31_add(m31_mul(omc, v[k].x), m31_mul(c, v[k].y));
           const uint32_t d = m31_add(m31_mul(omc, v[k].z), m31_mul(c, v[k].w));
           if (jj < quarter) {
@@ -311,23 +343,36 @@ __device__ void sumcheck_prove_block(const uint32_t* __restrict__ evals, uint32_
     } else if (t == 0) {
       nxt[0] = m31_add(m31_mul(omc, cur[0]), m31_mul(c, cur[1]));
     }
-    zs = block_sum_m31(z, red);  // synchronises: nxt is complete
-    os = block_sum_m31(o, red);
+    // the sums' barriers also complete nxt (and order this round's reads of sh.ch
+    // before the next round's write)
+    zs = group_sum_m31(grp, z, sh.red, parity);
+    os = group_sum_m31(grp, o, sh.red, parity);
     cur = nxt;
   }
   if (t == 0) out->final_eval = cur[0];
 }
 
 constexpr int kSumcheckThreads = 256;
+constexpr int kPackedThreads = 32 * kPackedTables * kPackedWarps;
 
 __global__ void __launch_bounds__(kSumcheckThreads) sumcheck_kernel(const uint32_t* __restrict__ evals, uint32_t log_n, uint32_t* __restrict__ scratch,
                                                                   SumcheckOut* __restrict__ out) {
-  sumcheck_prove_block(evals, log_n, scratch, out);
+  __shared__ SumcheckShared sh;
+  sumcheck_prove_group(CtaGroup{}, sh, evals, log_n, scratch, out);
 }
 
-__global__ void __launch_bounds__(kSumcheckThreads) sumcheck_batch_kernel(const __grid_constant__ SumcheckBatch batch) {
-  const SumcheckJob& j = batch.job[blockIdx.x];
-  sumcheck_prove_block(j.evals, j.log_n, j.scratch, j.out);
+// Up to four tables per CTA, table g on warps g, g + 4, g + 8, g + 12: the SM
+// places a CTA's warps on its four sub-partitions in turn, so the four digest
+// warps get a sub-partition each, beside only their own table's three summing
+// warps (which wait at the first barrier once round 0's sums are done), never
+// beside another of the CTA's digests.
+__global__ void __launch_bounds__(kPackedThreads, 1) sumcheck_packed_kernel(const __grid_constant__ SumcheckBatch batch, uint32_t count) {
+  __shared__ SumcheckShared sh[kPackedTables];
+  const uint32_t g = (threadIdx.x >> 5) & (kPackedTables - 1);
+  const uint32_t k = blockIdx.x * kPackedTables + g;
+  if (k >= count) return;  // the group's warps all leave; no other group waits on them
+  const SumcheckJob& j = batch.job[k];
+  sumcheck_prove_group(PackedGroup{g}, sh[g], j.evals, j.log_n, j.scratch, j.out);
 }
 
 cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scratch, SumcheckOut* out, cudaStream_t s) {
@@ -338,7 +383,7 @@ cudaError_t launch_sumcheck(const uint32_t* evals, uint32_t log_n, uint32_t* scr
 cudaError_t launch_sumcheck_batch(const SumcheckBatch& batch, uint32_t count, cudaStream_t s) {
   if (!count) return cudaSuccess;
   if (count > kSumcheckBatchMax) return cudaErrorInvalidValue;
-  sumcheck_batch_kernel<<<count, kSumcheckThreads, 0, s>>>(batch);
+  sumcheck_packed_kernel<<<(count + kPackedTables - 1) / kPackedTables, kPackedThreads, 0, s>>>(batch, count);
   return cudaGetLastError();
 }
 

@@ -923,12 +923,17 @@ class ProofServer:
     their device memory fits the HBM budget; a job larger than the whole budget
     raises AZKError(hbmBudget) at submission.  `poll` returns None while a
     job is queued or running, else (result, latency_seconds): proof bytes for a
-    PCS job, a dict like `sumcheck_prove`'s for a sum-check job."""
+    PCS job, a dict like `sumcheck_prove`'s for a sum-check job.
+
+    `copy=False` on a submission hands the array to the server without copying it
+    (azk_server_submit_*_nocopy): the server keeps a reference to it until `poll`
+    sees the job finished, and the caller must not change it meanwhile."""
 
     def __init__(self, ctx: Context, hbm_budget_bytes: int, slots: int = 4, schedule=None):
         self.ctx = ctx
         self._h = _vp()
         self._kind = {}
+        self._borrowed = {}  # job id -> the array a no-copy submission reads
         check(lib().azk_server_create(ctx.handle, int(hbm_budget_bytes), int(slots), _sched(schedule), ctypes.byref(self._h)), ctx.handle)
 
     def _check(self, rc):
@@ -939,12 +944,16 @@ class ProofServer:
         self._check(lib().azk_server_group_stats(self._h, ctypes.byref(g), ctypes.byref(j)))
         return {"groups": g.value, "grouped_jobs": j.value, "mean_group": j.value / g.value if g.value else 0.0}
 
-    def submit_pcs(self, log_size: int, log_blowup: int, queries: int, rounds: int, coefficients, public_digest: bytes) -> int:
+    def submit_pcs(self, log_size: int, log_blowup: int, queries: int, rounds: int, coefficients, public_digest: bytes,
+                   copy: bool = True) -> int:
         c = _q(coefficients)
         pub = _u8(public_digest)
         jid = ctypes.c_uint64()
-        self._check(lib().azk_server_submit_pcs(self._h, log_size, log_blowup, queries, rounds, _ptr(c), len(c), _ptr(pub), ctypes.byref(jid)))
+        fn = lib().azk_server_submit_pcs if copy else lib().azk_server_submit_pcs_nocopy
+        self._check(fn(self._h, log_size, log_blowup, queries, rounds, _ptr(c), len(c), _ptr(pub), ctypes.byref(jid)))
         self._kind[jid.value] = 0
+        if not copy:
+            self._borrowed[jid.value] = c
         return jid.value
 
     def warm(self, pcs_shapes=(), log_blowup: int = 2, queries: int = 64, sumcheck_logs=()):
@@ -958,18 +967,26 @@ class ProofServer:
         self._check(lib().azk_server_warm(self._h, _ptr(logs) if len(logs) else None, _ptr(rounds) if len(rounds) else None, len(logs),
                                           log_blowup, queries, _ptr(sc) if len(sc) else None, len(sc)))
 
-    def submit_sumcheck(self, evaluations) -> int:
+    def submit_sumcheck(self, evaluations, copy: bool = True) -> int:
         ev = np.ascontiguousarray(evaluations, dtype=np.uint32).reshape(-1)
         jid = ctypes.c_uint64()
-        self._check(lib().azk_server_submit_sumcheck(self._h, _ptr(ev), len(ev), ctypes.byref(jid)))
+        fn = lib().azk_server_submit_sumcheck if copy else lib().azk_server_submit_sumcheck_nocopy
+        self._check(fn(self._h, _ptr(ev), len(ev), ctypes.byref(jid)))
         self._kind[jid.value] = 1
+        if not copy:
+            self._borrowed[jid.value] = ev
         return jid.value
 
     def poll(self, job_id: int, release: bool = True):
         st, lat, n = ctypes.c_int(), ctypes.c_double(), ctypes.c_uint64()
-        self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), ctypes.byref(lat), None, ctypes.byref(n)))
+        try:
+            self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), ctypes.byref(lat), None, ctypes.byref(n)))
+        except AZKError:
+            self._borrowed.pop(job_id, None)  # a failed job reads nothing more
+            raise
         if st.value != 2:
             return None
+        self._borrowed.pop(job_id, None)
         out = np.empty(max(1, n.value), np.uint8)
         self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), None, _ptr(out), ctypes.byref(n)))
         if release:
@@ -990,6 +1007,7 @@ class ProofServer:
         if getattr(self, "_h", None) and self._h.value:
             lib().azk_server_destroy(self._h)
             self._h = _vp()
+            self._borrowed.clear()
 
     def __del__(self):
         try:

@@ -357,11 +357,13 @@ def run_serving(azk, ctx, args, batched_jobs_per_s, batched_elems_per_s=None):
     server = azk.ProofServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), slots=args.serve_slots,
                              schedule=dict(treelet_log=args.treelet_log, group_log=args.group_log, threads=args.threads, use_graph=1))
 
+    # the job inputs are arrays that nothing changes while the server runs: they are
+    # handed over without a copy (the workers read them into page-locked staging)
     def submit(job, i):
         kind, k = job
         if kind == "sc":
-            return server.submit_sumcheck(sc_tables[i % 2])
-        return server.submit_pcs(k, blowup, queries, k - final_log, rng_rows[k], pubs[32 * (i % 4096):32 * (i % 4096) + 32])
+            return server.submit_sumcheck(sc_tables[i % 2], copy=False)
+        return server.submit_pcs(k, blowup, queries, k - final_log, rng_rows[k], pubs[32 * (i % 4096):32 * (i % 4096) + 32], copy=False)
 
     def collect(ids):
         server.wait_all()
@@ -439,7 +441,7 @@ def run_serving(azk, ctx, args, batched_jobs_per_s, batched_elems_per_s=None):
     return {
         "mix": "commit-and-fold jobs log U*[12,22] with P(k) ~ 2^-(k-12)/2 (blowup 4, fold to log 6, 64 queries) : "
                "M31 multilinear sum-check over 2^20 evaluations = 4:1",
-        "slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb,
+        "slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb, "submission": "no-copy (azk_server_submit_*_nocopy)",
         "saturated": {"jobs_per_s": sat_jobs_s, "elems_per_s": sat_elems_s, "jobs": args.serve_backlog, "seconds": t_sat},
         "arrival_rate_jobs_per_s": lam,
         "sustained_jobs_per_s": sustained,

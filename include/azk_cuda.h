@@ -492,10 +492,11 @@ azk_status azk_sumcheck_prove(azk_ctx* ctx, const uint32_t* evaluations, uint64_
  * overlap differ). */
 typedef struct azk_server azk_server;
 azk_status azk_server_create(azk_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t slots, const azk_schedule* schedule, azk_server** out);
-/* Before serving: every worker runs, once, a job of zeros of each listed shape (PCS
- * proofs of 2^pcs_logn[i] coefficients folded for pcs_rounds[i] rounds; sum-checks
- * over 2^sumcheck_logn[i] evaluations), so its device memory for those shapes, its
- * pinned staging and every lazily built table exist before the first real job:
+/* Before serving: every worker proves, once, a group of zero jobs of each group size
+ * of each listed shape (PCS proofs of 2^pcs_logn[i] coefficients folded for
+ * pcs_rounds[i] rounds; sum-checks over 2^sumcheck_logn[i] evaluations), so its
+ * device memory for those shapes, its pinned staging, its captured graphs and every
+ * lazily built table exist before the first real job:
  * creating them in the middle of serving costs allocations and frees that wait for
  * the whole device.  Shapes that do not fit the HBM budget are skipped.  Returns
  * when all workers are done; warm-up jobs produce no results. */
@@ -507,6 +508,15 @@ azk_status azk_server_submit_pcs(azk_server* sv, uint32_t log_size, uint32_t log
 /* M31 multilinear sum-check over `count` (power of two) evaluations
  * (M31MultilinearSumcheckProofBuilderV1, SumcheckOracle.swift:797-868). */
 azk_status azk_server_submit_sumcheck(azk_server* sv, const uint32_t* evaluations, uint64_t count, uint64_t* job_id);
+/* The same two submissions without copying the input: the server keeps the
+ * address and reads the words when a worker takes the job, so they must stay
+ * valid and unchanged until azk_server_poll reports the job done or failed.  The
+ * arguments and the words' canonicality are checked here, as above.  Saves the
+ * copy into fresh host memory (page faults included: about 1.3 ms per 4 MiB table
+ * on the submitting thread). */
+azk_status azk_server_submit_pcs_nocopy(azk_server* sv, uint32_t log_size, uint32_t log_blowup, uint32_t queries, uint32_t rounds,
+                                        const uint32_t* coefficients, uint64_t count, const uint8_t public_digest[32], uint64_t* job_id);
+azk_status azk_server_submit_sumcheck_nocopy(azk_server* sv, const uint32_t* evaluations, uint64_t count, uint64_t* job_id);
 /* state: 0 queued, 1 running, 2 done, 3 failed.  Done: latency = completion -
  * submission; result = proof bytes (PCS) or u32 words {claimed sum, final
  * evaluation, digest[8], sums at 0 [rounds], sums at 1 [rounds], challenges [rounds]}

@@ -202,3 +202,32 @@ def test_sumcheck_lane_batches_many_tables(ctx, oracle):
         assert got["initial_digest"] == want["initial_digest"]
         for key in ("r0", "r1", "challenges"):
             assert np.array_equal(got[key], want[key])
+
+
+def test_nocopy_submissions_match_copied(ctx, oracle):
+    """Jobs submitted without a copy (the server reads the caller's arrays when a
+    worker takes them) give the bytes of the copied submissions; the wrapper holds
+    each array until the job is seen finished, and a non-canonical word is still
+    refused at submission."""
+    rng = np.random.default_rng(0x0C0)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=4 << 30, slots=4)
+    jobs = [_pcs_job(rng, int(k)) for k in rng.integers(10, 17, 16)]
+    tables = [rng.integers(0, P, 1 << int(k), dtype=np.uint32) for k in rng.integers(8, 16, 8)]
+    ids = [server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"], copy=False) for j in jobs]
+    sids = [server.submit_sumcheck(t, copy=False) for t in tables]
+    with pytest.raises(azk.AZKError) as e:
+        server.submit_sumcheck(np.full(16, P, np.uint32), copy=False)
+    assert e.value.name == "invalidInputLayout"
+    res = _wait(server, ids + sids)
+    assert not server._borrowed
+    cids = [server.submit_pcs(j["log_size"], 2, j["queries"], j["rounds"], j["coeffs"], j["pub"]) for j in jobs]
+    csids = [server.submit_sumcheck(t) for t in tables]
+    cres = _wait(server, cids + csids)
+    server.close()
+    for a, b in zip(ids, cids):
+        assert res[a][0] == cres[b][0]
+    for t, a, b in zip(tables, sids, csids):
+        want = oracle.sumcheck_multilinear(t)
+        for got in (res[a][0], cres[b][0]):
+            assert got["initial_digest"] == want["initial_digest"] and got["final"] == want["final"]
+            assert np.array_equal(got["challenges"], want["challenges"])
