@@ -11,6 +11,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/azk_cuda.h"
@@ -153,9 +154,23 @@ struct Timer {
   uint64_t ns() const { return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
-// Wait for everything queued on a stream without spinning a host core: the wait
-// sleeps on a blocking-sync event (the server's workers share the host's cores
-// with each other and with the threads that submit work).
+// Wait for an event by polling it: a short spin, then sleeps growing from 20 to
+// 160 us, so a waiting thread takes little of a host core (the server's workers
+// share the host's cores with each other and with the threads that submit work).
+// Not cudaEventSynchronize on a blocking-sync event, which sleeps until the
+// driver's completion interrupt: with the server's 32 workers waiting that way at
+// once, the device stopped starting work for 40-80 ms about every 2 s.
+inline void wait_event(cudaEvent_t e) {
+  for (int k = 0;; k++) {
+    const cudaError_t q = cudaEventQuery(e);
+    if (q == cudaSuccess) return;
+    if (q != cudaErrorNotReady) AZK_CU(q);
+    if (k < 8) continue;
+    std::this_thread::sleep_for(std::chrono::microseconds(k < 24 ? 20 : k < 48 ? 50 : 160));
+  }
+}
+
+// Wait for everything queued on a stream (wait_event on a per-thread event).
 inline void sync_stream(cudaStream_t s) {
   struct Ev {
     cudaEvent_t e = nullptr;
@@ -170,11 +185,11 @@ inline void sync_stream(cudaStream_t s) {
   if (!ev.e || ev.dev != dev) {
     if (ev.e) cudaEventDestroy(ev.e);
     ev.e = nullptr;
-    AZK_CU(cudaEventCreateWithFlags(&ev.e, cudaEventBlockingSync | cudaEventDisableTiming));
+    AZK_CU(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
     ev.dev = dev;
   }
   AZK_CU(cudaEventRecord(ev.e, s));
-  AZK_CU(cudaEventSynchronize(ev.e));
+  wait_event(ev.e);
 }
 
 // CUDA events around a region of one stream.
@@ -183,8 +198,8 @@ struct GpuTimer {
   cudaStream_t s;
   bool owns = true;
   explicit GpuTimer(cudaStream_t st) : s(st) {
-    AZK_CU(cudaEventCreateWithFlags(&a, cudaEventBlockingSync));
-    AZK_CU(cudaEventCreateWithFlags(&b, cudaEventBlockingSync));
+    AZK_CU(cudaEventCreate(&a));
+    AZK_CU(cudaEventCreate(&b));
     AZK_CU(cudaEventRecord(a, s));
   }
   // With events the caller keeps (nothing created or destroyed per region).
@@ -192,7 +207,7 @@ struct GpuTimer {
   void stop() { AZK_CU(cudaEventRecord(b, s)); }
   double seconds() {
     float ms = 0;
-    AZK_CU(cudaEventSynchronize(b));
+    wait_event(b);
     AZK_CU(cudaEventElapsedTime(&ms, a, b));
     return ms / 1000.0;
   }

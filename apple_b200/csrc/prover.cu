@@ -241,8 +241,8 @@ struct Engine {
       AZK_CU(cudaStreamCreateWithPriority(&s_up, cudaStreamNonBlocking, prio_hi));
     }
     size_t n = cfg.size();
-    if (!tm_a) AZK_CU(cudaEventCreateWithFlags(&tm_a, cudaEventBlockingSync));
-    if (!tm_b) AZK_CU(cudaEventCreateWithFlags(&tm_b, cudaEventBlockingSync));
+    if (!tm_a) AZK_CU(cudaEventCreate(&tm_a));
+    if (!tm_b) AZK_CU(cudaEventCreate(&tm_b));
     hsmall.ensure(64 + align_up(sizeof(InputInfo) * n, 16) + sizeof(ScanJob) * n);
     leaf_values = cfg.empty() ? 1 : cfg[0].leaf_values;
     for (auto& i : cfg) {
