@@ -1491,6 +1491,25 @@ void lane_submit(azk_server* sv, int slot) {
   sv->lane_cv.notify_all();
 }
 
+// A table of two zeros through a slot on lane stream `s`: a stream's first launch
+// and the first device-mapped writes into a slot's staging cost more than later
+// ones, so warm-up takes them before serving.
+void lane_touch(SumcheckSlot& sl, cudaStream_t s) {
+  uint8_t* pin = sl.pin.p;
+  SumcheckOut* h = reinterpret_cast<SumcheckOut*>(pin + align_up(4ull << sl.cap_log, 64));
+  SumcheckOut* dh = nullptr;
+  AZK_CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dh), h, 0));
+  uint32_t* drounds = reinterpret_cast<uint32_t*>(dh + 1);
+  *h = SumcheckOut{};
+  h->r0 = drounds;
+  h->r1 = drounds + 1;
+  h->challenges = drounds + 2;
+  AZK_CU(cudaMemsetAsync(sl.bufs.ev.p, 0, 8, s));
+  SumcheckBatch b{};
+  b.job[0] = SumcheckJob{sl.bufs.ev.as<uint32_t>(), sl.bufs.scratch.as<uint32_t>(), dh, 1, 0};
+  AZK_CU(launch_sumcheck_batch(b, 1, s));
+}
+
 // Lane launcher: whenever tables wait and a lane stream is idle, one batched
 // launch proves up to kLaneBatch of them.
 void lane_launcher(azk_server* sv) {
@@ -1508,6 +1527,12 @@ void lane_launcher(azk_server* sv) {
       }
       sid = sv->sc_idle.back();
       sv->sc_idle.pop_back();
+      // Tables arriving together (a burst or a backlog: workers stage them one after
+      // another) are gathered for up to 1 ms into one launch, so they share launches
+      // instead of each taking a lane stream for a whole digest; a table that waits
+      // alone goes at once.
+      if (sv->sc_pending.size() >= 2 && sv->sc_pending.size() < (size_t)kLaneBatch)
+        sv->lane_cv.wait_for(lk, std::chrono::milliseconds(1), [&] { return sv->sc_pending.size() >= (size_t)kLaneBatch || sv->lane_stop; });
       while (!sv->sc_pending.empty() && batch.size() < (size_t)kLaneBatch) {
         batch.push_back(sv->sc_pending.front());
         sv->sc_pending.pop_front();
@@ -1875,6 +1900,8 @@ azk_status azk_server_warm(azk_server* sv, const uint32_t* pcs_logn, const uint3
           sumcheck_alloc(sl->bufs, sc_log);
           sl->grow = false;
           sl->pin.ensure(sumcheck_pinned_bytes(sc_log));
+          lane_touch(*sl, sv->sc_stream[k % kLaneStreams].s);
+          sync_stream(sv->sc_stream[k % kLaneStreams].s);  // the slot's staging is idle again
         } catch (...) {
           std::lock_guard<std::mutex> lk(sv->mu);
           sl->grow = true;
