@@ -1369,34 +1369,42 @@ bool try_take(azk_server* sv, int w, Take& tk, Dropped& dropped) {
     while (pick != sv->queue.end() && (*pick)->kind == 1) ++pick;
     if (pick == sv->queue.end()) return false;
   }
-  std::shared_ptr<ServeJob> j = *pick;
-  if (j->kind == 1) {
-    // a sum-check goes to a free lane slot; a slot smaller than the table grows
+  // a sum-check goes to a free lane slot; a slot smaller than the table grows
+  auto admit_sumcheck = [&](std::deque<std::shared_ptr<ServeJob>>::iterator it) {
     if (sv->sc_free.empty()) return false;
+    const std::shared_ptr<ServeJob> sj = *it;
     // the slot leaves the free list first, so making room never takes its buffers
     const int slot = sv->sc_free.back();
     sv->sc_free.pop_back();
     SumcheckSlot& sl = *sv->sc_slot[slot];
-    if (sl.cap_log < j->logn) {
-      const uint64_t extra = sumcheck_table_bytes(j->logn) - (sl.cap_log ? sumcheck_table_bytes(sl.cap_log) : 0);
+    if (sl.cap_log < sj->logn) {
+      const uint64_t extra = sumcheck_table_bytes(sj->logn) - (sl.cap_log ? sumcheck_table_bytes(sl.cap_log) : 0);
       if (!make_room(sv, w, extra, dropped)) {
         sv->sc_free.push_back(slot);
         return false;
       }
       sv->held += extra;
-      sl.cap_log = j->logn;  // the worker reallocates before filling the slot
+      sl.cap_log = sj->logn;  // the worker reallocates before filling the slot
       sl.grow = true;
     }
-    sl.job = j;
-    sv->queue.erase(pick);
+    sl.job = sj;
+    sv->queue.erase(it);
     sv->queued_sc--;
     sv->running++;
     sv->busy[w] = 1;
-    j->state = 1;
-    j->started = std::chrono::steady_clock::now();
+    sj->state = 1;
+    sj->started = std::chrono::steady_clock::now();
     tk.slot = slot;
     return true;
+  };
+  if ((*pick)->kind == 1) {
+    if (admit_sumcheck(pick)) return true;
+    // a sum-check taken ahead of the front proof job whose slot cannot grow leaves
+    // that proof job to be taken instead
+    if (pick == sv->queue.begin()) return false;
+    pick = sv->queue.begin();
   }
+  std::shared_ptr<ServeJob> j = *pick;
   auto& cache = sv->cache[w];
   const ShapeKey key = shape_of(*j);
   if (!cache.count(key)) {
