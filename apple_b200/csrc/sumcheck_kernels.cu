@@ -73,7 +73,8 @@ struct WarpKeccak {
   }
 
   __device__ __forceinline__ void permute(uint64_t& a) const {
-#pragma unroll 1
+    // all 24 rounds unrolled: the round constants are immediates
+#pragma unroll
     for (int r = 0; r < 24; r += 8) {
 #pragma unroll
       for (int k = 0; k < 8; k++) {
