@@ -934,6 +934,7 @@ class ProofServer:
         self._h = _vp()
         self._kind = {}
         self._borrowed = {}  # job id -> the array a no-copy submission reads
+        self._pollbuf = np.empty(0, np.uint8)
         check(lib().azk_server_create(ctx.handle, int(hbm_budget_bytes), int(slots), _sched(schedule), ctypes.byref(self._h)), ctx.handle)
 
     def _check(self, rc):
@@ -987,12 +988,16 @@ class ProofServer:
         if st.value != 2:
             return None
         self._borrowed.pop(job_id, None)
-        out = np.empty(max(1, n.value), np.uint8)
+        # one reused landing buffer (a fresh one per result would take new pages for
+        # every proof); the result handed back is its own copy
+        if len(self._pollbuf) < max(1, n.value):
+            self._pollbuf = np.empty(max(1, n.value), np.uint8)
+        out = self._pollbuf
         self._check(lib().azk_server_poll(self._h, job_id, ctypes.byref(st), None, _ptr(out), ctypes.byref(n)))
         if release:
             self._check(lib().azk_server_release(self._h, job_id))
         kind = self._kind.pop(job_id, 0) if release else self._kind.get(job_id, 0)
-        res = out[:n.value].tobytes() if kind == 0 else _sumcheck_words(out[:n.value].view(np.uint32))
+        res = out[:n.value].tobytes() if kind == 0 else _sumcheck_words(out[:n.value].copy().view(np.uint32))
         return res, lat.value
 
     def wait_all(self):
