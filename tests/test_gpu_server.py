@@ -231,3 +231,23 @@ def test_nocopy_submissions_match_copied(ctx, oracle):
         for got in (res[a][0], cres[b][0]):
             assert got["initial_digest"] == want["initial_digest"] and got["final"] == want["final"]
             assert np.array_equal(got["challenges"], want["challenges"])
+
+
+def test_lane_smallest_tables_beside_larger_ones(ctx, oracle):
+    """Tables of 2, 4 and 8 evaluations (the round-0 sums of the smallest taken by
+    one thread, the fold of the last rounds by one thread) share packed launches
+    with larger tables and each give the oracle's proof."""
+    rng = np.random.default_rng(0x5C6)
+    server = azk.ProofServer(ctx, hbm_budget_bytes=1 << 30, slots=2)
+    sizes = [1, 2, 3, 12, 1, 9, 2, 16, 3, 1, 5]
+    tables = [rng.integers(0, P, 1 << k, dtype=np.uint32) for k in sizes]
+    ids = [server.submit_sumcheck(t, copy=False) for t in tables]
+    res = _wait(server, ids)
+    server.close()
+    for t, i in zip(tables, ids):
+        want = oracle.sumcheck_multilinear(t)
+        got = res[i][0]
+        assert got["claimed_sum"] == want["claimed_sum"] and got["final"] == want["final"]
+        assert got["initial_digest"] == want["initial_digest"]
+        for key in ("r0", "r1", "challenges"):
+            assert np.array_equal(got[key], want[key])
